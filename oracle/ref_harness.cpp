@@ -1,0 +1,397 @@
+/*
+ * C-ABI harness over the UNMODIFIED reference sources (test infrastructure).
+ *
+ * oracle/build_ref.py compiles every file of the reference's library/ and
+ * checks/ directories, exactly as they lie in the reference tree, together
+ * with this file into oracle/_ref/libyahmc_ref_<config>.so, once per
+ * compile-time physics configuration (-DNC, -DREPR_*, -DCLOVER_TERM,
+ * -DUPDATE_EO, -DBC_*: programs/Makefile:6-45).  This file only sets the
+ * reference's globals up the way programs/hmc.cpp:66-126 does and forwards
+ * plain pointers to the reference's own functions, so the parity tests, the
+ * golden-vector generator and the CPU baseline of bench.py can drive the
+ * reference through ctypes.
+ *
+ * Nothing in the product links or loads this library.
+ *
+ * Host data layouts are the reference's own:
+ *   spinor field : outer.vol4 x Spinor{ re[REPR_DIM][4], im[REPR_DIM][4] }  (include/spinor.h:7-9)
+ *   fund links   : 4*outer.vol4 x suNg{ re[NC*NC], im[NC*NC] }  index 4*id+mu  (include/gaugefield.h:6-7)
+ *   repr links   : 4*outer.vol4 x suNf                                         (include/gaugefield.h:9-10)
+ *   momenta      : 4*outer.vol4 x suNa{ av[NG] }                                (include/gaugefield.h:12-13)
+ *   clover term  : 4*outer.vol4 x suNf, clover force 6*outer.vol4 x suNf         (include/clover.h:12-16)
+ */
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+/* reference headers last: include/gaugefield.h:6 defines a macro named link */
+#include <global.h>
+#include <settings.h>
+#include <linalg.h>
+#include <dirac.h>
+#include <inverter.h>
+#include <forces.h>
+#include <clover.h>
+#include <bcs.h>
+#include <repr.h>
+#include <random.h>
+#include <rational.h>
+#include <staples.h>
+#include <wilsonloop.h>
+#include <checks.h>
+#include <timing.h>
+
+static int harness_ready = 0;
+
+static void wrap(SpinorField &sf, double *p)
+{
+	sf.ptr = (Spinor*)p;
+	sf.allocated = false;
+	spinor_type_default(sf);
+}
+
+/* view: 0 = the reference's default view, 1 = even, 2 = odd, 3 = full */
+static void set_view(SpinorField &sf, int view)
+{
+	switch(view)
+	{
+		case 1: spinor_type_even(sf); break;
+		case 2: spinor_type_odd(sf); break;
+		case 3: spinor_type_full(sf); break;
+		default: spinor_type_default(sf); break;
+	}
+}
+
+static mvm_operator op_from_id(int op)
+{
+	switch(op)
+	{
+		case 0: return Dphi;
+		case 1: return Hphi;
+		case 2: return Hphi_sq;
+		default: return 0;
+	}
+}
+
+extern "C" {
+
+/* Compile-time configuration of this build. */
+void yref_info(int *out)
+{
+	out[0] = NC;
+	out[1] = REPR_DIM;
+	out[2] = NG;
+	out[3] = REPR_ID;
+#ifdef CLOVER_TERM
+	out[4] = 1;
+#else
+	out[4] = 0;
+#endif
+#ifdef UPDATE_EO
+	out[5] = 1;
+#else
+	out[5] = 0;
+#endif
+#if defined(BC_ANTIPERIODIC)
+	out[6] = 1;
+#elif defined(BC_OPEN)
+	out[6] = 2;
+#elif defined(BC_SF)
+	out[6] = 3;
+#else
+	out[6] = 0;
+#endif
+	out[7] = (int)sizeof(Spinor);
+	out[8] = (int)sizeof(suNf);
+	out[9] = (int)sizeof(ldl_t);
+}
+
+/*
+ * Set up geometry, representation, boundary conditions and the clover term
+ * the way programs/hmc.cpp:72-117 does (single rank, border 1).  The lattice
+ * sizes reach the reference through its own settings reader, so they are
+ * written to a temporary cfg file first.  May be called once per process.
+ */
+int yref_init(int T, int X, int Y, int Z, double csw, double cf, int threads, int seed, int log_level)
+{
+	if(harness_ready)
+	{
+		return (global.dim_t == T && global.dim_x == X && global.dim_y == Y && global.dim_z == Z) ? 0 : -1;
+	}
+
+	char path[] = "/tmp/yahmc_oracle_cfgXXXXXX";
+	int fd = mkstemp(path);
+	if(fd < 0) return -2;
+	FILE *fp = fdopen(fd, "w");
+	fprintf(fp, "[lattice]\ndim_t = %d\ndim_x = %d\ndim_y = %d\ndim_z = %d\n", T, X, Y, Z);
+	fprintf(fp, "[parallel]\nthreads = %d\nnp_t = 1\nnp_x = 1\nnp_y = 1\nnp_z = 1\n", threads);
+	fprintf(fp, "[log]\nlevel = %d\n", log_level);
+	fclose(fp);
+
+	char *argv0 = (char*)"oracle";
+	mp_init(1, &argv0);
+	var_init(path);
+	remove(path);
+	if(log_level >= 0)
+	{
+		logger_init("", log_level);
+	}
+	geometry_init(1);
+	mp_setup();
+	rand_init(seed);
+	repr_init();
+	bcs_init(cf);
+	clover_init(csw);
+	gauge_field_init();
+	gauge_field_set_unit();
+	harness_ready = 1;
+	return 0;
+}
+
+long yref_volume(void)
+{
+	return (long)outer.vol4;
+}
+
+void yref_set_threads(int threads)
+{
+#ifdef _OPENMP
+	omp_set_num_threads(threads);
+#endif
+}
+
+/* site[id].coord (t,x,y,z) and fw/bk neighbour tables, 4 ints each per site */
+void yref_geometry(int *coord, int *fw, int *bk)
+{
+	for(int id = 0; id < outer.vol4; id++)
+	{
+		for(int mu = 0; mu < 4; mu++)
+		{
+			coord[4*id+mu] = site[id].coord[mu];
+			fw[4*id+mu] = site[id].fw[mu];
+			bk[4*id+mu] = site[id].bk[mu];
+		}
+	}
+}
+
+/* Fundamental links in, then the reference's represent_gauge_field() (repr.cpp:265-280). */
+void yref_set_links(const double *fund)
+{
+	memcpy(gfield_fund, fund, sizeof(suNg)*4*outer.vol4);
+	represent_gauge_field();
+}
+
+void yref_get_links(double *fund)
+{
+	memcpy(fund, gfield_fund, sizeof(suNg)*4*outer.vol4);
+}
+
+/* The reference's own random start (suNg::random, suNg.cpp:375-380) + gauge BCs + represent. */
+void yref_set_random_links(void)
+{
+	gauge_field_set_random();
+}
+
+void yref_apply_bcs_on_gauge_field(void)
+{
+	apply_bcs_on_gauge_field();
+}
+
+void yref_get_repr_links(double *out)
+{
+	memcpy(out, gfield_repr, sizeof(suNf)*4*outer.vol4);
+}
+
+void yref_get_clover_term(double *out)
+{
+#ifdef CLOVER_TERM
+	memcpy(out, cl_term, sizeof(suNf)*4*outer.vol4);
+#endif
+}
+
+/* LDL factors for sigma = 4+mass (clover.cpp:307-328), both blocks, odd sites filled. */
+void yref_get_ldl(double mass, double *out)
+{
+#ifdef CLOVER_TERM
+	compute_ldl_decomp(4.0+mass);
+	memcpy(out, cl_ldl, sizeof(ldl_t)*outer.vol4);
+#endif
+}
+
+void yref_get_clover_force(double *out)
+{
+#ifdef CLOVER_TERM
+	memcpy(out, cl_force, sizeof(suNf)*6*outer.vol4);
+#endif
+}
+
+void yref_set_clover_force(const double *in)
+{
+#ifdef CLOVER_TERM
+	memcpy(cl_force, in, sizeof(suNf)*6*outer.vol4);
+#endif
+}
+
+void yref_get_generators(double *fund, double *repr)
+{
+	memcpy(fund, iTfund, sizeof(suNg)*NG);
+	memcpy(repr, iTrepr, sizeof(suNf)*NG);
+}
+
+void yref_represent(double *repr_out, const double *fund_in, int count)
+{
+	represent_links((suNf*)repr_out, (suNg*)fund_in, count);
+}
+
+/* ---- Dirac operator (dirac.h) ---- */
+void yref_Dphi_oe(double *dst, double *src) { SpinorField d, s; wrap(d, dst); wrap(s, src); Dphi_oe(d, s); }
+void yref_Dphi_eo(double *dst, double *src) { SpinorField d, s; wrap(d, dst); wrap(s, src); Dphi_eo(d, s); }
+void yref_Dphi_ee(double m, double *dst, double *src) { SpinorField d, s; wrap(d, dst); wrap(s, src); Dphi_ee(m, d, s); }
+void yref_Dphi_oo(double m, double *dst, double *src) { SpinorField d, s; wrap(d, dst); wrap(s, src); Dphi_oo(m, d, s); }
+void yref_Dphi_oo_inv(double m, double *dst, double *src) { SpinorField d, s; wrap(d, dst); wrap(s, src); Dphi_oo_inv(m, d, s); }
+void yref_Dphi(double m, double *dst, double *src) { SpinorField d, s; wrap(d, dst); wrap(s, src); Dphi(m, d, s); }
+void yref_Hphi(double m, double *dst, double *src) { SpinorField d, s; wrap(d, dst); wrap(s, src); Hphi(m, d, s); }
+void yref_Hphi_sq(double m, double *dst, double *src) { SpinorField d, s; wrap(d, dst); wrap(s, src); Hphi_sq(m, d, s); }
+int yref_mvm_get(void) { return mvm_get(); }
+void yref_mvm_reset(void) { mvm_reset(); }
+
+/* ---- clover (clover.h) ---- */
+double yref_clover_logdet(double m) { return clover_logdet(m); }
+
+/* ---- spinor linear algebra (linalg.h), view as in set_view() ---- */
+void yref_spinor_random(double *a, int view) { SpinorField f; wrap(f, a); set_view(f, view); spinor_random(f); }
+void yref_spinor_zero(double *a) { SpinorField f; wrap(f, a); spinor_zero(f); }
+void yref_spinor_copy(double *a, double *b) { SpinorField f, g; wrap(f, a); wrap(g, b); spinor_copy(f, g); }
+void yref_spinor_g5(double *a, int view) { SpinorField f; wrap(f, a); set_view(f, view); spinor_g5(f); }
+double yref_spinor_sqnorm(double *a, int view) { SpinorField f; wrap(f, a); set_view(f, view); return spinor_sqnorm(f); }
+double yref_spinor_product_re(double *a, double *b, int view)
+{
+	SpinorField f, g; wrap(f, a); wrap(g, b); set_view(f, view); set_view(g, view);
+	return spinor_product_re(f, g);
+}
+void yref_spinor_product(double *a, double *b, int view, double *out)
+{
+	SpinorField f, g; wrap(f, a); wrap(g, b); set_view(f, view); set_view(g, view);
+	complex c = spinor_product(f, g);
+	out[0] = c.re; out[1] = c.im;
+}
+/* op: 0 add, 1 sub, 2 mulr, 3 mulc, 4 mulr_assign, 5 mulc_assign,
+ *     6 mulr_add, 7 mulc_add, 8 mulr_sub, 9 mulc_sub */
+void yref_spinor_axpy(int op, double *a, double re, double im, double *b, int view)
+{
+	SpinorField f, g; wrap(f, a); set_view(f, view);
+	if(b) { wrap(g, b); set_view(g, view); }
+	complex c(re, im);
+	switch(op)
+	{
+		case 0: spinor_add_assign(f, g); break;
+		case 1: spinor_sub_assign(f, g); break;
+		case 2: spinor_mulr(f, re, g); break;
+		case 3: spinor_mulc(f, c, g); break;
+		case 4: spinor_mulr_assign(f, re); break;
+		case 5: spinor_mulc_assign(f, c); break;
+		case 6: spinor_mulr_add_assign(f, re, g); break;
+		case 7: spinor_mulc_add_assign(f, c, g); break;
+		case 8: spinor_mulr_sub_assign(f, re, g); break;
+		case 9: spinor_mulc_sub_assign(f, c, g); break;
+	}
+}
+
+/* ---- inverters (inverter.h); op: 0 Dphi, 1 Hphi, 2 Hphi_sq ---- */
+int yref_cg(int op, double mass, double prec, double *x, double *b)
+{
+	inv_par par; SpinorField fx, fb; wrap(fx, x); wrap(fb, b);
+	par.prec = prec; par.mass = mass; par.mvm = op_from_id(op);
+	return cg_inverter(par, fx, fb);
+}
+int yref_bicgstab(int op, double mass, double prec, double *x, double *b)
+{
+	inv_par par; SpinorField fx, fb; wrap(fx, x); wrap(fb, b);
+	par.prec = prec; par.mass = mass; par.mvm = op_from_id(op);
+	return bicgstab_inverter(par, fx, fb);
+}
+int yref_minres(int op, double mass, double prec, double *x, double *b)
+{
+	inv_par par; SpinorField fx, fb; wrap(fx, x); wrap(fb, b);
+	par.prec = prec; par.mass = mass; par.mvm = op_from_id(op);
+	return minres_inverter(par, fx, fb);
+}
+int yref_auto_inverter(int op, double mass, double prec, double *x, double *b)
+{
+	inv_par par; SpinorField fx, fb; wrap(fx, x); wrap(fb, b);
+	par.prec = prec; par.mass = mass; par.mvm = op_from_id(op);
+	return auto_inverter(par, fx, fb);
+}
+/* xs: num consecutive spinor fields */
+int yref_cg_mshift(int op, double mass, double prec, int num, double *shifts, double *xs, double *b)
+{
+	inv_par par; SpinorField fb; wrap(fb, b);
+	SpinorField *fx = new SpinorField[num];
+	long stride = (long)outer.vol4 * (sizeof(Spinor)/sizeof(double));
+	for(int n = 0; n < num; n++) wrap(fx[n], xs + n*stride);
+	par.prec = prec; par.mass = mass; par.mvm = op_from_id(op); par.num = num; par.shift = shifts;
+	int it = cg_mshift(par, fx, fb);
+	delete[] fx;
+	return it;
+}
+
+/* rational_find + rational_calc (rational.cpp:68-166); meta out: order, a0, poles[], residues[] */
+void yref_rational(int n, int d, double rprec, double emin, double emax, int op, double mass,
+                   double prec, double *x, double *b, double *meta)
+{
+	rational_app app;
+	rational_find(app, n, d, rprec, emin, emax);
+	SpinorField fx, fb; wrap(fx, x); wrap(fb, b);
+	rational_calc(app, op_from_id(op), mass, prec, fx, fb);
+	meta[0] = app.order;
+	meta[1] = app.a0;
+	for(int i = 0; i < app.order; i++)
+	{
+		meta[2+i] = app.pole[i];
+		meta[2+48+i] = app.residue[i];
+	}
+}
+
+/* ---- forces (forces.h); momenta live in afield_momenta ---- */
+void yref_zero_momenta(void)
+{
+	suNa zero;
+	for(int id = 0; id < 4*outer.vol4; id++) afield_momenta[id] = zero;
+}
+void yref_get_momenta(double *out) { memcpy(out, afield_momenta, sizeof(suNa)*4*outer.vol4); }
+void yref_set_momenta(const double *in) { memcpy(afield_momenta, in, sizeof(suNa)*4*outer.vol4); }
+void yref_begin_fermion_force(void) { begin_fermion_force(); }
+void yref_end_fermion_force(double dt) { end_fermion_force(dt); }
+void yref_wilson_fermion_force(double dt, double mass, double residue, double *lhs, double *rhs)
+{
+	SpinorField l, r; wrap(l, lhs); wrap(r, rhs);
+	wilson_fermion_force(dt, mass, residue, l, r);
+}
+void yref_wilson_fermion_force_q(double dt, double mass, double residue, double *rhs)
+{
+	SpinorField r; wrap(r, rhs);
+	wilson_fermion_force_q(dt, mass, residue, r);
+}
+void yref_clover_fermion_force(double residue, double *lhs, double *rhs)
+{
+#ifdef CLOVER_TERM
+	SpinorField l, r; wrap(l, lhs); wrap(r, rhs);
+	clover_fermion_force(residue, l, r);
+#endif
+}
+void yref_clover_logdet_force(double mass, double residue) { clover_logdet_force(mass, residue); }
+void yref_wilson_gauge_force(double dt, double beta) { wilson_gauge_force(dt, beta); }
+void yref_improved_gauge_force(double dt, double beta, double c0, double c1) { improved_gauge_force(dt, beta, c0, c1); }
+double yref_avr_wilson(int h, int w) { return avr_wilson(h, w); }
+
+/* ---- the reference's own self-checks (checks/check.cpp:4-26) ---- */
+int yref_check_group(void) { return check_group(); }
+int yref_check_dirac(void) { return check_dirac(); }
+int yref_check_inverters(void) { return check_inverters(); }
+
+double yref_timestamp(void) { return timestamp(); }
+
+}

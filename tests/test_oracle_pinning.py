@@ -1,0 +1,155 @@
+"""Pin the numpy oracle (oracle/yahmc_oracle.py) to the unmodified reference.
+
+The reference is compiled from its own sources into oracle/_ref by
+oracle/build_ref.py; these tests feed both the same seeded 8^4 fields (8^4 is
+the smallest lattice the reference accepts, geometry.cpp:1140-1144) and
+require agreement to rounding.  Skipped when oracle/_ref has not been built
+(for example on a machine without the reference sources); the committed golden
+vectors in tests/golden/ pin the oracle there instead.
+"""
+import numpy as np
+import pytest
+
+from oracle import ref, yahmc_oracle as yo
+from yahmc_b200 import fields
+
+DIMS = (8, 8, 8, 8)
+TOL = 1e-13
+
+
+def _setup(name, seed):
+    if not ref.available(name):
+        pytest.skip("oracle/_ref not built")
+    nc, rep, bc, clover, eo = ref.CONFIGS[name]
+    R = ref.get(name, DIMS)
+    O = yo.Oracle(yo.Params(DIMS, nc, rep, bc, clover, eo, 1.0, 1.0))
+    rng = np.random.default_rng(seed)
+    U = fields.haar_su(nc, O.V * 4, rng).reshape(O.V, 4, nc, nc)
+    R.set_links(fields.complex_to_raw(U))
+    O.set_links(U)
+    src = fields.gaussian_spinor(O.V, O.d, rng)
+    O.bcs_on_spinor(src)
+    return R, O, rng, src
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.parametrize("name", list(ref.CONFIGS))
+def test_geometry_links_clover(name):
+    R, O, rng, src = _setup(name, 1)
+    c, f, b = R.geometry()
+    assert np.array_equal(c, O.coord) and np.array_equal(f, O.fw) and np.array_equal(b, O.bk)
+    V, d = O.V, O.d
+    assert _rel(yo.mat_from_raw(R.repr_links(), d).reshape(V, 4, d, d), O.links) < TOL
+    gf, gr = R.generators()
+    assert _rel(yo.mat_from_raw(gf, O.nc), O.itfund) < TOL
+    assert _rel(yo.mat_from_raw(gr, d), O.itrepr) < TOL
+    if O.p.clover:
+        assert _rel(yo.mat_from_raw(R.clover_term(), d).reshape(V, 4, d, d), O.cl_term) < TOL
+        for m in (-0.75, 0.1):
+            lr = R.ldl(m).reshape(V, 2, d * (2 * d + 1), 2)
+            lr = lr[..., 0] + 1j * lr[..., 1]
+            lo = O.compute_ldl(4 + m)
+            assert _rel(lr[V // 2:], lo[V // 2:]) < TOL
+            assert abs(R.call("clover_logdet", m) - O.clover_logdet(m)) < 1e-12 * abs(O.clover_logdet(m))
+
+
+@pytest.mark.parametrize("name", list(ref.CONFIGS))
+def test_dirac_operators(name):
+    R, O, rng, src = _setup(name, 2)
+    d = O.d
+    fns = [("Dphi", -0.75), ("Hphi", -0.3), ("Hphi_sq", -0.75)]
+    if O.p.eo:
+        fns += [("Dphi_oe", None), ("Dphi_eo", None)]
+        if O.p.clover:
+            fns += [("Dphi_ee", -0.75), ("Dphi_oo", 0.2), ("Dphi_oo_inv", -0.75)]
+    for fn, mass in fns:
+        s1 = yo.spinor_to_raw(src)
+        d1 = R.spinor()
+        args = ([mass] if mass is not None else []) + [d1, s1]
+        R.call(fn, *args)
+        s2 = src.copy()
+        d2 = O.new_field()
+        getattr(O, fn)(*(([mass] if mass is not None else []) + [d2, s2]))
+        assert _rel(yo.spinor_from_raw(d1, d), d2) < TOL, fn
+        # aliasing semantics: Dphi writes scratch into the odd half of its source
+        assert _rel(yo.spinor_from_raw(s1, d), s2) < TOL, fn
+
+
+@pytest.mark.parametrize("name", ["su3_fund_ap", "su2_adj_ap", "su3_fund_open", "su3_fund_ap_nocl", "su3_fund_ap_full"])
+def test_inverters(name):
+    R, O, rng, src = _setup(name, 3)
+    d = O.d
+    lo, hi = O.default_range()
+    m = -0.2
+    cases = [("cg", 2, "Hphi_sq"), ("bicgstab", 0, "Dphi"), ("minres", 1, "Hphi"), ("auto_inverter", 2, "Hphi_sq")]
+    for fn, op, opn in cases:
+        x1 = R.spinor()
+        b1 = yo.spinor_to_raw(src)
+        it1 = R.call(fn, op, m, 1e-24, x1, b1)
+        x2 = O.new_field()
+        it2 = getattr(O, fn)(opn, m, 1e-24, x2, src.copy())
+        assert abs(it1 - it2) <= 2, (fn, it1, it2)
+        assert _rel(yo.spinor_from_raw(x1, d)[lo:hi], x2[lo:hi]) < 1e-11, fn
+    sh = np.array([0.5, 0.1, 0.05, 1.05])     # the shifts of checks/inverters.cpp:143-146
+    xs1 = np.zeros(4 * O.V * 8 * d)
+    it1 = R.call("cg_mshift", 2, m, 1e-24, 4, sh, xs1, yo.spinor_to_raw(src))
+    it2, xs2 = O.cg_mshift("Hphi_sq", m, 1e-24, list(sh), src.copy())
+    assert abs(it1 - it2) <= 1
+    xs1 = yo.spinor_from_raw(xs1, d).reshape(4, O.V, d, 4)
+    for i in range(4):
+        assert _rel(xs1[i][lo:hi], xs2[i][lo:hi]) < 1e-11
+
+
+@pytest.mark.parametrize("name", ["su3_fund_ap", "su2_adj_ap", "su3_sym_ap", "su3_fund_sf", "su3_fund_ap_nocl"])
+def test_forces(name):
+    R, O, rng, src = _setup(name, 4)
+    V, d = O.V, O.d
+    R.zero_momenta()
+    O.mom[:] = 0
+    R.call("begin_fermion_force")
+    O.begin_fermion_force()
+    a = fields.gaussian_spinor(V, d, rng)
+    b = fields.gaussian_spinor(V, d, rng)
+    O.bcs_on_spinor(a)
+    O.bcs_on_spinor(b)
+    a1, b1 = yo.spinor_to_raw(a), yo.spinor_to_raw(b)
+    a2, b2 = a.copy(), b.copy()
+    R.call("wilson_fermion_force", 0.1, -0.75, 1.3, a1, b1)
+    O.wilson_fermion_force(0.1, -0.75, 1.3, a2, b2)
+    assert _rel(R.momenta().reshape(V, 4, -1), O.mom) < TOL
+    assert _rel(yo.spinor_from_raw(a1, d), a2) < TOL and _rel(yo.spinor_from_raw(b1, d), b2) < TOL
+    R.call("wilson_fermion_force_q", 0.07, -0.75, 0.9, b1)
+    O.wilson_fermion_force_q(0.07, -0.75, 0.9, b2)
+    if O.p.clover:
+        assert _rel(yo.mat_from_raw(R.clover_force(), d).reshape(V, 6, d, d), O.cl_force) < TOL
+        R.call("clover_logdet_force", -0.75, 2.0)
+        O.clover_logdet_force(-0.75, 2.0)
+        assert _rel(yo.mat_from_raw(R.clover_force(), d).reshape(V, 6, d, d), O.cl_force) < TOL
+        R.call("end_fermion_force", 0.1)
+        O.end_fermion_force(0.1)
+    assert _rel(R.momenta().reshape(V, 4, -1), O.mom) < TOL
+
+
+@pytest.mark.parametrize("name", ["su3_fund_ap", "su2_fund_ap", "su4_fund_ap"])
+def test_gauge_support(name):
+    R, O, rng, src = _setup(name, 5)
+    R.zero_momenta()
+    O.mom[:] = 0
+    R.call("wilson_gauge_force", 0.1, 5.6)
+    O.wilson_gauge_force(0.1, 5.6)
+    assert _rel(R.momenta().reshape(O.V, 4, -1), O.mom) < TOL
+    assert abs(R.call("avr_wilson", 1, 1) - O.plaquette()) < 1e-14
+
+
+def test_reference_self_checks_pass():
+    """The reference's own --run-checks (checks/check.cpp:4-26) pass on the compiled oracle."""
+    if not ref.available("su3_fund_ap"):
+        pytest.skip("oracle/_ref not built")
+    R = ref.get("su3_fund_ap", DIMS, seed=99)
+    R.set_random_links()
+    assert R.call("check_group") == 0
+    assert R.call("check_dirac") == 0
+    assert R.call("check_inverters") == 0
