@@ -1,0 +1,193 @@
+/*
+ * yahmc_gpu.h -- C ABI of the B200 (sm_100a) fermion engine for YaHMC.
+ *
+ * The engine replaces YaHMC's fermion hot path: the even-odd preconditioned
+ * Wilson-clover Dirac operator, the clover term and its site-local inverse, the
+ * inverters, the spinor-field linear algebra and the fermion forces.  Every
+ * entry point below names the reference function it replaces (file:line in
+ * the YaHMC tree).  A C++ shim with YaHMC's own signatures (dirac.h,
+ * inverter.h, linalg.h, clover.h, forces.h) sits on top of this ABI; see
+ * INTEGRATION.md.
+ *
+ * Conventions
+ *  - Plain C types only.  Every function returns an int status (yg_status);
+ *    yg_last_error() gives the message of the last failure on this thread.
+ *  - A lattice handle owns the device copies of the global state the reference
+ *    keeps in globals: represented links (gfield_repr), fundamental links
+ *    (gfield_fund), clover term (cl_term), LDL factors (cl_ldl), clover force
+ *    (cl_force) and momenta (afield_momenta).
+ *  - Spinor fields are device buffers of yg_info.field_doubles doubles
+ *    allocated by yg_field_alloc.  Their device layout is private (site-major
+ *    structure of arrays); yg_field_upload / yg_field_download convert from /
+ *    to the reference's host layout: V records Spinor{re[d][4], im[d][4]}
+ *    (include/spinor.h:7-9) in the reference's site order.
+ *  - view arguments select the site range like spinor_select_* / spinor_type_*
+ *    (linalg.cpp:272-329): YG_VIEW_DEFAULT (even sites with even-odd
+ *    preconditioning, all sites without), YG_VIEW_EVEN, YG_VIEW_ODD, YG_VIEW_FULL.
+ *  - Precisions are squared relative residuals, as in the reference
+ *    (README.md:154, cg.cpp:189).
+ *  - All work is issued on the lattice's stream (default: the legacy default
+ *    stream); functions returning host scalars synchronise it.
+ */
+#ifndef YAHMC_GPU_H
+#define YAHMC_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  YG_OK = 0,
+  YG_ERR_ARG = 1,          /* invalid argument or unsupported configuration */
+  YG_ERR_CUDA = 2,         /* CUDA runtime error */
+  YG_ERR_OOM = 3,          /* device allocation failed (memory.cpp:11-18 analogue) */
+  YG_MAXITER = 4,          /* solver reached maxiter before the stopping criterion */
+  YG_STALL = 5,            /* solver stopped making progress */
+  YG_NONFINITE = 6,        /* NaN/Inf met in a reduction */
+  YG_TIMEOUT = 7           /* a bounded device-side wait gave up */
+} yg_status;
+
+enum { YG_BC_PERIODIC = 0, YG_BC_ANTIPERIODIC = 1, YG_BC_OPEN = 2, YG_BC_SF = 3 };
+enum { YG_REPR_FUNDAMENTAL = 0, YG_REPR_ADJOINT = 1, YG_REPR_SYMMETRIC = 2, YG_REPR_ANTISYMMETRIC = 3 };
+enum { YG_VIEW_DEFAULT = 0, YG_VIEW_EVEN = 1, YG_VIEW_ODD = 2, YG_VIEW_FULL = 3 };
+enum { YG_OP_DPHI = 0, YG_OP_HPHI = 1, YG_OP_HPHI_SQ = 2 };
+
+typedef struct yg_lattice yg_lattice;
+
+/* Compile-time physics switches of the reference (programs/Makefile:6-45)
+ * become run-time parameters: NC, REPR_*, BC_*, CLOVER_TERM, UPDATE_EO. */
+typedef struct {
+  int dims[4];   /* T, X, Y, Z: even, >= 2 (the reference itself needs >= 8, geometry.cpp:1140) */
+  int nc;        /* N of SU(N): 2, 3 or 4 */
+  int repr;      /* YG_REPR_*, the REPR_ID of include/repr.h:9-39 */
+  int bc;        /* YG_BC_* (include/bcs.h:1-31) */
+  int clover;    /* CLOVER_TERM */
+  int eo;        /* UPDATE_EO */
+  double csw;    /* clover coefficient (clover_init, clover.cpp:349-361) */
+  double cf;     /* Dirac boundary coefficient for open / SF (bcs_init, bcs.cpp:68, 131) */
+} yg_params;
+
+typedef struct {
+  long volume;         /* V (outer.vol4 on one rank) */
+  long half_volume;    /* V/2 */
+  int repr_dim;        /* d = REPR_DIM */
+  int nc;
+  int ng;              /* NC*NC-1 */
+  long field_doubles;  /* doubles per spinor field = 8*d*V */
+  long link_doubles;   /* doubles of the represented links = 4*V*2*d*d */
+  long fund_doubles;   /* doubles of the fundamental links = 4*V*2*N*N */
+  long mom_doubles;    /* doubles of the momenta = 4*V*NG */
+} yg_info;
+
+typedef struct {
+  int op;              /* YG_OP_*: the mvm of inv_par (inverter.h:6-16) */
+  double mass;         /* inv_par.mass */
+  double prec;         /* inv_par.prec: squared relative residual */
+  int log;             /* inv_par.log: print one line per solve to stderr */
+  int maxiter;         /* 0 = unlimited, as the reference */
+} yg_inv_par;
+
+typedef struct {
+  int iterations;      /* inner (operator-level) iterations */
+  int reliable_updates;
+  int fallback;        /* 1 if the solver fell back to plain FP64 CG */
+  double true_residual;/* |b - A x|^2 / |b|^2 recomputed in FP64 at exit */
+  double seconds;
+} yg_solve_stats;
+
+/* ---- lifecycle --------------------------------------------------------- */
+/* replaces geometry_init + repr_init + bcs_init + clover_init + gauge_field_init
+ * (programs/hmc.cpp:94-117; geometry.cpp:1032-1191, repr.cpp:17-105,
+ * bcs.cpp:11-137, clover.cpp:349-361, gaugefield.cpp:15-30) */
+int yg_lattice_create(const yg_params *p, yg_lattice **out);
+void yg_lattice_destroy(yg_lattice *lat);
+int yg_lattice_query(const yg_lattice *lat, yg_info *out);
+int yg_set_stream(yg_lattice *lat, void *cuda_stream);
+int yg_synchronize(yg_lattice *lat);
+const char *yg_last_error(void);
+
+/* ---- spinor fields (SpinorField, spinorfield.h:6-39; spinor_allocate linalg.cpp:10-27) */
+int yg_field_alloc(yg_lattice *lat, double **dev_field);
+int yg_field_free(yg_lattice *lat, double *dev_field);
+int yg_field_upload(yg_lattice *lat, double *dev_field, const double *host_spinors);
+int yg_field_download(yg_lattice *lat, double *host_spinors, const double *dev_field);
+
+/* ---- gauge field ------------------------------------------------------- */
+/* gfield_fund upload + represent_gauge_field (repr.cpp:265-280): represent links
+ * (repr.cpp:107-263), rebuild the clover term (clover.cpp:330-347) and apply the
+ * antiperiodic sign (bcs.cpp:264-272).  host: 4*V suNg records, index 4*id+mu. */
+int yg_gauge_upload(yg_lattice *lat, const double *host_fund_links);
+int yg_gauge_download(yg_lattice *lat, double *host_fund_links);
+/* gfield_repr (4*V suNf records), cl_term (4*V suNf), cl_ldl for sigma=4+mass (V ldl_t) */
+int yg_repr_links_download(yg_lattice *lat, double *host);
+int yg_clover_term_download(yg_lattice *lat, double *host);
+int yg_ldl_download(yg_lattice *lat, double mass, double *host);
+
+/* ---- Dirac operator (dirac.h:6-16, dirac.cpp:706-781) ------------------ */
+int yg_Dphi_oe(yg_lattice *lat, double *dst, double *src);
+int yg_Dphi_eo(yg_lattice *lat, double *dst, double *src);
+int yg_Dphi_ee(yg_lattice *lat, double mass, double *dst, double *src);
+int yg_Dphi_oo(yg_lattice *lat, double mass, double *dst, double *src);
+int yg_Dphi_oo_inv(yg_lattice *lat, double mass, double *dst, double *src);
+/* Dphi writes scratch into the odd half of src, like the reference (dirac.cpp:743). */
+int yg_Dphi(yg_lattice *lat, double mass, double *dst, double *src);
+int yg_Hphi(yg_lattice *lat, double mass, double *dst, double *src);
+int yg_Hphi_sq(yg_lattice *lat, double mass, double *dst, double *src);
+int yg_mvm_get(yg_lattice *lat);                       /* dirac.cpp:11-18 */
+void yg_mvm_reset(yg_lattice *lat);                    /* dirac.cpp:20-23 */
+
+/* ---- clover (clover.h:39-44) ------------------------------------------- */
+int yg_clover_logdet(yg_lattice *lat, double mass, double *out);   /* clover.cpp:281-305 */
+
+/* ---- spinor linear algebra (linalg.h:7-34, linalg.cpp:29-270) ---------- */
+int yg_spinor_zero(yg_lattice *lat, double *f);
+int yg_spinor_copy(yg_lattice *lat, double *dst, const double *src);
+int yg_spinor_g5(yg_lattice *lat, double *f, int view);
+int yg_spinor_sqnorm(yg_lattice *lat, const double *f, int view, double *out);
+int yg_spinor_product(yg_lattice *lat, const double *a, const double *b, int view, double *out_re_im);
+int yg_spinor_product_re(yg_lattice *lat, const double *a, const double *b, int view, double *out);
+int yg_spinor_add_assign(yg_lattice *lat, double *lhs, const double *rhs, int view);
+int yg_spinor_sub_assign(yg_lattice *lat, double *lhs, const double *rhs, int view);
+int yg_spinor_mulr(yg_lattice *lat, double *lhs, double v, const double *rhs, int view);
+int yg_spinor_mulc(yg_lattice *lat, double *lhs, double re, double im, const double *rhs, int view);
+int yg_spinor_mulr_assign(yg_lattice *lat, double *lhs, double v, int view);
+int yg_spinor_mulc_assign(yg_lattice *lat, double *lhs, double re, double im, int view);
+int yg_spinor_mulr_add_assign(yg_lattice *lat, double *lhs, double v, const double *rhs, int view);
+int yg_spinor_mulc_add_assign(yg_lattice *lat, double *lhs, double re, double im, const double *rhs, int view);
+int yg_spinor_mulr_sub_assign(yg_lattice *lat, double *lhs, double v, const double *rhs, int view);
+int yg_spinor_mulc_sub_assign(yg_lattice *lat, double *lhs, double re, double im, const double *rhs, int view);
+
+/* ---- inverters (inverter.h:18-22); iterations returned through *iters --- */
+int yg_cg_inverter(yg_lattice *lat, const yg_inv_par *par, double *x, double *b, int *iters);        /* cg.cpp:132-202 */
+int yg_bicgstab_inverter(yg_lattice *lat, const yg_inv_par *par, double *x, double *b, int *iters);  /* bicgstab.cpp:9-97 */
+int yg_minres_inverter(yg_lattice *lat, const yg_inv_par *par, double *x, double *b, int *iters);    /* minres.cpp:12-117 */
+int yg_auto_inverter(yg_lattice *lat, const yg_inv_par *par, double *x, double *b, int *iters);      /* inverter.cpp:9-55 */
+/* cg.cpp:11-130; xs: num device fields; x_n solves (A + shifts[n]) x_n = b from a zero guess */
+int yg_cg_mshift(yg_lattice *lat, const yg_inv_par *par, int num, const double *shifts,
+                 double *const *xs, double *b, int *iters);
+/* rational.cpp:134-166: x = a0*b + sum_i residues[i] * (A + poles[i])^-1 b */
+int yg_rational_calc(yg_lattice *lat, const yg_inv_par *par, double a0, int order, const double *poles,
+                     const double *residues, double *x, double *b, int *iters);
+/* No reference counterpart: CG on the same operator with FP32 inner iterations and FP64
+ * reliable updates; stops on the TRUE FP64 squared residual |b-Ax|^2 < prec*|b|^2. */
+int yg_cg_mixed(yg_lattice *lat, const yg_inv_par *par, double *x, double *b, yg_solve_stats *stats);
+
+/* ---- forces (forces.h:6-15) -------------------------------------------- */
+int yg_momenta_upload(yg_lattice *lat, const double *host);     /* afield_momenta, 4*V suNa */
+int yg_momenta_download(yg_lattice *lat, double *host);
+int yg_momenta_zero(yg_lattice *lat);
+int yg_clover_force_download(yg_lattice *lat, double *host);    /* cl_force, 6*V suNf */
+int yg_begin_fermion_force(yg_lattice *lat);                                                        /* forces.cpp:239-251 */
+int yg_end_fermion_force(yg_lattice *lat, double dt);                                               /* forces.cpp:254-259 */
+int yg_wilson_fermion_force(yg_lattice *lat, double dt, double mass, double residue, double *lhs, double *rhs); /* forces.cpp:175-227 */
+int yg_wilson_fermion_force_q(yg_lattice *lat, double dt, double mass, double residue, double *rhs);            /* forces.cpp:230-236 */
+int yg_clover_fermion_force(yg_lattice *lat, double residue, double *lhs, double *rhs);             /* forces.cpp:122-172 */
+int yg_clover_logdet_force(yg_lattice *lat, double mass, double residue);                           /* forces.cpp:109-119 */
+int yg_wilson_gauge_force(yg_lattice *lat, double dt, double beta);                                 /* forces.cpp:262-283 */
+int yg_avr_plaquette(yg_lattice *lat, double *out);                                                 /* wilsonloop.cpp:116-133 (1x1) */
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,386 @@
+"""yahmc_b200 -- B200 (sm_100a) engine for YaHMC's fermion hot path.
+
+Python mirror of the reference's C++ call surface (dirac.h, inverter.h, linalg.h,
+clover.h, forces.h) over the C ABI of include/yahmc_gpu.h, which is implemented by
+the in-tree library yahmc_b200/_lib/libyahmc_b200.so (build it with
+``python -m yahmc_b200.build``).  There is no CPU fallback: importing works
+anywhere, but creating a Lattice needs the library and a CUDA device and raises
+otherwise.
+
+Host arrays use the reference's own layouts as complex numpy arrays:
+  spinor field  (V, d, 4)       Spinor{re[d][4], im[d][4]}
+  fund links    (V, 4, N, N)    gfield_fund[4*id+mu]
+  repr links    (V, 4, d, d)    gfield_repr[4*id+mu]
+  momenta       (V, 4, NG)      afield_momenta[4*id+mu]
+with sites in the reference's order (even-odd: id = (parity*V + lex)//2).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+from .fields import complex_to_raw, raw_to_complex
+
+__all__ = ["Lattice", "Field", "YGError", "load_library", "LIB_PATH",
+           "VIEW_DEFAULT", "VIEW_EVEN", "VIEW_ODD", "VIEW_FULL", "OP_DPHI", "OP_HPHI", "OP_HPHI_SQ"]
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libyahmc_b200.so"
+
+VIEW_DEFAULT, VIEW_EVEN, VIEW_ODD, VIEW_FULL = 0, 1, 2, 3
+OP_DPHI, OP_HPHI, OP_HPHI_SQ = 0, 1, 2
+_OPS = {"Dphi": OP_DPHI, "Hphi": OP_HPHI, "Hphi_sq": OP_HPHI_SQ}
+_BC = {"periodic": 0, "antiperiodic": 1, "open": 2, "sf": 3}
+_REPR = {"fundamental": 0, "adjoint": 1, "symmetric": 2, "antisymmetric": 3}
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_OOM", 4: "MAXITER", 5: "STALL", 6: "NONFINITE", 7: "TIMEOUT"}
+
+
+class YGError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("dims", ctypes.c_int * 4), ("nc", ctypes.c_int), ("repr", ctypes.c_int), ("bc", ctypes.c_int),
+                ("clover", ctypes.c_int), ("eo", ctypes.c_int), ("csw", ctypes.c_double), ("cf", ctypes.c_double)]
+
+
+class _Info(ctypes.Structure):
+    _fields_ = [("volume", ctypes.c_long), ("half_volume", ctypes.c_long), ("repr_dim", ctypes.c_int),
+                ("nc", ctypes.c_int), ("ng", ctypes.c_int), ("field_doubles", ctypes.c_long),
+                ("link_doubles", ctypes.c_long), ("fund_doubles", ctypes.c_long), ("mom_doubles", ctypes.c_long)]
+
+
+class InvPar(ctypes.Structure):
+    _fields_ = [("op", ctypes.c_int), ("mass", ctypes.c_double), ("prec", ctypes.c_double), ("log", ctypes.c_int),
+                ("maxiter", ctypes.c_int)]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("reliable_updates", ctypes.c_int), ("fallback", ctypes.c_int),
+                ("true_residual", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+
+_lib = None
+_D = ctypes.c_double
+_I = ctypes.c_int
+_P = ctypes.c_void_p
+
+_SIGNATURES = {
+    "yg_lattice_create": [ctypes.POINTER(_Params), ctypes.POINTER(_P)],
+    "yg_lattice_destroy": [_P], "yg_lattice_query": [_P, ctypes.POINTER(_Info)],
+    "yg_set_stream": [_P, _P], "yg_synchronize": [_P],
+    "yg_field_alloc": [_P, ctypes.POINTER(_P)], "yg_field_free": [_P, _P],
+    "yg_field_upload": [_P, _P, _P], "yg_field_download": [_P, _P, _P],
+    "yg_gauge_upload": [_P, _P], "yg_gauge_download": [_P, _P], "yg_repr_links_download": [_P, _P],
+    "yg_clover_term_download": [_P, _P], "yg_ldl_download": [_P, _D, _P],
+    "yg_Dphi_oe": [_P, _P, _P], "yg_Dphi_eo": [_P, _P, _P], "yg_Dphi_ee": [_P, _D, _P, _P],
+    "yg_Dphi_oo": [_P, _D, _P, _P], "yg_Dphi_oo_inv": [_P, _D, _P, _P], "yg_Dphi": [_P, _D, _P, _P],
+    "yg_Hphi": [_P, _D, _P, _P], "yg_Hphi_sq": [_P, _D, _P, _P], "yg_mvm_get": [_P], "yg_mvm_reset": [_P],
+    "yg_clover_logdet": [_P, _D, _P],
+    "yg_spinor_zero": [_P, _P], "yg_spinor_copy": [_P, _P, _P], "yg_spinor_g5": [_P, _P, _I],
+    "yg_spinor_sqnorm": [_P, _P, _I, _P], "yg_spinor_product": [_P, _P, _P, _I, _P],
+    "yg_spinor_product_re": [_P, _P, _P, _I, _P],
+    "yg_spinor_add_assign": [_P, _P, _P, _I], "yg_spinor_sub_assign": [_P, _P, _P, _I],
+    "yg_spinor_mulr": [_P, _P, _D, _P, _I], "yg_spinor_mulc": [_P, _P, _D, _D, _P, _I],
+    "yg_spinor_mulr_assign": [_P, _P, _D, _I], "yg_spinor_mulc_assign": [_P, _P, _D, _D, _I],
+    "yg_spinor_mulr_add_assign": [_P, _P, _D, _P, _I], "yg_spinor_mulc_add_assign": [_P, _P, _D, _D, _P, _I],
+    "yg_spinor_mulr_sub_assign": [_P, _P, _D, _P, _I], "yg_spinor_mulc_sub_assign": [_P, _P, _D, _D, _P, _I],
+    "yg_cg_inverter": [_P, ctypes.POINTER(InvPar), _P, _P, ctypes.POINTER(_I)],
+    "yg_bicgstab_inverter": [_P, ctypes.POINTER(InvPar), _P, _P, ctypes.POINTER(_I)],
+    "yg_minres_inverter": [_P, ctypes.POINTER(InvPar), _P, _P, ctypes.POINTER(_I)],
+    "yg_auto_inverter": [_P, ctypes.POINTER(InvPar), _P, _P, ctypes.POINTER(_I)],
+    "yg_cg_mshift": [_P, ctypes.POINTER(InvPar), _I, _P, _P, _P, ctypes.POINTER(_I)],
+    "yg_rational_calc": [_P, ctypes.POINTER(InvPar), _D, _I, _P, _P, _P, _P, ctypes.POINTER(_I)],
+    "yg_cg_mixed": [_P, ctypes.POINTER(InvPar), _P, _P, ctypes.POINTER(SolveStats)],
+    "yg_momenta_upload": [_P, _P], "yg_momenta_download": [_P, _P], "yg_momenta_zero": [_P],
+    "yg_clover_force_download": [_P, _P], "yg_begin_fermion_force": [_P], "yg_end_fermion_force": [_P, _D],
+    "yg_wilson_fermion_force": [_P, _D, _D, _D, _P, _P], "yg_wilson_fermion_force_q": [_P, _D, _D, _D, _P],
+    "yg_clover_fermion_force": [_P, _D, _P, _P], "yg_clover_logdet_force": [_P, _D, _D],
+    "yg_wilson_gauge_force": [_P, _D, _D], "yg_avr_plaquette": [_P, _P],
+}
+
+
+def load_library(path: Path | str | None = None):
+    """Load the engine library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path or os.environ.get("YAHMC_B200_LIB", LIB_PATH))
+    if not p.exists():
+        raise RuntimeError(f"{p} not found: build the CUDA library with `python -m yahmc_b200.build`")
+    lib = ctypes.CDLL(str(p))
+    lib.yg_last_error.restype = ctypes.c_char_p
+    for name, args in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = None if name in ("yg_lattice_destroy", "yg_mvm_reset") else ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray):
+    assert a.flags.c_contiguous
+    return a.ctypes.data_as(_P)
+
+
+class Field:
+    """A device spinor field (SpinorField with its storage on the GPU)."""
+
+    def __init__(self, lat: "Lattice"):
+        self.lat = lat
+        p = _P()
+        lat._check(lat.lib.yg_field_alloc(lat.h, ctypes.byref(p)))
+        self.ptr = p.value
+
+    def free(self):
+        if self.ptr and self.lat.h:
+            self.lat.lib.yg_field_free(self.lat.h, self.ptr)
+        self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Lattice:
+    """One lattice with its device gauge field, clover term and momenta.  Method names and
+    argument order follow the reference (dirac.h, inverter.h, linalg.h, forces.h)."""
+
+    def __init__(self, dims, nc=3, repr="fundamental", bc="antiperiodic", clover=True, eo=True,
+                 csw=1.0, cf=1.0, lib=None):
+        self.lib = lib or load_library()
+        p = _Params()
+        for i in range(4):
+            p.dims[i] = int(dims[i])
+        p.nc, p.repr, p.bc = int(nc), _REPR[repr], _BC[bc]
+        p.clover, p.eo, p.csw, p.cf = int(bool(clover)), int(bool(eo)), float(csw), float(cf)
+        h = _P()
+        self.h = None
+        self._check(self.lib.yg_lattice_create(ctypes.byref(p), ctypes.byref(h)))
+        self.h = h.value
+        info = _Info()
+        self._check(self.lib.yg_lattice_query(self.h, ctypes.byref(info)))
+        self.dims = tuple(int(x) for x in dims)
+        self.V, self.Vh, self.d, self.nc, self.ng = info.volume, info.half_volume, info.repr_dim, info.nc, info.ng
+        self.field_doubles = info.field_doubles
+        self.eo, self.clover, self.bc, self.repr = bool(eo), bool(clover), bc, repr
+        self.last_status = 0
+
+    # ---- plumbing
+    def _check(self, rc):
+        if rc != 0:
+            raise YGError(rc, self.lib.yg_last_error().decode())
+        return rc
+
+    def close(self):
+        if self.h:
+            self.lib.yg_lattice_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def synchronize(self):
+        self._check(self.lib.yg_synchronize(self.h))
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self.lib.yg_set_stream(self.h, stream_ptr))
+
+    # ---- fields
+    def field(self, host=None) -> Field:
+        f = Field(self)
+        if host is not None:
+            self.upload(f, host)
+        return f
+
+    def upload(self, f: Field, host):
+        host = np.asarray(host)
+        raw = host if (host.dtype == np.float64 and host.ndim == 1) else complex_to_raw(host)
+        raw = np.ascontiguousarray(raw, dtype=np.float64)
+        assert raw.size == self.field_doubles
+        self._check(self.lib.yg_field_upload(self.h, f.ptr, _ptr(raw)))
+
+    def download(self, f: Field, raw=False):
+        out = np.empty(self.field_doubles)
+        self._check(self.lib.yg_field_download(self.h, _ptr(out), f.ptr))
+        return out if raw else raw_to_complex(out, self.d, 4)
+
+    # ---- gauge field (represent_gauge_field, repr.cpp:265-280)
+    def set_links(self, fund):
+        fund = np.asarray(fund)
+        raw = np.ascontiguousarray(complex_to_raw(fund) if np.iscomplexobj(fund) else fund, dtype=np.float64)
+        self._check(self.lib.yg_gauge_upload(self.h, _ptr(raw)))
+
+    def get_links(self):
+        out = np.empty(self.V * 4 * 2 * self.nc * self.nc)
+        self._check(self.lib.yg_gauge_download(self.h, _ptr(out)))
+        return raw_to_complex(out, self.nc, self.nc).reshape(self.V, 4, self.nc, self.nc)
+
+    def repr_links(self):
+        out = np.empty(self.V * 4 * 2 * self.d * self.d)
+        self._check(self.lib.yg_repr_links_download(self.h, _ptr(out)))
+        return raw_to_complex(out, self.d, self.d).reshape(self.V, 4, self.d, self.d)
+
+    def clover_term(self):
+        out = np.empty(self.V * 4 * 2 * self.d * self.d)
+        self._check(self.lib.yg_clover_term_download(self.h, _ptr(out)))
+        return raw_to_complex(out, self.d, self.d).reshape(self.V, 4, self.d, self.d)
+
+    def ldl(self, mass):
+        P = self.d * (2 * self.d + 1)
+        out = np.empty(self.V * 2 * P * 2)
+        self._check(self.lib.yg_ldl_download(self.h, mass, _ptr(out)))
+        r = out.reshape(self.V, 2, P, 2)
+        return r[..., 0] + 1j * r[..., 1]
+
+    # ---- dirac.h
+    def Dphi_oe(self, dst, src): self._check(self.lib.yg_Dphi_oe(self.h, dst.ptr, src.ptr))
+    def Dphi_eo(self, dst, src): self._check(self.lib.yg_Dphi_eo(self.h, dst.ptr, src.ptr))
+    def Dphi_ee(self, m, dst, src): self._check(self.lib.yg_Dphi_ee(self.h, m, dst.ptr, src.ptr))
+    def Dphi_oo(self, m, dst, src): self._check(self.lib.yg_Dphi_oo(self.h, m, dst.ptr, src.ptr))
+    def Dphi_oo_inv(self, m, dst, src): self._check(self.lib.yg_Dphi_oo_inv(self.h, m, dst.ptr, src.ptr))
+    def Dphi(self, m, dst, src): self._check(self.lib.yg_Dphi(self.h, m, dst.ptr, src.ptr))
+    def Hphi(self, m, dst, src): self._check(self.lib.yg_Hphi(self.h, m, dst.ptr, src.ptr))
+    def Hphi_sq(self, m, dst, src): self._check(self.lib.yg_Hphi_sq(self.h, m, dst.ptr, src.ptr))
+    def mvm_get(self): return self.lib.yg_mvm_get(self.h)
+    def mvm_reset(self): self.lib.yg_mvm_reset(self.h)
+
+    def clover_logdet(self, mass):
+        out = ctypes.c_double()
+        self._check(self.lib.yg_clover_logdet(self.h, mass, ctypes.byref(out)))
+        return out.value
+
+    # ---- linalg.h
+    def spinor_zero(self, f): self._check(self.lib.yg_spinor_zero(self.h, f.ptr))
+    def spinor_copy(self, dst, src): self._check(self.lib.yg_spinor_copy(self.h, dst.ptr, src.ptr))
+    def spinor_g5(self, f, view=VIEW_DEFAULT): self._check(self.lib.yg_spinor_g5(self.h, f.ptr, view))
+
+    def spinor_sqnorm(self, f, view=VIEW_DEFAULT):
+        out = ctypes.c_double()
+        self._check(self.lib.yg_spinor_sqnorm(self.h, f.ptr, view, ctypes.byref(out)))
+        return out.value
+
+    def spinor_product(self, a, b, view=VIEW_DEFAULT):
+        out = (ctypes.c_double * 2)()
+        self._check(self.lib.yg_spinor_product(self.h, a.ptr, b.ptr, view, out))
+        return complex(out[0], out[1])
+
+    def spinor_product_re(self, a, b, view=VIEW_DEFAULT):
+        out = ctypes.c_double()
+        self._check(self.lib.yg_spinor_product_re(self.h, a.ptr, b.ptr, view, ctypes.byref(out)))
+        return out.value
+
+    def spinor_add_assign(self, a, b, view=VIEW_DEFAULT): self._check(self.lib.yg_spinor_add_assign(self.h, a.ptr, b.ptr, view))
+    def spinor_sub_assign(self, a, b, view=VIEW_DEFAULT): self._check(self.lib.yg_spinor_sub_assign(self.h, a.ptr, b.ptr, view))
+    def spinor_mulr(self, a, v, b, view=VIEW_DEFAULT): self._check(self.lib.yg_spinor_mulr(self.h, a.ptr, v, b.ptr, view))
+    def spinor_mulc(self, a, c, b, view=VIEW_DEFAULT): self._check(self.lib.yg_spinor_mulc(self.h, a.ptr, c.real, c.imag, b.ptr, view))
+    def spinor_mulr_assign(self, a, v, view=VIEW_DEFAULT): self._check(self.lib.yg_spinor_mulr_assign(self.h, a.ptr, v, view))
+    def spinor_mulc_assign(self, a, c, view=VIEW_DEFAULT): self._check(self.lib.yg_spinor_mulc_assign(self.h, a.ptr, c.real, c.imag, view))
+    def spinor_mulr_add_assign(self, a, v, b, view=VIEW_DEFAULT): self._check(self.lib.yg_spinor_mulr_add_assign(self.h, a.ptr, v, b.ptr, view))
+    def spinor_mulc_add_assign(self, a, c, b, view=VIEW_DEFAULT): self._check(self.lib.yg_spinor_mulc_add_assign(self.h, a.ptr, c.real, c.imag, b.ptr, view))
+    def spinor_mulr_sub_assign(self, a, v, b, view=VIEW_DEFAULT): self._check(self.lib.yg_spinor_mulr_sub_assign(self.h, a.ptr, v, b.ptr, view))
+    def spinor_mulc_sub_assign(self, a, c, b, view=VIEW_DEFAULT): self._check(self.lib.yg_spinor_mulc_sub_assign(self.h, a.ptr, c.real, c.imag, b.ptr, view))
+
+    # ---- inverter.h
+    @staticmethod
+    def _par(op, mass, prec, log=0, maxiter=0):
+        return InvPar(_OPS[op] if isinstance(op, str) else int(op), float(mass), float(prec), int(log), int(maxiter))
+
+    def _solve(self, fn, op, mass, prec, x, b, log, maxiter, allow=(0, 4)):
+        it = ctypes.c_int()
+        par = self._par(op, mass, prec, log, maxiter)
+        rc = fn(self.h, ctypes.byref(par), x.ptr, b.ptr, ctypes.byref(it))
+        if rc not in allow:
+            self._check(rc)
+        self.last_status = rc
+        return it.value
+
+    def cg_inverter(self, op, mass, prec, x, b, log=0, maxiter=0):
+        return self._solve(self.lib.yg_cg_inverter, op, mass, prec, x, b, log, maxiter)
+
+    def bicgstab_inverter(self, op, mass, prec, x, b, log=0, maxiter=0):
+        return self._solve(self.lib.yg_bicgstab_inverter, op, mass, prec, x, b, log, maxiter)
+
+    def minres_inverter(self, op, mass, prec, x, b, log=0, maxiter=0):
+        return self._solve(self.lib.yg_minres_inverter, op, mass, prec, x, b, log, maxiter)
+
+    def auto_inverter(self, op, mass, prec, x, b, log=0, maxiter=0):
+        return self._solve(self.lib.yg_auto_inverter, op, mass, prec, x, b, log, maxiter)
+
+    def cg_mshift(self, op, mass, prec, shifts, xs, b, log=0, maxiter=0):
+        it = ctypes.c_int()
+        par = self._par(op, mass, prec, log, maxiter)
+        sh = np.ascontiguousarray(shifts, dtype=np.float64)
+        ptrs = (_P * len(xs))(*[x.ptr for x in xs])
+        rc = self.lib.yg_cg_mshift(self.h, ctypes.byref(par), len(xs), _ptr(sh), ptrs, b.ptr, ctypes.byref(it))
+        if rc not in (0, 4):
+            self._check(rc)
+        self.last_status = rc
+        return it.value
+
+    def rational_calc(self, op, mass, prec, a0, poles, residues, x, b, log=0):
+        it = ctypes.c_int()
+        par = self._par(op, mass, prec, log, 0)
+        po = np.ascontiguousarray(poles, dtype=np.float64)
+        re = np.ascontiguousarray(residues, dtype=np.float64)
+        self._check(self.lib.yg_rational_calc(self.h, ctypes.byref(par), a0, len(po), _ptr(po), _ptr(re),
+                                              x.ptr, b.ptr, ctypes.byref(it)))
+        return it.value
+
+    def cg_mixed(self, op, mass, prec, x, b, log=0, maxiter=0):
+        st = SolveStats()
+        par = self._par(op, mass, prec, log, maxiter)
+        rc = self.lib.yg_cg_mixed(self.h, ctypes.byref(par), x.ptr, b.ptr, ctypes.byref(st))
+        if rc not in (0, 4, 5):
+            self._check(rc)
+        return {"status": rc, "iterations": st.iterations, "reliable_updates": st.reliable_updates,
+                "fallback": st.fallback, "true_residual": st.true_residual, "seconds": st.seconds}
+
+    # ---- forces.h
+    def momenta(self):
+        out = np.empty(self.V * 4 * self.ng)
+        self._check(self.lib.yg_momenta_download(self.h, _ptr(out)))
+        return out.reshape(self.V, 4, self.ng)
+
+    def set_momenta(self, mom):
+        raw = np.ascontiguousarray(mom, dtype=np.float64).reshape(-1)
+        self._check(self.lib.yg_momenta_upload(self.h, _ptr(raw)))
+
+    def zero_momenta(self): self._check(self.lib.yg_momenta_zero(self.h))
+
+    def clover_force(self):
+        out = np.empty(self.V * 6 * 2 * self.d * self.d)
+        self._check(self.lib.yg_clover_force_download(self.h, _ptr(out)))
+        return raw_to_complex(out, self.d, self.d).reshape(self.V, 6, self.d, self.d)
+
+    def begin_fermion_force(self): self._check(self.lib.yg_begin_fermion_force(self.h))
+    def end_fermion_force(self, dt): self._check(self.lib.yg_end_fermion_force(self.h, dt))
+
+    def wilson_fermion_force(self, dt, mass, residue, lhs, rhs):
+        self._check(self.lib.yg_wilson_fermion_force(self.h, dt, mass, residue, lhs.ptr, rhs.ptr))
+
+    def wilson_fermion_force_q(self, dt, mass, residue, rhs):
+        self._check(self.lib.yg_wilson_fermion_force_q(self.h, dt, mass, residue, rhs.ptr))
+
+    def clover_fermion_force(self, residue, lhs, rhs):
+        self._check(self.lib.yg_clover_fermion_force(self.h, residue, lhs.ptr, rhs.ptr))
+
+    def clover_logdet_force(self, mass, residue):
+        self._check(self.lib.yg_clover_logdet_force(self.h, mass, residue))
+
+    def wilson_gauge_force(self, dt, beta):
+        self._check(self.lib.yg_wilson_gauge_force(self.h, dt, beta))
+
+    def plaquette(self):
+        out = ctypes.c_double()
+        self._check(self.lib.yg_avr_plaquette(self.h, ctypes.byref(out)))
+        return out.value

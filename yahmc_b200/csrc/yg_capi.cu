@@ -1,0 +1,261 @@
+// extern "C" entry points of include/yahmc_gpu.h: argument checks, exception-to-status
+// conversion, and the thin mapping onto the engine functions.
+#include <cstdio>
+#include <string>
+#include "yg_lattice.h"
+
+using yg::Error;
+using yg::Lattice;
+
+static thread_local std::string g_last_error;
+
+template <typename F>
+static int guard(F &&f) {
+  try {
+    f();
+    return YG_OK;
+  } catch (const Error &e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::exception &e) {
+    g_last_error = e.what();
+    return YG_ERR_ARG;
+  }
+}
+
+template <typename F>
+static int guard_status(F &&f) {
+  try {
+    return f();
+  } catch (const Error &e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::exception &e) {
+    g_last_error = e.what();
+    return YG_ERR_ARG;
+  }
+}
+
+static Lattice &lat(yg_lattice *l) {
+  if (!l) throw Error(YG_ERR_ARG, "null lattice handle");
+  return *reinterpret_cast<Lattice *>(l);
+}
+
+static void need(const void *p, const char *what) {
+  if (!p) throw Error(YG_ERR_ARG, std::string("null pointer: ") + what);
+}
+
+static void range(Lattice &L, int view, long &lo, long &n) { L.view_range(view, lo, n); }
+
+static void need_clover(Lattice &L) {
+  if (!L.p.clover) throw Error(YG_ERR_ARG, "this operator needs the clover term (CLOVER_TERM)");
+}
+
+extern "C" {
+
+const char *yg_last_error(void) { return g_last_error.c_str(); }
+
+int yg_lattice_create(const yg_params *p, yg_lattice **out) {
+  return guard([&] {
+    need(p, "params");
+    need(out, "out");
+    *out = reinterpret_cast<yg_lattice *>(yg::lattice_create(*p));
+  });
+}
+
+void yg_lattice_destroy(yg_lattice *l) { delete reinterpret_cast<Lattice *>(l); }
+
+int yg_lattice_query(const yg_lattice *l, yg_info *out) {
+  return guard([&] {
+    need(out, "out");
+    const Lattice &L = lat(const_cast<yg_lattice *>(l));
+    out->volume = L.V;
+    out->half_volume = L.Vh;
+    out->repr_dim = L.d;
+    out->nc = L.nc;
+    out->ng = L.ng;
+    out->field_doubles = L.field_doubles();
+    out->link_doubles = 4L * L.V * 2 * L.d * L.d;
+    out->fund_doubles = 4L * L.V * 2 * L.nc * L.nc;
+    out->mom_doubles = 4L * L.V * L.ng;
+  });
+}
+
+int yg_set_stream(yg_lattice *l, void *s) {
+  return guard([&] { lat(l).stream = reinterpret_cast<cudaStream_t>(s); });
+}
+
+int yg_synchronize(yg_lattice *l) {
+  return guard([&] { YG_CUDA(cudaStreamSynchronize(lat(l).stream)); });
+}
+
+int yg_field_alloc(yg_lattice *l, double **f) {
+  return guard([&] {
+    need(f, "out");
+    Lattice &L = lat(l);
+    YG_CUDA(cudaMalloc(f, L.field_bytes()));
+    YG_CUDA(cudaMemsetAsync(*f, 0, L.field_bytes(), L.stream));
+  });
+}
+
+int yg_field_free(yg_lattice *l, double *f) {
+  return guard([&] {
+    lat(l);
+    if (f) YG_CUDA(cudaFree(f));
+  });
+}
+
+int yg_field_upload(yg_lattice *l, double *dev, const double *host) {
+  return guard([&] { need(dev, "dev"); need(host, "host"); yg::field_upload(lat(l), dev, host); });
+}
+
+int yg_field_download(yg_lattice *l, double *host, const double *dev) {
+  return guard([&] { need(dev, "dev"); need(host, "host"); yg::field_download(lat(l), host, dev); });
+}
+
+int yg_gauge_upload(yg_lattice *l, const double *h) { return guard([&] { need(h, "host"); yg::gauge_upload(lat(l), h); }); }
+int yg_gauge_download(yg_lattice *l, double *h) { return guard([&] { need(h, "host"); yg::gauge_download(lat(l), h); }); }
+int yg_repr_links_download(yg_lattice *l, double *h) { return guard([&] { need(h, "host"); yg::repr_download(lat(l), h); }); }
+int yg_clover_term_download(yg_lattice *l, double *h) { return guard([&] { need(h, "host"); yg::clover_download(lat(l), h); }); }
+int yg_ldl_download(yg_lattice *l, double m, double *h) { return guard([&] { need(h, "host"); yg::ldl_download(lat(l), m, h); }); }
+
+int yg_Dphi_oe(yg_lattice *l, double *dst, double *src) {
+  return guard([&] { need(dst, "dst"); need(src, "src"); yg::hop(lat(l), dst, src, 2, 1.0, false); });
+}
+int yg_Dphi_eo(yg_lattice *l, double *dst, double *src) {
+  return guard([&] { need(dst, "dst"); need(src, "src"); yg::hop(lat(l), dst, src, 1, 1.0, false); });
+}
+int yg_Dphi_ee(yg_lattice *l, double m, double *dst, double *src) {
+  return guard([&] { Lattice &L = lat(l); need_clover(L); need(dst, "dst"); need(src, "src"); yg::clover_apply(L, m, dst, src, 1, false); });
+}
+int yg_Dphi_oo(yg_lattice *l, double m, double *dst, double *src) {
+  return guard([&] { Lattice &L = lat(l); need_clover(L); need(dst, "dst"); need(src, "src"); yg::clover_apply(L, m, dst, src, 2, false); });
+}
+int yg_Dphi_oo_inv(yg_lattice *l, double m, double *dst, double *src) {
+  return guard([&] { Lattice &L = lat(l); need_clover(L); need(dst, "dst"); need(src, "src"); yg::clover_inv_apply(L, m, dst, src, 2, false); });
+}
+int yg_Dphi(yg_lattice *l, double m, double *dst, double *src) {
+  return guard([&] { need(dst, "dst"); need(src, "src"); yg::dphi(lat(l), m, dst, src); });
+}
+int yg_Hphi(yg_lattice *l, double m, double *dst, double *src) {
+  return guard([&] { need(dst, "dst"); need(src, "src"); yg::hphi(lat(l), m, dst, src); });
+}
+int yg_Hphi_sq(yg_lattice *l, double m, double *dst, double *src) {
+  return guard([&] { need(dst, "dst"); need(src, "src"); yg::hphi_sq(lat(l), m, dst, src); });
+}
+int yg_mvm_get(yg_lattice *l) {
+  if (!l) return -1;
+  Lattice &L = lat(l);
+  return L.p.eo ? (L.mvm >> 1) : L.mvm;    // dirac.cpp:11-18
+}
+void yg_mvm_reset(yg_lattice *l) {
+  if (l) lat(l).mvm = 0;
+}
+
+int yg_clover_logdet(yg_lattice *l, double m, double *out) {
+  return guard([&] { need(out, "out"); *out = yg::clover_logdet(lat(l), m); });
+}
+
+// ---- linalg
+int yg_spinor_zero(yg_lattice *l, double *f) {
+  return guard([&] { Lattice &L = lat(l); need(f, "f"); yg::blas_zero(L, f, 0, L.V); });
+}
+int yg_spinor_copy(yg_lattice *l, double *dst, const double *src) {
+  return guard([&] { need(dst, "dst"); need(src, "src"); yg::blas_copy(lat(l), dst, src); });
+}
+int yg_spinor_g5(yg_lattice *l, double *f, int view) {
+  return guard([&] { Lattice &L = lat(l); need(f, "f"); long lo, n; range(L, view, lo, n); yg::blas_g5(L, f, lo, n); });
+}
+int yg_spinor_sqnorm(yg_lattice *l, const double *f, int view, double *out) {
+  return guard([&] { Lattice &L = lat(l); need(f, "f"); need(out, "out"); long lo, n; range(L, view, lo, n); *out = yg::blas_sqnorm(L, f, lo, n); });
+}
+int yg_spinor_product(yg_lattice *l, const double *a, const double *b, int view, double *out) {
+  return guard([&] {
+    Lattice &L = lat(l); need(a, "a"); need(b, "b"); need(out, "out");
+    long lo, n; range(L, view, lo, n);
+    double2 v = yg::blas_product(L, a, b, lo, n);
+    out[0] = v.x; out[1] = v.y;
+  });
+}
+int yg_spinor_product_re(yg_lattice *l, const double *a, const double *b, int view, double *out) {
+  return guard([&] { Lattice &L = lat(l); need(a, "a"); need(b, "b"); need(out, "out"); long lo, n; range(L, view, lo, n); *out = yg::blas_product_re(L, a, b, lo, n); });
+}
+
+static int axpby(yg_lattice *l, double *lhs, double2 al, double2 be, const double *rhs, int view, bool need_rhs) {
+  return guard([&] {
+    Lattice &L = lat(l); need(lhs, "lhs");
+    if (need_rhs) need(rhs, "rhs");
+    long lo, n; range(L, view, lo, n);
+    yg::blas_axpby(L, lhs, al, be, rhs, lo, n);
+  });
+}
+int yg_spinor_add_assign(yg_lattice *l, double *a, const double *b, int v) { return axpby(l, a, make_double2(1, 0), make_double2(1, 0), b, v, true); }
+int yg_spinor_sub_assign(yg_lattice *l, double *a, const double *b, int v) { return axpby(l, a, make_double2(1, 0), make_double2(-1, 0), b, v, true); }
+int yg_spinor_mulr(yg_lattice *l, double *a, double s, const double *b, int v) { return axpby(l, a, make_double2(0, 0), make_double2(s, 0), b, v, true); }
+int yg_spinor_mulc(yg_lattice *l, double *a, double re, double im, const double *b, int v) { return axpby(l, a, make_double2(0, 0), make_double2(re, im), b, v, true); }
+int yg_spinor_mulr_assign(yg_lattice *l, double *a, double s, int v) { return axpby(l, a, make_double2(s, 0), make_double2(0, 0), nullptr, v, false); }
+int yg_spinor_mulc_assign(yg_lattice *l, double *a, double re, double im, int v) { return axpby(l, a, make_double2(re, im), make_double2(0, 0), nullptr, v, false); }
+int yg_spinor_mulr_add_assign(yg_lattice *l, double *a, double s, const double *b, int v) { return axpby(l, a, make_double2(1, 0), make_double2(s, 0), b, v, true); }
+int yg_spinor_mulc_add_assign(yg_lattice *l, double *a, double re, double im, const double *b, int v) { return axpby(l, a, make_double2(1, 0), make_double2(re, im), b, v, true); }
+int yg_spinor_mulr_sub_assign(yg_lattice *l, double *a, double s, const double *b, int v) { return axpby(l, a, make_double2(1, 0), make_double2(-s, 0), b, v, true); }
+int yg_spinor_mulc_sub_assign(yg_lattice *l, double *a, double re, double im, const double *b, int v) { return axpby(l, a, make_double2(1, 0), make_double2(-re, -im), b, v, true); }
+
+// ---- inverters
+static void check_par(const yg_inv_par *p) {
+  need(p, "par");
+  if (p->op < 0 || p->op > 2) throw Error(YG_ERR_ARG, "invalid operator id");
+}
+
+int yg_cg_inverter(yg_lattice *l, const yg_inv_par *p, double *x, double *b, int *it) {
+  return guard_status([&] { check_par(p); need(x, "x"); need(b, "b"); need(it, "iters"); return yg::cg(lat(l), *p, x, b, it); });
+}
+int yg_bicgstab_inverter(yg_lattice *l, const yg_inv_par *p, double *x, double *b, int *it) {
+  return guard_status([&] { check_par(p); need(x, "x"); need(b, "b"); need(it, "iters"); return yg::bicgstab(lat(l), *p, x, b, it); });
+}
+int yg_minres_inverter(yg_lattice *l, const yg_inv_par *p, double *x, double *b, int *it) {
+  return guard_status([&] { check_par(p); need(x, "x"); need(b, "b"); need(it, "iters"); return yg::minres(lat(l), *p, x, b, it); });
+}
+int yg_auto_inverter(yg_lattice *l, const yg_inv_par *p, double *x, double *b, int *it) {
+  return guard_status([&] { check_par(p); need(x, "x"); need(b, "b"); need(it, "iters"); return yg::auto_inverter(lat(l), *p, x, b, it); });
+}
+int yg_cg_mshift(yg_lattice *l, const yg_inv_par *p, int num, const double *shifts, double *const *xs, double *b, int *it) {
+  return guard_status([&] {
+    check_par(p); need(shifts, "shifts"); need(xs, "xs"); need(b, "b"); need(it, "iters");
+    for (int i = 0; i < num; i++) need(xs[i], "xs[i]");
+    return yg::cg_mshift(lat(l), *p, num, shifts, xs, b, it);
+  });
+}
+int yg_rational_calc(yg_lattice *l, const yg_inv_par *p, double a0, int order, const double *poles,
+                     const double *residues, double *x, double *b, int *it) {
+  return guard_status([&] {
+    check_par(p); need(poles, "poles"); need(residues, "residues"); need(x, "x"); need(b, "b"); need(it, "iters");
+    return yg::rational_calc(lat(l), *p, a0, order, poles, residues, x, b, it);
+  });
+}
+int yg_cg_mixed(yg_lattice *l, const yg_inv_par *p, double *x, double *b, yg_solve_stats *st) {
+  return guard_status([&] { check_par(p); need(x, "x"); need(b, "b"); return yg::cg_mixed(lat(l), *p, x, b, st); });
+}
+
+// ---- forces
+int yg_momenta_upload(yg_lattice *l, const double *h) { return guard([&] { need(h, "host"); yg::momenta_upload(lat(l), h); }); }
+int yg_momenta_download(yg_lattice *l, double *h) { return guard([&] { need(h, "host"); yg::momenta_download(lat(l), h); }); }
+int yg_momenta_zero(yg_lattice *l) {
+  return guard([&] { Lattice &L = lat(l); YG_CUDA(cudaMemsetAsync(L.mom.p, 0, L.mom.bytes, L.stream)); });
+}
+int yg_clover_force_download(yg_lattice *l, double *h) { return guard([&] { need(h, "host"); yg::clover_force_download(lat(l), h); }); }
+int yg_begin_fermion_force(yg_lattice *l) { return guard([&] { yg::begin_fermion_force(lat(l)); }); }
+int yg_end_fermion_force(yg_lattice *l, double dt) { return guard([&] { yg::end_fermion_force(lat(l), dt); }); }
+int yg_wilson_fermion_force(yg_lattice *l, double dt, double m, double res, double *lhs, double *rhs) {
+  return guard([&] { need(lhs, "lhs"); need(rhs, "rhs"); yg::wilson_fermion_force(lat(l), dt, m, res, lhs, rhs); });
+}
+int yg_wilson_fermion_force_q(yg_lattice *l, double dt, double m, double res, double *rhs) {
+  return guard([&] { need(rhs, "rhs"); yg::wilson_fermion_force_q(lat(l), dt, m, res, rhs); });
+}
+int yg_clover_fermion_force(yg_lattice *l, double res, double *lhs, double *rhs) {
+  return guard([&] { need(lhs, "lhs"); need(rhs, "rhs"); yg::clover_fermion_force(lat(l), res, lhs, rhs); });
+}
+int yg_clover_logdet_force(yg_lattice *l, double m, double res) { return guard([&] { yg::clover_logdet_force(lat(l), m, res); }); }
+int yg_wilson_gauge_force(yg_lattice *l, double dt, double beta) { return guard([&] { yg::wilson_gauge_force(lat(l), dt, beta); }); }
+int yg_avr_plaquette(yg_lattice *l, double *out) { return guard([&] { need(out, "out"); *out = yg::avr_plaquette(lat(l)); }); }
+
+}  // extern "C"

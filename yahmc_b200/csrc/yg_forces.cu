@@ -1,0 +1,88 @@
+// Host orchestration of the fermion forces (forces.cpp) and of the gauge-side support
+// (wilson_gauge_force, plaquette, clover logdet); device code in yg_forces_impl.cuh.
+#include <cmath>
+#include <vector>
+#include "yg_lattice.h"
+#include "yg_kernels.h"
+
+namespace yg {
+
+void clover_fermion_force(Lattice &L, double residue, double *lhs, double *rhs) {
+  if (!L.p.clover) return;
+  YG_DISPATCH_D(L.d, K::clover_fermion_force(L.cl_force.as<double2>(), (const double2 *)lhs, (const double2 *)rhs,
+                                             L.g, residue, L.stream));
+  YG_CUDA(cudaGetLastError());
+}
+
+// wilson_fermion_force, forces.cpp:175-227
+void wilson_fermion_force(Lattice &L, double dt, double mass, double residue, double *lhs, double *rhs) {
+  double coeff = dt * residue;
+  if (L.p.eo) {
+    hop(L, rhs, rhs, 2, 1.0, false);      // Dphi_oe(rhs, rhs)
+    hop(L, lhs, lhs, 2, 1.0, false);
+    if (L.p.clover) {
+      clover_inv_apply(L, mass, rhs, rhs, 2, false);    // Dphi_oo_inv(mass, rhs, rhs)
+      clover_inv_apply(L, mass, lhs, lhs, 2, false);
+    }
+    coeff = -coeff;
+  }
+  if (L.p.clover) clover_fermion_force(L, residue, lhs, rhs);
+  YG_DISPATCH_D(L.d, K::hopping_force(L.mom.as<double>(), (const double2 *)lhs, (const double2 *)rhs,
+                                      L.links.as<double2>(), L.g, L.rt.itrepr, L.ng, coeff, L.stream));
+  YG_CUDA(cudaGetLastError());
+}
+
+// wilson_fermion_force_q, forces.cpp:230-236
+void wilson_fermion_force_q(Lattice &L, double dt, double mass, double residue, double *rhs) {
+  double *tmp = L.scratch_field(9);
+  hphi(L, mass, tmp, rhs);
+  wilson_fermion_force(L, dt, mass, residue, tmp, rhs);
+}
+
+void begin_fermion_force(Lattice &L) {
+  if (!L.p.clover) return;
+  YG_CUDA(cudaMemsetAsync(L.cl_force.p, 0, L.cl_force.bytes, L.stream));
+}
+
+void clover_logdet_force(Lattice &L, double mass, double residue) {
+  if (!L.p.clover) return;
+  ensure_ldl(L, 4.0 + mass);
+  YG_DISPATCH_D(L.d, K::clover_ldl_force(L.cl_force.as<double2>(), L.ldl.as<double2>(), L.g, residue, L.stream));
+  YG_CUDA(cudaGetLastError());
+}
+
+void end_fermion_force(Lattice &L, double dt) {
+  if (!L.p.clover) return;
+  double coeff = L.p.csw * dt / 8.0;
+  YG_DISPATCH_D(L.d, K::clover_force_core(L.mom.as<double>(), L.cl_force.as<double2>(), L.links.as<double2>(), L.g,
+                                          L.rt.itrepr, L.ng, coeff, L.stream));
+  YG_CUDA(cudaGetLastError());
+}
+
+void wilson_gauge_force(Lattice &L, double dt, double beta) {
+  if (L.p.bc == YG_BC_OPEN || L.p.bc == YG_BC_SF)
+    throw Error(YG_ERR_ARG, "gauge force with open/SF plaquette weights is not provided");
+  double coeff = dt * (beta / L.nc);
+  YG_DISPATCH_N(L.nc, K::gauge_force(L.mom.as<double>(), L.fund.as<double2>(), L.g, L.rt.itfund, coeff, L.stream));
+  YG_CUDA(cudaGetLastError());
+}
+
+double clover_logdet(Lattice &L, double mass) {
+  if (!L.p.clover) return 0.0;
+  ensure_ldl(L, 4.0 + mass);
+  double *tmp = L.scratch_field(0);
+  YG_DISPATCH_D(L.d, K::logdet(tmp, L.ldl.as<double2>(), (int)L.Vh, L.stream));
+  YG_CUDA(cudaGetLastError());
+  return sum_device(L, tmp, L.Vh);
+}
+
+double avr_plaquette(Lattice &L) {
+  if (L.p.bc == YG_BC_OPEN || L.p.bc == YG_BC_SF)
+    throw Error(YG_ERR_ARG, "plaquette with open/SF weights is not provided");
+  double *tmp = L.scratch_field(0);
+  YG_DISPATCH_N(L.nc, K::plaquette(tmp, L.fund.as<double2>(), L.g, L.stream));
+  YG_CUDA(cudaGetLastError());
+  return sum_device(L, tmp, L.V) / (L.nc * 6.0 * L.V);
+}
+
+}  // namespace yg

@@ -1,0 +1,13 @@
+// Instantiation unit: force, representation and gauge kernels for d = 4
+// (declarations in yg_kernels.h, device code in yg_forces_impl.cuh / yg_repr_impl.cuh).
+#include "yg_forces_impl.cuh"
+#include "yg_repr_impl.cuh"
+
+namespace yg {
+template void DK<4>::clover_fermion_force(double2 *, const double2 *, const double2 *, Geom, double, cudaStream_t);
+template void DK<4>::hopping_force(double *, const double2 *, const double2 *, const double2 *, Geom, const double2 *, int, double, cudaStream_t);
+template void DK<4>::clover_ldl_force(double2 *, const double2 *, Geom, double, cudaStream_t);
+template void DK<4>::clover_force_core(double *, const double2 *, const double2 *, Geom, const double2 *, int, double, cudaStream_t);
+template struct RK<4, 4>;
+template struct GK<4>;
+}  // namespace yg

@@ -1,0 +1,156 @@
+// Private state of a yg_lattice handle and the engine functions shared by the host
+// translation units.  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+#include <stdexcept>
+#include "yg_core.cuh"
+#include "../../include/yahmc_gpu.h"
+
+namespace yg {
+
+// Error carrying a yg_status; the C ABI layer converts it to a return code.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+void check_cuda(cudaError_t e, const char *what);
+#define YG_CUDA(x) ::yg::check_cuda((x), #x)
+
+// Device buffer owned by a lattice.
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  void alloc(size_t n);
+  void release();
+  template <typename T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+// Device tables describing the representation.
+struct ReprTables {
+  double2 *basis;    // d x N x N basis matrices b_n (repr.cpp:25-59)
+  double2 *itrepr;   // NG x d x d generators of the fermion representation (repr.cpp:73-104)
+  double2 *itfund;   // NG x N x N generators of the fundamental representation
+};
+
+struct Lattice {
+  yg_params p{};
+  Geom g{};
+  int d = 0, nc = 0, ng = 0;
+  long V = 0, Vh = 0;
+  cudaStream_t stream = 0;
+  int mvm = 0;
+
+  DevBuf fund;      // fundamental links, 4 x N x N per site        (gfield_fund)
+  DevBuf links;     // represented links with the AP sign, 4 x d x d (gfield_repr)
+  DevBuf clover;    // clover term, 4 x d x d per site                (cl_term)
+  DevBuf ldl;       // LDL factors, 2 x d(2d+1) per site of block 1   (cl_ldl)
+  double ldl_sigma = 0;
+  bool ldl_valid = false;
+  DevBuf cl_force;  // 6 x d x d per site                            (cl_force)
+  DevBuf mom;       // 4 x NG per site                               (afield_momenta)
+  DevBuf tables;    // basis / generators
+  ReprTables rt{};
+
+  // reduction scratch: per-block partial sums + result
+  DevBuf red_partial;
+  DevBuf red_result;
+  double *host_result = nullptr;   // pinned
+  int red_blocks = 0;
+
+  // scratch spinor fields (the reference's static SpinorFields, e.g. dirac.cpp:741)
+  std::vector<double *> scratch;
+  double *scratch_field(int i);
+
+  // single-precision mirrors for the mixed-precision solver
+  DevBuf links_f;   // represented links in float2
+  DevBuf clover_f;  // clover term in float2
+  DevBuf cinv_f;    // explicit inverse of the odd-site clover blocks, float2
+  double cinv_f_sigma = 0;
+  bool links_f_valid = false;
+  bool cinv_f_valid = false;
+
+  long field_doubles() const { return 8L * d * V; }
+  size_t field_bytes() const { return sizeof(double) * field_doubles(); }
+
+  // site range of a view (spinor_select_* / spinor_type_*, linalg.cpp:272-329)
+  void view_range(int view, long &lo, long &n) const;
+
+  ~Lattice();
+};
+
+// ---- yg_lattice.cu
+Lattice *lattice_create(const yg_params &p);
+void represent_and_clover(Lattice &L);
+void ensure_ldl(Lattice &L, double sigma);
+void gauge_upload(Lattice &L, const double *host);
+void gauge_download(Lattice &L, double *host);
+void repr_download(Lattice &L, double *host);
+void clover_download(Lattice &L, double *host);
+void clover_force_download(Lattice &L, double *host);
+void ldl_download(Lattice &L, double mass, double *host);
+void field_upload(Lattice &L, double *dev, const double *host);
+void field_download(Lattice &L, double *host, const double *dev);
+void momenta_upload(Lattice &L, const double *host);
+void momenta_download(Lattice &L, double *host);
+
+// ---- yg_dirac.cu: hop (dirac_kernel, dirac.cpp:227-704); part 1 even, 2 odd, 3 both
+void bc_zero_field(Lattice &L, double *f);
+void hop(Lattice &L, double *dst, const double *src, int part, double sign, bool assign);
+void clover_apply(Lattice &L, double mass, double *dst, const double *src, int part, bool assign);
+void clover_inv_apply(Lattice &L, double mass, double *dst, const double *src, int part, bool assign);
+//   step 1: tmp_o = A_oo^-1 ( 1/2 H_oe src_e ), optionally also writing 1/2 H_oe src_e to clob_o
+//   step 2: dst_e = A_ee src_e - 1/2 H_eo tmp_o  [then gamma5]
+void schur_step1(Lattice &L, double mass, double *tmp, const double *src, double *clob);
+void schur_step2(Lattice &L, double mass, double *dst, const double *tmp, const double *src, bool g5);
+void dphi(Lattice &L, double mass, double *dst, double *src);
+void hphi(Lattice &L, double mass, double *dst, double *src);
+void hphi_sq(Lattice &L, double mass, double *dst, double *src);
+void apply_op(Lattice &L, int op, double mass, double *dst, double *src);
+void hphi_float(Lattice &L, double mass, float2 *dst, float2 *src, float2 *tmp);
+
+// ---- yg_blas.cu: BLAS-1 (linalg.cpp) over [lo, lo+n) sites
+double blas_sqnorm(Lattice &L, const double *a, long lo, long n);
+double2 blas_product(Lattice &L, const double *a, const double *b, long lo, long n);
+double blas_product_re(Lattice &L, const double *a, const double *b, long lo, long n);
+// lhs = alpha*lhs + beta*rhs (complex coefficients; rhs may be null)
+void blas_axpby(Lattice &L, double *lhs, double2 alpha, double2 beta, const double *rhs, long lo, long n);
+void blas_g5(Lattice &L, double *f, long lo, long n);
+void blas_copy(Lattice &L, double *dst, const double *src);
+void blas_zero(Lattice &L, double *f, long lo, long n);
+// fused CG update: x += a p ; r -= a q ; return |r|^2
+double blas_cg_update(Lattice &L, double *x, double *r, const double *p, const double *q, double a, long lo, long n);
+double sum_device(Lattice &L, const double *v, long n);
+// FP32 helpers of the mixed-precision solver (counts in complex words)
+void f_from_d(Lattice &L, float *dst, const double *src, long cnt);
+void d_add_f(Lattice &L, double *dst, const float *src, long cnt);
+double f_sqnorm(Lattice &L, const float *a, long cnt);
+double f_product_re(Lattice &L, const float *a, const float *b, long cnt);
+double f_cg_update(Lattice &L, float *x, float *r, const float *p, const float *q, float a, long cnt);
+void f_xpay(Lattice &L, float *p, float b, const float *r, long cnt);
+
+// ---- yg_solvers.cu
+int cg(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
+int cg_mshift(Lattice &L, const yg_inv_par &par, int num, const double *shift, double *const *xs, double *b, int *iters);
+int bicgstab(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
+int minres(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
+int auto_inverter(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
+int rational_calc(Lattice &L, const yg_inv_par &par, double a0, int order, const double *poles,
+                  const double *residues, double *x, double *b, int *iters);
+int cg_mixed(Lattice &L, const yg_inv_par &par, double *x, double *b, yg_solve_stats *st);
+
+// ---- yg_forces.cu
+void clover_fermion_force(Lattice &L, double residue, double *lhs, double *rhs);
+void wilson_fermion_force(Lattice &L, double dt, double mass, double residue, double *lhs, double *rhs);
+void wilson_fermion_force_q(Lattice &L, double dt, double mass, double residue, double *rhs);
+void begin_fermion_force(Lattice &L);
+void end_fermion_force(Lattice &L, double dt);
+void clover_logdet_force(Lattice &L, double mass, double residue);
+void wilson_gauge_force(Lattice &L, double dt, double beta);
+double clover_logdet(Lattice &L, double mass);
+double avr_plaquette(Lattice &L);
+
+}  // namespace yg
