@@ -1,0 +1,331 @@
+"""Benchmark: CG time-to-solution on the even-odd Wilson-clover operator, one B200.
+
+Workload (defaults): 32^4 SU(3) fundamental, even-odd preconditioned Wilson-clover,
+m = -0.75, csw = 1.0, periodic space / antiperiodic time.  One step = one solve of
+Hphi_sq x = b (the D^dag D system of cg_inverter, cg.cpp:132-202) to a TRUE FP64
+relative residual of 1e-12 (prec = 1e-24 in the reference's squared convention), with
+the mixed-precision solver (FP32 inner iterations, FP64 reliable updates).
+
+Reported beside it: the same solve with the plain FP64 CG (the reference's algorithm on
+the GPU), the FP64 Dslash (Dphi_oe) bandwidth against the measured HBM peak, the same
+metric end to end through the public API with the source uploaded from pinned host
+memory and the solution downloaded every step, and the reference's own CPU code
+(oracle/_ref, built from the reference sources) timed on this host's cores.
+
+Synthetic inputs: links are the reference's random start (exp of a Gaussian su(3)
+algebra element per link, library/suNg.cpp:375-380) from a fixed seed, standing in for
+a thermalised beta=5.6 field; the source is a complex Gaussian, unit variance per
+component.  Every input (links 604 MB, clover 604 MB, fields 201 MB each) is larger than
+the 126 MB L2, so no flush is needed between timed steps.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                       [--dims T X Y Z] [--no-cpu-baseline]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+MASS, CSW, PREC = -0.75, 1.0, 1e-24
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--dims", type=int, nargs=4, default=[32, 32, 32, 32])
+    ap.add_argument("--seed", type=int, default=20241203)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--dslash-iters", type=int, default=50)
+    return ap.parse_args()
+
+
+def hbm_peak():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def make_inputs(dims, seed, rank=0):
+    from yahmc_b200 import fields
+    T, X, Y, Z = dims
+    V = T * X * Y * Z
+    rng = np.random.default_rng(seed + 7919 * rank)
+    U = fields.random_start_su(3, 4 * V, rng).reshape(V, 4, 3, 3)
+    b = fields.gaussian_spinor(V, 3, rng)
+    return U, b
+
+
+def workload_name(dims):
+    return f"{'x'.join(map(str, dims))} SU(3) fund even-odd Wilson-clover CG on Hphi_sq to true rel. residual 1e-12"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, gpu_index=0):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ reference (CPU) arm
+def reference_solve_ms(dims, U, b, steps, threads):
+    """The reference's own cg_inverter (oracle/_ref, compiled from the reference sources) on
+    Hphi_sq with the same links, source and squared precision; returns (ms per solve, iters)."""
+    from oracle import ref as oref
+    from oracle import yahmc_oracle as yo
+    from yahmc_b200 import fields
+    R = oref.get("su3_fund_ap", tuple(dims), csw=CSW, cf=1.0, threads=threads)
+    R.lib.yref_set_threads(threads)
+    R.set_links(fields.complex_to_raw(U))
+    braw = yo.spinor_to_raw(b)
+    times, its = [], []
+    for _ in range(steps):
+        x = R.spinor()
+        bb = braw.copy()
+        t0 = time.perf_counter()
+        it = R.call("cg", 2, MASS, PREC, x, bb)
+        times.append((time.perf_counter() - t0) * 1e3)
+        its.append(it)
+    return float(np.median(times)), int(its[-1])
+
+
+def run_reference(a, rank, world):
+    if rank != 0:
+        return
+    from oracle import ref as oref
+    if not oref.available("su3_fund_ap"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (no reference sources on this host)"}))
+        return
+    threads = os.cpu_count() or 1
+    U, b = make_inputs(a.dims, a.seed)
+    steps = max(1, min(a.steps, 3))
+    warm = min(a.warmup, 1)
+    if warm:
+        reference_solve_ms(a.dims, U, b, warm, threads)
+    ms, it = reference_solve_ms(a.dims, U, b, steps, threads)
+    line = {
+        "impl": "reference", "metric": "CG time-to-solution (true rel. residual 1e-12)", "value": ms, "unit": "ms",
+        "n_gpus": a.gpus, "steps": steps, "warmup": warm, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(a.dims), "iterations": it, "threads": threads},
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
+                         "sample": f"{steps} full reference cg_inverter solves (prec 1e-24) on {threads} OpenMP threads"},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(a, rank, world, dist):
+    import torch
+    import yahmc_b200 as yg
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    dev = torch.cuda.current_device()
+    U, b = make_inputs(a.dims, a.seed, rank)
+    lat = yg.Lattice(a.dims, nc=3, repr="fundamental", bc="antiperiodic", clover=True, eo=True, csw=CSW)
+    lat.set_links(U)
+    V, d = lat.V, lat.d
+    field_bytes = lat.field_doubles * 8
+    bf = lat.field(b)
+    x = lat.field()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, k):
+        """k calls of fn bracketed by a barrier + synchronize on both sides, CUDA events on the
+        default stream (the engine's stream); returns per-call ms, max over ranks."""
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = [fn() for _ in range(k)]
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1) / k
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, out
+
+    def mixed():
+        lat.spinor_zero(x)
+        return lat.cg_mixed("Hphi_sq", MASS, PREC, x, bf)
+
+    def fp64():
+        lat.spinor_zero(x)
+        return lat.cg_inverter("Hphi_sq", MASS, PREC, x, bf)
+
+    # warm-up (W >= 3 solves), then the timed mixed-precision solves with clocks sampled
+    for _ in range(max(3, a.warmup)):
+        mixed()
+    clk = Clocks(dev)
+    n0 = yg.launch_count()
+    ms_mixed, stats = timed(mixed, a.steps)
+    launches = (yg.launch_count() - n0) // a.steps
+    clocks = clk.stop()
+    st = stats[-1]
+    # independent check of the stopping criterion on the true residual
+    xc, r = lat.field(), lat.field()
+    lat.spinor_copy(xc, x)
+    lat.Hphi_sq(MASS, r, xc)
+    lat.spinor_sub_assign(r, bf)
+    true_res = lat.spinor_sqnorm(r) / lat.spinor_sqnorm(bf)
+
+    # plain FP64 CG (the reference's algorithm on the GPU)
+    fp64()
+    ms_fp64, its = timed(fp64, max(1, min(a.steps, 3)))
+    it_fp64 = its[-1]
+
+    # FP64 Dslash (Dphi_oe): one hop over V/2 output sites
+    src, dst = lat.field(b), lat.field()
+    for _ in range(5):
+        lat.Dphi_oe(dst, src)
+    ms_hop, _ = timed(lambda: lat.Dphi_oe(dst, src), a.dslash_iters)
+    link_reals = 2 * d * d
+    bytes_per_site = (2 * 8 * d + 8 * link_reals) * 8          # 1 spinor in + 1 out + 8 links, FP64
+    hop_bytes = bytes_per_site * (V // 2)
+    hop_gbs = hop_bytes / (ms_hop * 1e-3) / 1e9
+    peak, peak_kind = hbm_peak()
+
+    # end to end through the public API: pinned host source in, solution out, every step
+    hb = torch.empty(lat.field_doubles, dtype=torch.float64, pin_memory=True).numpy()
+    hx = torch.empty(lat.field_doubles, dtype=torch.float64, pin_memory=True).numpy()
+    from yahmc_b200.fields import complex_to_raw
+    hb[:] = complex_to_raw(b)
+
+    def e2e():
+        lat.upload(bf, hb)
+        lat.spinor_zero(x)
+        s = lat.cg_mixed("Hphi_sq", MASS, PREC, x, bf)
+        lat.download(x, raw=True, out=hx)
+        return s
+
+    e2e()
+    ms_e2e, _ = timed(e2e, a.steps)
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            from oracle import ref as oref
+            if oref.available("su3_fund_ap"):
+                threads = os.cpu_count() or 1
+                cms, cit = reference_solve_ms(a.dims, U, b, 1, threads)
+                cpu = {"value": cms, "unit": "ms", "cores": threads, "kind": "reference",
+                       "sample": f"1 full reference cg_inverter solve (prec 1e-24, {cit} iterations) of the same "
+                                 f"system on {threads} OpenMP threads"}
+            else:
+                cpu = {"value": None, "unit": "ms", "cores": 0, "kind": "reference",
+                       "sample": "oracle/_ref not built on this host"}
+        except Exception as e:     # the baseline is reported, never required
+            cpu = {"value": None, "unit": "ms", "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
+
+    if rank != 0:
+        return
+    value = ms_mixed / world          # whole-job time per solve: world solves run concurrently
+    line = {
+        "metric": "CG time-to-solution (true rel. residual 1e-12), mixed precision",
+        "value": value, "unit": "ms", "n_gpus": world, "steps": a.steps, "warmup": max(3, a.warmup),
+        "ms_per_step": ms_mixed, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 inner / f64 reliable updates and residual", "data": "synthetic",
+        "config": {"workload": workload_name(a.dims), "mass": MASS, "csw": CSW, "prec_squared": PREC,
+                   "links": "random start exp(Gaussian su(3) algebra), seeded",
+                   "l2": "inputs larger than L2 (links 604 MB, clover 604 MB), no flush",
+                   "parallelism": f"replicas x{world}"},
+        "solver": {"iterations": st["iterations"], "reliable_updates": st["reliable_updates"],
+                   "fallback": st["fallback"], "true_residual": true_res},
+        "fp64_cg": {"ms": ms_fp64, "iterations": it_fp64, "speedup_mixed_vs_fp64": ms_fp64 / ms_mixed},
+        "dslash_fp64": {"ms": ms_hop, "GB_s": hop_gbs, "bytes_per_site": bytes_per_site, "sites": V // 2},
+        "roofline": {"bound": "hbm", "kernel": "k_hop<3,double,PLAIN> (Dphi_oe, FP64 18-real links)",
+                     "achieved": hop_gbs, "peak": peak, "unit": "GB/s", "frac": hop_gbs / peak,
+                     "peak_kind": peak_kind, "traffic": None},
+        "e2e": {"value": ms_e2e / world, "unit": "ms", "h2d_bytes_per_step": field_bytes,
+                "d2h_bytes_per_step": field_bytes},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+
+
+def main():
+    a = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        import datetime
+        backend = "nccl" if a.impl == "ours" else "gloo"
+        if a.impl == "ours":
+            import torch
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist_mod.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        dist = dist_mod
+    try:
+        if a.impl == "reference":
+            run_reference(a, rank, world)
+        else:
+            run_ours(a, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

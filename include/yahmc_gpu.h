@@ -105,6 +105,9 @@ int yg_lattice_query(const yg_lattice *lat, yg_info *out);
 int yg_set_stream(yg_lattice *lat, void *cuda_stream);
 int yg_synchronize(yg_lattice *lat);
 const char *yg_last_error(void);
+/* No reference counterpart: number of kernels this library has launched since it was
+ * loaded (all lattices); benchmarks difference it around a timed region. */
+long yg_launch_count(void);
 
 /* ---- spinor fields (SpinorField, spinorfield.h:6-39; spinor_allocate linalg.cpp:10-27) */
 int yg_field_alloc(yg_lattice *lat, double **dev_field);

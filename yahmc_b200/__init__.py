@@ -114,12 +114,19 @@ def load_library(path: Path | str | None = None):
         raise RuntimeError(f"{p} not found: build the CUDA library with `python -m yahmc_b200.build`")
     lib = ctypes.CDLL(str(p))
     lib.yg_last_error.restype = ctypes.c_char_p
+    lib.yg_launch_count.restype = ctypes.c_long
+    lib.yg_launch_count.argtypes = []
     for name, args in _SIGNATURES.items():
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = None if name in ("yg_lattice_destroy", "yg_mvm_reset") else ctypes.c_int
     _lib = lib
     return lib
+
+
+def launch_count() -> int:
+    """Kernels launched by the engine library since it was loaded."""
+    return int(load_library().yg_launch_count())
 
 
 def _ptr(a: np.ndarray):
@@ -209,8 +216,11 @@ class Lattice:
         assert raw.size == self.field_doubles
         self._check(self.lib.yg_field_upload(self.h, f.ptr, _ptr(raw)))
 
-    def download(self, f: Field, raw=False):
-        out = np.empty(self.field_doubles)
+    def download(self, f: Field, raw=False, out=None):
+        """Field to host; `out` (a contiguous float64 buffer, e.g. pinned) receives the raw
+        reference-layout doubles when given."""
+        if out is None:
+            out = np.empty(self.field_doubles)
         self._check(self.lib.yg_field_download(self.h, _ptr(out), f.ptr))
         return out if raw else raw_to_complex(out, self.d, 4)
 

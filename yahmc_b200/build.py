@@ -11,6 +11,7 @@ from __future__ import annotations
 import argparse
 import concurrent.futures as cf
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -44,6 +45,19 @@ def headers():
     return sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [ROOT / "include" / "yahmc_gpu.h"]
 
 
+def deps(src: Path, seen=None) -> set:
+    """The file and every quoted #include it reaches (resolved relative to the includer)."""
+    seen = set() if seen is None else seen
+    if src in seen or not src.exists():
+        return seen
+    seen.add(src)
+    for line in src.read_text().splitlines():
+        m = re.match(r'\s*#\s*include\s+"([^"]+)"', line)
+        if m:
+            deps((src.parent / m.group(1)).resolve(), seen)
+    return seen
+
+
 def _compile(args):
     src, obj, flags, verbose = args
     t0 = time.time()
@@ -64,7 +78,6 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None, out: Pat
     lib = out_dir / LIB.name
     obj_dir.mkdir(parents=True, exist_ok=True)
     flags = NVCC_FLAGS + list(extra_flags or [])
-    hdr_time = max(p.stat().st_mtime for p in headers())
     jobs = []
     # largest translation units first so that the parallel build ends sooner
     weight = {"yg_inst_d15_op": 0, "yg_inst_d10_op": 1, "yg_inst_d15_aux": 2, "yg_inst_d10_aux": 3,
@@ -72,7 +85,8 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None, out: Pat
     srcs = sorted(sources(), key=lambda s: (weight.get(s.stem, 99), s.name))
     for src in srcs:
         obj = obj_dir / (src.stem + ".o")
-        stale = force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, hdr_time)
+        newest = max(p.stat().st_mtime for p in deps(src.resolve()))
+        stale = force or not obj.exists() or obj.stat().st_mtime < newest
         if stale:
             jobs.append((src, obj, flags, verbose))
     if jobs:

@@ -74,7 +74,7 @@ static int red_grid(Lattice &L, long n) {
 
 static double2 finish_reduce(Lattice &L, int grid) {
   k_reduce_final<<<1, 1024, 0, L.stream>>>(L.red_result.as<double2>(), L.red_partial.as<double2>(), grid);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   YG_CUDA(cudaMemcpyAsync(L.host_result, L.red_result.p, sizeof(double2), cudaMemcpyDeviceToHost, L.stream));
   YG_CUDA(cudaStreamSynchronize(L.stream));
   return make_double2(L.host_result[0], L.host_result[1]);
@@ -87,7 +87,7 @@ double blas_sqnorm(Lattice &L, const double *a, long lo, long n) {
   long cnt = wcnt(L, n);
   int grid = red_grid(L, cnt);
   k_reduce<0><<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (const double2 *)a + woff(L, lo), nullptr, cnt);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   return finish_reduce(L, grid).x;
 }
 
@@ -96,7 +96,7 @@ double2 blas_product(Lattice &L, const double *a, const double *b, long lo, long
   int grid = red_grid(L, cnt);
   k_reduce<1><<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (const double2 *)a + woff(L, lo),
                                            (const double2 *)b + woff(L, lo), cnt);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   return finish_reduce(L, grid);
 }
 
@@ -105,7 +105,7 @@ double blas_product_re(Lattice &L, const double *a, const double *b, long lo, lo
   int grid = red_grid(L, cnt);
   k_reduce<2><<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (const double2 *)a + woff(L, lo),
                                            (const double2 *)b + woff(L, lo), cnt);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   return finish_reduce(L, grid).x;
 }
 
@@ -131,7 +131,7 @@ void blas_axpby(Lattice &L, double *lhs, double2 alpha, double2 beta, const doub
   int read_lhs = !(alpha.x == 0.0 && alpha.y == 0.0);
   k_axpby<<<stream_grid(cnt), 256, 0, L.stream>>>((double2 *)lhs + woff(L, lo), alpha, beta,
                                                     rhs ? (const double2 *)rhs + woff(L, lo) : nullptr, cnt, read_lhs);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
 }
 
 __global__ void __launch_bounds__(256) k_neg(double2 *f, long n) {
@@ -148,7 +148,7 @@ void blas_g5(Lattice &L, double *f, long lo, long n) {
     double2 *base = (double2 *)f + blk * per_blk + 2L * L.d * L.Vh;
     long cnt = 2L * L.d * L.Vh;
     k_neg<<<stream_grid(cnt), 256, 0, L.stream>>>(base, cnt);
-    YG_CUDA(cudaGetLastError());
+    YG_LAUNCHED();
   }
 }
 
@@ -186,7 +186,7 @@ double blas_cg_update(Lattice &L, double *x, double *r, const double *p, const d
   long o = woff(L, lo);
   k_cg_update<<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (double2 *)x + o, (double2 *)r + o,
                                            (const double2 *)p + o, (const double2 *)q + o, a, cnt);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   return finish_reduce(L, grid).x;
 }
 
@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(256) k_sum_partial(double2 *partial, const dou
 double sum_device(Lattice &L, const double *v, long n) {
   int grid = red_grid(L, n);
   k_sum_partial<<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), v, n);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   return finish_reduce(L, grid).x;
 }
 
@@ -266,25 +266,25 @@ __global__ void k_xpay_f(float2 *p, float b, const float2 *r, long n) {
 
 void f_from_d(Lattice &L, float *dst, const double *src, long cnt) {
   k_d2f<<<stream_grid(cnt), 256, 0, L.stream>>>((float2 *)dst, (const double2 *)src, cnt);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
 }
 
 void d_add_f(Lattice &L, double *dst, const float *src, long cnt) {
   k_f2d_add<<<stream_grid(cnt), 256, 0, L.stream>>>((double2 *)dst, (const float2 *)src, cnt);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
 }
 
 double f_sqnorm(Lattice &L, const float *a, long cnt) {
   int grid = red_grid(L, cnt);
   k_reduce_f<0><<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (const float2 *)a, nullptr, cnt);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   return finish_reduce(L, grid).x;
 }
 
 double f_product_re(Lattice &L, const float *a, const float *b, long cnt) {
   int grid = red_grid(L, cnt);
   k_reduce_f<2><<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (const float2 *)a, (const float2 *)b, cnt);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   return finish_reduce(L, grid).x;
 }
 
@@ -292,13 +292,13 @@ double f_cg_update(Lattice &L, float *x, float *r, const float *p, const float *
   int grid = red_grid(L, cnt);
   k_cg_update_f<<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (float2 *)x, (float2 *)r,
                                              (const float2 *)p, (const float2 *)q, a, cnt);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   return finish_reduce(L, grid).x;
 }
 
 void f_xpay(Lattice &L, float *p, float b, const float *r, long cnt) {
   k_xpay_f<<<stream_grid(cnt), 256, 0, L.stream>>>((float2 *)p, b, (const float2 *)r, cnt);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
 }
 
 }  // namespace yg

@@ -55,6 +55,8 @@ extern "C" {
 
 const char *yg_last_error(void) { return g_last_error.c_str(); }
 
+long yg_launch_count(void) { return yg::g_launch_count; }
+
 int yg_lattice_create(const yg_params *p, yg_lattice **out) {
   return guard([&] {
     need(p, "params");

@@ -35,7 +35,7 @@ void bc_zero_field(Lattice &L, double *f) {
   if (!has_spinor_bcs(L)) return;
   int vol3 = L.g.dim[1] * L.g.dim[2] * L.g.dim[3];
   k_bc_zero<<<nblk(3L * vol3, 128), 128, 0, L.stream>>>((double2 *)f, L.g, 4 * L.d);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
 }
 
 template <typename R>
@@ -49,7 +49,7 @@ static HopArgs<R> base_args(const Lattice &L) {
 template <int EPI, typename R>
 static void launch_hop(Lattice &L, const HopArgs<R> &a) {
   YG_DISPATCH_D(L.d, K::hop(a, EPI, L.stream));
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
 }
 
 void hop(Lattice &L, double *dst, const double *src, int part, double sign, bool assign) {
@@ -71,7 +71,7 @@ void clover_apply(Lattice &L, double mass, double *dst, const double *src, int p
   part_range(L, part, lo, n);
   YG_DISPATCH_D(L.d, K::clover((double2 *)dst, (const double2 *)src, L.clover.as<double2>(), L.g, 4.0 + mass,
                                 L.p.cf - 1.0, lo, n, assign, L.stream));
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
 }
 
 void clover_inv_apply(Lattice &L, double mass, double *dst, const double *src, int part, bool assign) {
@@ -79,7 +79,7 @@ void clover_inv_apply(Lattice &L, double mass, double *dst, const double *src, i
   if (part != 2) throw Error(YG_ERR_ARG, "the clover inverse is stored for the odd block only");
   ensure_ldl(L, 4.0 + mass);
   YG_DISPATCH_D(L.d, K::clover_inv((double2 *)dst, (const double2 *)src, L.ldl.as<double2>(), L.g, assign, L.stream));
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
 }
 
 void schur_step1(Lattice &L, double mass, double *tmp, const double *src, double *clob) {
@@ -189,11 +189,11 @@ static void ensure_float_operator(Lattice &L, double mass) {
   if (!L.links_f_valid) {
     L.links_f.alloc(sizeof(float2) * nl);
     k_to_float<<<nblk(nl, 256), 256, 0, L.stream>>>(L.links_f.as<float2>(), L.links.as<double2>(), nl);
-    YG_CUDA(cudaGetLastError());
+    YG_LAUNCHED();
     if (L.p.clover) {
       L.clover_f.alloc(sizeof(float2) * nl);
       k_to_float<<<nblk(nl, 256), 256, 0, L.stream>>>(L.clover_f.as<float2>(), L.clover.as<double2>(), nl);
-      YG_CUDA(cudaGetLastError());
+      YG_LAUNCHED();
     }
     L.links_f_valid = true;
   }
@@ -202,7 +202,7 @@ static void ensure_float_operator(Lattice &L, double mass) {
     long n = 2L * (2 * L.d) * (2 * L.d) * L.Vh;
     L.cinv_f.alloc(sizeof(float2) * n);
     YG_DISPATCH_D(L.d, K::cinv_float(L.cinv_f.as<float2>(), L.ldl.as<double2>(), (int)L.Vh, L.stream));
-    YG_CUDA(cudaGetLastError());
+    YG_LAUNCHED();
     L.cinv_f_sigma = 4.0 + mass;
     L.cinv_f_valid = true;
   }

@@ -11,7 +11,7 @@ void clover_fermion_force(Lattice &L, double residue, double *lhs, double *rhs) 
   if (!L.p.clover) return;
   YG_DISPATCH_D(L.d, K::clover_fermion_force(L.cl_force.as<double2>(), (const double2 *)lhs, (const double2 *)rhs,
                                              L.g, residue, L.stream));
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
 }
 
 // wilson_fermion_force, forces.cpp:175-227
@@ -29,7 +29,7 @@ void wilson_fermion_force(Lattice &L, double dt, double mass, double residue, do
   if (L.p.clover) clover_fermion_force(L, residue, lhs, rhs);
   YG_DISPATCH_D(L.d, K::hopping_force(L.mom.as<double>(), (const double2 *)lhs, (const double2 *)rhs,
                                       L.links.as<double2>(), L.g, L.rt.itrepr, L.ng, coeff, L.stream));
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
 }
 
 // wilson_fermion_force_q, forces.cpp:230-236
@@ -48,7 +48,7 @@ void clover_logdet_force(Lattice &L, double mass, double residue) {
   if (!L.p.clover) return;
   ensure_ldl(L, 4.0 + mass);
   YG_DISPATCH_D(L.d, K::clover_ldl_force(L.cl_force.as<double2>(), L.ldl.as<double2>(), L.g, residue, L.stream));
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
 }
 
 void end_fermion_force(Lattice &L, double dt) {
@@ -56,7 +56,7 @@ void end_fermion_force(Lattice &L, double dt) {
   double coeff = L.p.csw * dt / 8.0;
   YG_DISPATCH_D(L.d, K::clover_force_core(L.mom.as<double>(), L.cl_force.as<double2>(), L.links.as<double2>(), L.g,
                                           L.rt.itrepr, L.ng, coeff, L.stream));
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
 }
 
 void wilson_gauge_force(Lattice &L, double dt, double beta) {
@@ -64,7 +64,7 @@ void wilson_gauge_force(Lattice &L, double dt, double beta) {
     throw Error(YG_ERR_ARG, "gauge force with open/SF plaquette weights is not provided");
   double coeff = dt * (beta / L.nc);
   YG_DISPATCH_N(L.nc, K::gauge_force(L.mom.as<double>(), L.fund.as<double2>(), L.g, L.rt.itfund, coeff, L.stream));
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
 }
 
 double clover_logdet(Lattice &L, double mass) {
@@ -72,7 +72,7 @@ double clover_logdet(Lattice &L, double mass) {
   ensure_ldl(L, 4.0 + mass);
   double *tmp = L.scratch_field(0);
   YG_DISPATCH_D(L.d, K::logdet(tmp, L.ldl.as<double2>(), (int)L.Vh, L.stream));
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   return sum_device(L, tmp, L.Vh);
 }
 
@@ -81,7 +81,7 @@ double avr_plaquette(Lattice &L) {
     throw Error(YG_ERR_ARG, "plaquette with open/SF weights is not provided");
   double *tmp = L.scratch_field(0);
   YG_DISPATCH_N(L.nc, K::plaquette(tmp, L.fund.as<double2>(), L.g, L.stream));
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   return sum_device(L, tmp, L.V) / (L.nc * 6.0 * L.V);
 }
 

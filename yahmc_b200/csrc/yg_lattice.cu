@@ -16,6 +16,8 @@
 
 namespace yg {
 
+long g_launch_count = 0;
+
 void check_cuda(cudaError_t e, const char *what) {
   if (e != cudaSuccess) {
     int code = (e == cudaErrorMemoryAllocation) ? YG_ERR_OOM : YG_ERR_CUDA;
@@ -226,11 +228,11 @@ __global__ void k_spinor_to_host(double *dst, const double2 *src, Geom g, int d)
 // ------------------------------------------------------------------ gauge field
 void represent_and_clover(Lattice &L) {
   YG_DISPATCH_ND(L.nc, L.d, K::represent(L.links.as<double2>(), L.fund.as<double2>(), L.g, L.rt.basis, L.p.repr, L.stream));
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   if (L.p.clover) {
     YG_DISPATCH_ND(L.nc, L.d, K::clover_term(L.clover.as<double2>(), L.fund.as<double2>(), L.g, L.rt.basis, L.p.repr,
                                               L.p.csw, L.stream));
-    YG_CUDA(cudaGetLastError());
+    YG_LAUNCHED();
   }
   L.ldl_valid = false;          // cl_sigma = 0xF00F, clover.cpp:337
   L.cinv_f_valid = false;
@@ -242,7 +244,7 @@ void ensure_ldl(Lattice &L, double sigma) {
   if (L.ldl_valid && L.ldl_sigma == sigma) return;    // clover.cpp:314-321
   int boundary_term = (L.p.bc == YG_BC_OPEN || L.p.bc == YG_BC_SF);
   YG_DISPATCH_D(L.d, K::ldl(L.ldl.as<double2>(), L.clover.as<double2>(), L.g, sigma, L.p.cf, boundary_term, L.stream));
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   L.ldl_sigma = sigma;
   L.ldl_valid = true;
 }
@@ -328,7 +330,7 @@ Lattice *lattice_create(const yg_params &p) {
     tmp.alloc(unit.size() * sizeof(double));
     YG_CUDA(cudaMemcpy(tmp.p, unit.data(), unit.size() * sizeof(double), cudaMemcpyHostToDevice));
     k_aos_to_soa<<<nblk(4 * V, 128), 128, 0, L->stream>>>(L->fund.as<double2>(), tmp.as<double>(), g, nc * nc, 4, 4 * V);
-    YG_CUDA(cudaGetLastError());
+    YG_LAUNCHED();
     represent_and_clover(*L);
     YG_CUDA(cudaStreamSynchronize(L->stream));
     tmp.release();
@@ -348,7 +350,7 @@ static void upload_records(Lattice &L, DevBuf &dst, const double *host, int rec,
   if (bytes > L.field_bytes()) { big.alloc(bytes); buf = big.as<double>(); }
   YG_CUDA(cudaMemcpyAsync(buf, host, bytes, cudaMemcpyHostToDevice, L.stream));
   k_aos_to_soa<<<nblk(nrec, 128), 128, 0, L.stream>>>(dst.as<double2>(), buf, L.g, rec, per_site, nrec);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   YG_CUDA(cudaStreamSynchronize(L.stream));
   big.release();
 }
@@ -360,7 +362,7 @@ static void download_records(Lattice &L, double *host, const void *src, int rec,
   double *buf = L.scratch_field(0);
   if (bytes > L.field_bytes()) { big.alloc(bytes); buf = big.as<double>(); }
   k_soa_to_aos<<<nblk(nrec, 128), 128, 0, L.stream>>>(buf, (const double2 *)src, L.g, rec, per_site, nrec);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   YG_CUDA(cudaMemcpyAsync(host, buf, bytes, cudaMemcpyDeviceToHost, L.stream));
   YG_CUDA(cudaStreamSynchronize(L.stream));
   big.release();
@@ -409,13 +411,13 @@ void field_upload(Lattice &L, double *dev, const double *host) {
   double *stage = L.scratch_field(0);
   YG_CUDA(cudaMemcpyAsync(stage, host, L.field_bytes(), cudaMemcpyHostToDevice, L.stream));
   k_spinor_to_dev<<<nblk(L.V, 128), 128, 0, L.stream>>>((double2 *)dev, stage, L.g, L.d);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
 }
 
 void field_download(Lattice &L, double *host, const double *dev) {
   double *stage = L.scratch_field(0);
   k_spinor_to_host<<<nblk(L.V, 128), 128, 0, L.stream>>>(stage, (const double2 *)dev, L.g, L.d);
-  YG_CUDA(cudaGetLastError());
+  YG_LAUNCHED();
   YG_CUDA(cudaMemcpyAsync(host, stage, L.field_bytes(), cudaMemcpyDeviceToHost, L.stream));
   YG_CUDA(cudaStreamSynchronize(L.stream));
 }

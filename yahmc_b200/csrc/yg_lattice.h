@@ -20,6 +20,15 @@ struct Error : std::runtime_error {
 void check_cuda(cudaError_t e, const char *what);
 #define YG_CUDA(x) ::yg::check_cuda((x), #x)
 
+// Kernels launched by this library since load (all lattices).  Every launch site is followed
+// by YG_LAUNCHED(), which checks the launch and counts it; callers are single-threaded.
+extern long g_launch_count;
+#define YG_LAUNCHED()                                              \
+  do {                                                             \
+    ::yg::check_cuda(cudaGetLastError(), "kernel launch");         \
+    ++::yg::g_launch_count;                                        \
+  } while (0)
+
 // Device buffer owned by a lattice.
 struct DevBuf {
   void *p = nullptr;
