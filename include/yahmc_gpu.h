@@ -189,6 +189,16 @@ int yg_clover_logdet_force(yg_lattice *lat, double mass, double residue);       
 int yg_wilson_gauge_force(yg_lattice *lat, double dt, double beta);                                 /* forces.cpp:262-283 */
 int yg_avr_plaquette(yg_lattice *lat, double *out);                                                 /* wilsonloop.cpp:116-133 (1x1) */
 
+/* ---- allocation-free reduction ------------------------------------------ */
+/* No counterpart in the reference.  For callers that cannot allocate device memory (no
+ * lattice handle needed): sum of |a_i|^2 over n_words complex FP64 words at dev_words,
+ * written to the device double *dev_out on the given stream (NULL = legacy default).
+ * Uses a fixed 128 KiB scratch array inside the library instead of cudaMalloc, so
+ * n_words <= 16,777,216 (larger sizes return YG_ERR_ARG).  The first call on a device
+ * looks up that array's device address and should come before any stream capture;
+ * calls that overlap on the GPU share the array and race. */
+int yg_field_sqnorm_noalloc(const double *dev_words, long n_words, double *dev_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -101,6 +101,7 @@ _SIGNATURES = {
     "yg_wilson_fermion_force": [_P, _D, _D, _D, _P, _P], "yg_wilson_fermion_force_q": [_P, _D, _D, _D, _P],
     "yg_clover_fermion_force": [_P, _D, _P, _P], "yg_clover_logdet_force": [_P, _D, _D],
     "yg_wilson_gauge_force": [_P, _D, _D], "yg_avr_plaquette": [_P, _P],
+    "yg_field_sqnorm_noalloc": [_P, ctypes.c_long, _P, _P],
 }
 
 

@@ -9,6 +9,10 @@ using yg::Lattice;
 
 static thread_local std::string g_last_error;
 
+namespace yg {
+void set_last_error(const char *msg) { g_last_error = msg; }
+}
+
 template <typename F>
 static int guard(F &&f) {
   try {
