@@ -53,7 +53,31 @@ def parse():
     ap.add_argument("--seed", type=int, default=20241203)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dslash-iters", type=int, default=50)
+    ap.add_argument("--inner", default="f16-l12", choices=list(INNER),
+                    help="inner operator of the mixed solver: generic FP32, or the compressed d = 3 "
+                         "operator with FP32/FP16 spinors and 18/12-real links")
+    ap.add_argument("--delta", type=float, default=0.1, help="reliable-update threshold")
+    ap.add_argument("--variants", action="store_true", help="also time every inner operator once")
     return ap.parse_args()
+
+
+# inner operator of the mixed-precision solver: None = generic FP32 (every representation),
+# (spinor bits, link reals) = the compressed d = 3 operator
+INNER = {"generic-f32": None, "f32-l18": (32, 18), "f32-l12": (32, 12), "f16-l18": (16, 18), "f16-l12": (16, 12)}
+
+
+DTYPE = {"generic-f32": "f32 inner / f64 reliable updates and residual",
+         "f32-l18": "f32 inner / f64 reliable updates and residual",
+         "f32-l12": "f32 inner (12-real links) / f64 reliable updates and residual",
+         "f16-l18": "f32 inner arithmetic on f16 storage / f64 reliable updates and residual",
+         "f16-l12": "f32 inner arithmetic on f16 storage (12-real links) / f64 reliable updates and residual"}
+
+
+def solve_mixed(lat, x, b, inner, delta):
+    spec = INNER[inner]
+    if spec is None:
+        return lat.cg_mixed("Hphi_sq", MASS, PREC, x, b)
+    return lat.cg_mixed("Hphi_sq", MASS, PREC, x, b, inner_precision=spec[0], link_reals=spec[1], delta=delta)
 
 
 def hbm_peak():
@@ -205,7 +229,7 @@ def run_ours(a, rank, world, dist):
 
     def mixed():
         lat.spinor_zero(x)
-        return lat.cg_mixed("Hphi_sq", MASS, PREC, x, bf)
+        return solve_mixed(lat, x, bf, a.inner, a.delta)
 
     def fp64():
         lat.spinor_zero(x)
@@ -252,12 +276,25 @@ def run_ours(a, rank, world, dist):
     def e2e():
         lat.upload(bf, hb)
         lat.spinor_zero(x)
-        s = lat.cg_mixed("Hphi_sq", MASS, PREC, x, bf)
+        s = solve_mixed(lat, x, bf, a.inner, a.delta)
         lat.download(x, raw=True, out=hx)
         return s
 
     e2e()
     ms_e2e, _ = timed(e2e, a.steps)
+
+    variants = None
+    if a.variants:
+        variants = {}
+        for name in INNER:
+            def one(name=name):
+                lat.spinor_zero(x)
+                return solve_mixed(lat, x, bf, name, a.delta)
+            one()
+            vms, vst = timed(one, 2)
+            variants[name] = {"ms": vms, "iterations": vst[-1]["iterations"],
+                              "reliable_updates": vst[-1]["reliable_updates"], "fallback": vst[-1]["fallback"],
+                              "true_residual": vst[-1]["true_residual"]}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -282,13 +319,13 @@ def run_ours(a, rank, world, dist):
         "metric": "CG time-to-solution (true rel. residual 1e-12), mixed precision",
         "value": value, "unit": "ms", "n_gpus": world, "steps": a.steps, "warmup": max(3, a.warmup),
         "ms_per_step": ms_mixed, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 inner / f64 reliable updates and residual", "data": "synthetic",
+        "dtype": DTYPE[a.inner], "data": "synthetic",
         "config": {"workload": workload_name(a.dims), "mass": MASS, "csw": CSW, "prec_squared": PREC,
                    "links": "random start exp(Gaussian su(3) algebra), seeded",
                    "l2": "inputs larger than L2 (links 604 MB, clover 604 MB), no flush",
                    "parallelism": f"replicas x{world}"},
-        "solver": {"iterations": st["iterations"], "reliable_updates": st["reliable_updates"],
-                   "fallback": st["fallback"], "true_residual": true_res},
+        "solver": {"inner": a.inner, "delta": a.delta, "iterations": st["iterations"],
+                   "reliable_updates": st["reliable_updates"], "fallback": st["fallback"], "true_residual": true_res},
         "fp64_cg": {"ms": ms_fp64, "iterations": it_fp64, "speedup_mixed_vs_fp64": ms_fp64 / ms_mixed},
         "dslash_fp64": {"ms": ms_hop, "GB_s": hop_gbs, "bytes_per_site": bytes_per_site, "sites": V // 2},
         "roofline": {"bound": "hbm", "kernel": "k_hop<3,double,PLAIN> (Dphi_oe, FP64 18-real links)",
@@ -300,6 +337,8 @@ def run_ours(a, rank, world, dist):
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
+    if variants is not None:
+        line["inner_variants"] = variants
     print(json.dumps(line))
 
 

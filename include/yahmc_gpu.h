@@ -175,6 +175,20 @@ int yg_rational_calc(yg_lattice *lat, const yg_inv_par *par, double a0, int orde
  * reliable updates; stops on the TRUE FP64 squared residual |b-Ax|^2 < prec*|b|^2. */
 int yg_cg_mixed(yg_lattice *lat, const yg_inv_par *par, double *x, double *b, yg_solve_stats *stats);
 
+/* No reference counterpart: options of the mixed-precision solver.
+ *   inner_precision  32 (FP32 storage) or 16 (FP16 storage with per-site norms); FP32 arithmetic
+ *   link_reals       18, or 12 (two rows, third rebuilt; SU(3) fundamental only)
+ *   delta            reliable update when |r| falls below delta * |r| at the last update
+ * The compressed inner operator exists for d = 3 representations with even-odd
+ * preconditioning; the stopping test is the true FP64 residual, as for yg_cg_mixed. */
+typedef struct {
+  int inner_precision;
+  int link_reals;
+  double delta;
+} yg_mixed_opts;
+int yg_cg_mixed_opts(yg_lattice *lat, const yg_inv_par *par, const yg_mixed_opts *opts, double *x, double *b,
+                     yg_solve_stats *stats);
+
 /* ---- forces (forces.h:6-15) -------------------------------------------- */
 int yg_momenta_upload(yg_lattice *lat, const double *host);     /* afield_momenta, 4*V suNa */
 int yg_momenta_download(yg_lattice *lat, double *host);

@@ -59,6 +59,10 @@ class InvPar(ctypes.Structure):
                 ("maxiter", ctypes.c_int)]
 
 
+class MixedOpts(ctypes.Structure):
+    _fields_ = [("inner_precision", ctypes.c_int), ("link_reals", ctypes.c_int), ("delta", ctypes.c_double)]
+
+
 class SolveStats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("reliable_updates", ctypes.c_int), ("fallback", ctypes.c_int),
                 ("true_residual", ctypes.c_double), ("seconds", ctypes.c_double)]
@@ -96,6 +100,7 @@ _SIGNATURES = {
     "yg_cg_mshift": [_P, ctypes.POINTER(InvPar), _I, _P, _P, _P, ctypes.POINTER(_I)],
     "yg_rational_calc": [_P, ctypes.POINTER(InvPar), _D, _I, _P, _P, _P, _P, ctypes.POINTER(_I)],
     "yg_cg_mixed": [_P, ctypes.POINTER(InvPar), _P, _P, ctypes.POINTER(SolveStats)],
+    "yg_cg_mixed_opts": [_P, ctypes.POINTER(InvPar), ctypes.POINTER(MixedOpts), _P, _P, ctypes.POINTER(SolveStats)],
     "yg_momenta_upload": [_P, _P], "yg_momenta_download": [_P, _P], "yg_momenta_zero": [_P],
     "yg_clover_force_download": [_P, _P], "yg_begin_fermion_force": [_P], "yg_end_fermion_force": [_P, _D],
     "yg_wilson_fermion_force": [_P, _D, _D, _D, _P, _P], "yg_wilson_fermion_force_q": [_P, _D, _D, _D, _P],
@@ -347,10 +352,17 @@ class Lattice:
                                               x.ptr, b.ptr, ctypes.byref(it)))
         return it.value
 
-    def cg_mixed(self, op, mass, prec, x, b, log=0, maxiter=0):
+    def cg_mixed(self, op, mass, prec, x, b, log=0, maxiter=0, inner_precision=None, link_reals=18, delta=0.1):
+        """Mixed-precision CG (true FP64 stopping criterion).  inner_precision None: the
+        generic FP32 inner operator; 32 or 16: the compressed d = 3 inner operator with
+        link_reals 18 or 12 and reliable-update threshold delta."""
         st = SolveStats()
         par = self._par(op, mass, prec, log, maxiter)
-        rc = self.lib.yg_cg_mixed(self.h, ctypes.byref(par), x.ptr, b.ptr, ctypes.byref(st))
+        if inner_precision is None:
+            rc = self.lib.yg_cg_mixed(self.h, ctypes.byref(par), x.ptr, b.ptr, ctypes.byref(st))
+        else:
+            o = MixedOpts(int(inner_precision), int(link_reals), float(delta))
+            rc = self.lib.yg_cg_mixed_opts(self.h, ctypes.byref(par), ctypes.byref(o), x.ptr, b.ptr, ctypes.byref(st))
         if rc not in (0, 4, 5):
             self._check(rc)
         return {"status": rc, "iterations": st.iterations, "reliable_updates": st.reliable_updates,

@@ -72,7 +72,7 @@ static int red_grid(Lattice &L, long n) {
   return g < L.red_blocks ? g : L.red_blocks;
 }
 
-static double2 finish_reduce(Lattice &L, int grid) {
+double2 reduce_partials(Lattice &L, int grid) {
   k_reduce_final<<<1, 1024, 0, L.stream>>>(L.red_result.as<double2>(), L.red_partial.as<double2>(), grid);
   YG_LAUNCHED();
   YG_CUDA(cudaMemcpyAsync(L.host_result, L.red_result.p, sizeof(double2), cudaMemcpyDeviceToHost, L.stream));
@@ -88,7 +88,7 @@ double blas_sqnorm(Lattice &L, const double *a, long lo, long n) {
   int grid = red_grid(L, cnt);
   k_reduce<0><<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (const double2 *)a + woff(L, lo), nullptr, cnt);
   YG_LAUNCHED();
-  return finish_reduce(L, grid).x;
+  return reduce_partials(L, grid).x;
 }
 
 double2 blas_product(Lattice &L, const double *a, const double *b, long lo, long n) {
@@ -97,7 +97,7 @@ double2 blas_product(Lattice &L, const double *a, const double *b, long lo, long
   k_reduce<1><<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (const double2 *)a + woff(L, lo),
                                            (const double2 *)b + woff(L, lo), cnt);
   YG_LAUNCHED();
-  return finish_reduce(L, grid);
+  return reduce_partials(L, grid);
 }
 
 double blas_product_re(Lattice &L, const double *a, const double *b, long lo, long n) {
@@ -106,7 +106,7 @@ double blas_product_re(Lattice &L, const double *a, const double *b, long lo, lo
   k_reduce<2><<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (const double2 *)a + woff(L, lo),
                                            (const double2 *)b + woff(L, lo), cnt);
   YG_LAUNCHED();
-  return finish_reduce(L, grid).x;
+  return reduce_partials(L, grid).x;
 }
 
 // lhs = alpha*lhs + beta*rhs  (alpha == 0 does not read lhs; rhs == null drops the term)
@@ -187,7 +187,7 @@ double blas_cg_update(Lattice &L, double *x, double *r, const double *p, const d
   k_cg_update<<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (double2 *)x + o, (double2 *)r + o,
                                            (const double2 *)p + o, (const double2 *)q + o, a, cnt);
   YG_LAUNCHED();
-  return finish_reduce(L, grid).x;
+  return reduce_partials(L, grid).x;
 }
 
 // sum of n doubles (per-site partials of logdet / plaquette), deterministic
@@ -202,7 +202,7 @@ double sum_device(Lattice &L, const double *v, long n) {
   int grid = red_grid(L, n);
   k_sum_partial<<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), v, n);
   YG_LAUNCHED();
-  return finish_reduce(L, grid).x;
+  return reduce_partials(L, grid).x;
 }
 
 // ---------------------------------------------------------------- FP32 helpers (mixed solver)
@@ -278,14 +278,14 @@ double f_sqnorm(Lattice &L, const float *a, long cnt) {
   int grid = red_grid(L, cnt);
   k_reduce_f<0><<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (const float2 *)a, nullptr, cnt);
   YG_LAUNCHED();
-  return finish_reduce(L, grid).x;
+  return reduce_partials(L, grid).x;
 }
 
 double f_product_re(Lattice &L, const float *a, const float *b, long cnt) {
   int grid = red_grid(L, cnt);
   k_reduce_f<2><<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (const float2 *)a, (const float2 *)b, cnt);
   YG_LAUNCHED();
-  return finish_reduce(L, grid).x;
+  return reduce_partials(L, grid).x;
 }
 
 double f_cg_update(Lattice &L, float *x, float *r, const float *p, const float *q, float a, long cnt) {
@@ -293,7 +293,7 @@ double f_cg_update(Lattice &L, float *x, float *r, const float *p, const float *
   k_cg_update_f<<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (float2 *)x, (float2 *)r,
                                              (const float2 *)p, (const float2 *)q, a, cnt);
   YG_LAUNCHED();
-  return finish_reduce(L, grid).x;
+  return reduce_partials(L, grid).x;
 }
 
 void f_xpay(Lattice &L, float *p, float b, const float *r, long cnt) {

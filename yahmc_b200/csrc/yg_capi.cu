@@ -238,6 +238,13 @@ int yg_rational_calc(yg_lattice *l, const yg_inv_par *p, double a0, int order, c
     return yg::rational_calc(lat(l), *p, a0, order, poles, residues, x, b, it);
   });
 }
+int yg_cg_mixed_opts(yg_lattice *l, const yg_inv_par *p, const yg_mixed_opts *o, double *x, double *b,
+                     yg_solve_stats *st) {
+  return guard_status([&] {
+    check_par(p); need(o, "opts"); need(x, "x"); need(b, "b");
+    return yg::cg_mixed_sloppy(lat(l), *p, o->inner_precision, o->link_reals, o->delta, x, b, st);
+  });
+}
 int yg_cg_mixed(yg_lattice *l, const yg_inv_par *p, double *x, double *b, yg_solve_stats *st) {
   return guard_status([&] { check_par(p); need(x, "x"); need(b, "b"); return yg::cg_mixed(lat(l), *p, x, b, st); });
 }

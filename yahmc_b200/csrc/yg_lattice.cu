@@ -43,7 +43,7 @@ Lattice::~Lattice() {
   for (double *s : scratch) if (s) cudaFree(s);
   if (host_result) cudaFreeHost(host_result);
   for (DevBuf *b : {&fund, &links, &clover, &ldl, &cl_force, &mom, &tables, &red_partial, &red_result, &links_f,
-                    &clover_f, &cinv_f})
+                    &clover_f, &cinv_f, &sl_links, &sl_clover})
     b->release();
 }
 
@@ -237,6 +237,7 @@ void represent_and_clover(Lattice &L) {
   L.ldl_valid = false;          // cl_sigma = 0xF00F, clover.cpp:337
   L.cinv_f_valid = false;
   L.links_f_valid = false;
+  L.sl_valid = false;
 }
 
 void ensure_ldl(Lattice &L, double sigma) {

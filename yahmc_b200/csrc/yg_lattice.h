@@ -82,6 +82,13 @@ struct Lattice {
   bool links_f_valid = false;
   bool cinv_f_valid = false;
 
+  // compressed inner operator of the mixed solver for d = 3 (yg_sloppy.cu)
+  DevBuf sl_links;  // 12 or 18 reals per link, FP32 or FP16
+  DevBuf sl_clover; // packed Hermitian blocks: M_e on even sites, M_o^-1 on odd sites
+  int sl_prec = 0, sl_reals = 0;
+  double sl_mass = 0;
+  bool sl_valid = false;
+
   long field_doubles() const { return 8L * d * V; }
   size_t field_bytes() const { return sizeof(double) * field_doubles(); }
 
@@ -133,6 +140,8 @@ void blas_zero(Lattice &L, double *f, long lo, long n);
 // fused CG update: x += a p ; r -= a q ; return |r|^2
 double blas_cg_update(Lattice &L, double *x, double *r, const double *p, const double *q, double a, long lo, long n);
 double sum_device(Lattice &L, const double *v, long n);
+// sum the first `grid` double2 partials in L.red_partial (deterministic), to the host
+double2 reduce_partials(Lattice &L, int grid);
 // FP32 helpers of the mixed-precision solver (counts in complex words)
 void f_from_d(Lattice &L, float *dst, const double *src, long cnt);
 void d_add_f(Lattice &L, double *dst, const float *src, long cnt);
@@ -150,6 +159,8 @@ int auto_inverter(Lattice &L, const yg_inv_par &par, double *x, double *b, int *
 int rational_calc(Lattice &L, const yg_inv_par &par, double a0, int order, const double *poles,
                   const double *residues, double *x, double *b, int *iters);
 int cg_mixed(Lattice &L, const yg_inv_par &par, double *x, double *b, yg_solve_stats *st);
+int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, double delta, double *x, double *b,
+                    yg_solve_stats *st);
 
 // ---- yg_forces.cu
 void clover_fermion_force(Lattice &L, double residue, double *lhs, double *rhs);

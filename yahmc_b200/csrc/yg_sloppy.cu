@@ -1,0 +1,733 @@
+// Inner ("sloppy") operator of the mixed-precision solver for d = 3 representations.
+//
+// The FP64 engine (yg_dirac.cu) keeps the reference's layouts and arithmetic; the inner
+// iterations of cg_mixed only need an approximation of the same operator, so they read
+// compressed copies built once per gauge field and mass:
+//   * spinors in FP32 (2 complex per 16-byte word) or FP16 (4 complex per 16-byte word,
+//     scaled by a per-site FP32 norm = max |component|);
+//   * links with 18 reals (9 complex) or, for SU(3) fundamental, 12 reals (rows 0 and 1;
+//     row 2 = conj(row0 x row1), times the antiperiodic sign the stored rows carry);
+//   * the clover term as two packed Hermitian 6x6 blocks per site (6 real diagonal entries
+//     + 15 complex lower-triangle entries each): M_e = (4+m+cf) + A on even sites and the
+//     explicit inverse M_o^-1 on odd sites, so that the Schur operator of dirac.cpp:738-751
+//     is   t_o = M_o^-1 (1/2 H psi_e),   out_e = gamma5 (M_e psi_e - 1/2 H t_o).
+//     Without a clover term M_o^-1 = 1 and M_e = (4+m)^2 (dirac.cpp:755-765).
+// Arithmetic is FP32 throughout; FP16 is a storage format only.
+#include <cuda_fp16.h>
+#include "yg_lattice.h"
+#include "yg_kernels.h"
+
+namespace yg {
+
+// ------------------------------------------------------------------ storage formats
+// Spinor word w of site (blk, h): FP32 -> float4 F[(blk*6 + w)*Vh + h], 6 words, complex 2w, 2w+1
+//                                 FP16 -> uint4  F[(blk*3 + w)*Vh + h], 3 words, complex 4w..4w+3
+// complex index k = spin*3 + colour (as the FP64 layout)
+template <int P> struct SpinorFmt;
+template <> struct SpinorFmt<32> {
+  using word = float4;
+  static constexpr int words = 6;
+};
+template <> struct SpinorFmt<16> {
+  using word = uint4;
+  static constexpr int words = 3;
+};
+
+__device__ __forceinline__ float2 h2f(unsigned v) {
+  __half2 h = *reinterpret_cast<__half2 *>(&v);
+  return __half22float2(h);
+}
+__device__ __forceinline__ unsigned f2h(float2 f) {
+  __half2 h = __float22half2_rn(f);
+  return *reinterpret_cast<unsigned *>(&h);
+}
+
+template <int P>
+__device__ __forceinline__ void sload(float2 (&s)[12], const void *base, const float *norm, int blk, int h, int Vh) {
+  if (P == 32) {
+    const float4 *f = reinterpret_cast<const float4 *>(base);
+#pragma unroll
+    for (int w = 0; w < 6; w++) {
+      float4 v = __ldg(f + (long)(blk * 6 + w) * Vh + h);
+      s[2 * w] = make_float2(v.x, v.y);
+      s[2 * w + 1] = make_float2(v.z, v.w);
+    }
+  } else {
+    const uint4 *f = reinterpret_cast<const uint4 *>(base);
+    float n = __ldg(norm + (long)blk * Vh + h);
+#pragma unroll
+    for (int w = 0; w < 3; w++) {
+      uint4 v = __ldg(f + (long)(blk * 3 + w) * Vh + h);
+      float2 a = h2f(v.x), b = h2f(v.y), c = h2f(v.z), d = h2f(v.w);
+      s[4 * w + 0] = make_float2(a.x * n, a.y * n);
+      s[4 * w + 1] = make_float2(b.x * n, b.y * n);
+      s[4 * w + 2] = make_float2(c.x * n, c.y * n);
+      s[4 * w + 3] = make_float2(d.x * n, d.y * n);
+    }
+  }
+}
+
+template <int P>
+__device__ __forceinline__ void sstore(void *base, float *norm, const float2 (&s)[12], int blk, int h, int Vh) {
+  if (P == 32) {
+    float4 *f = reinterpret_cast<float4 *>(base);
+#pragma unroll
+    for (int w = 0; w < 6; w++)
+      f[(long)(blk * 6 + w) * Vh + h] = make_float4(s[2 * w].x, s[2 * w].y, s[2 * w + 1].x, s[2 * w + 1].y);
+  } else {
+    float m = 0.f;
+#pragma unroll
+    for (int k = 0; k < 12; k++) m = fmaxf(m, fmaxf(fabsf(s[k].x), fabsf(s[k].y)));
+    float inv = m > 0.f ? 1.f / m : 0.f;
+    uint4 *f = reinterpret_cast<uint4 *>(base);
+#pragma unroll
+    for (int w = 0; w < 3; w++) {
+      uint4 v;
+      v.x = f2h(make_float2(s[4 * w].x * inv, s[4 * w].y * inv));
+      v.y = f2h(make_float2(s[4 * w + 1].x * inv, s[4 * w + 1].y * inv));
+      v.z = f2h(make_float2(s[4 * w + 2].x * inv, s[4 * w + 2].y * inv));
+      v.w = f2h(make_float2(s[4 * w + 3].x * inv, s[4 * w + 3].y * inv));
+      f[(long)(blk * 3 + w) * Vh + h] = v;
+    }
+    norm[(long)blk * Vh + h] = m;
+  }
+}
+
+// Links: complex word k of link (site blk,h ; mu): FP32 float2 / FP16 half2 at
+//   U[((blk*4 + mu)*K + k)*Vh + h], K = 9 (18 reals, row-major) or 6 (rows 0,1)
+template <int P>
+__device__ __forceinline__ float2 lload(const void *base, long i) {
+  if (P == 32) return __ldg(reinterpret_cast<const float2 *>(base) + i);
+  unsigned v = __ldg(reinterpret_cast<const unsigned *>(base) + i);
+  return h2f(v);
+}
+
+template <int P, int K>
+__device__ __forceinline__ void link_load(float2 (&u)[9], const void *U, int blk, int h, int Vh, int mu, float sgn) {
+#pragma unroll
+  for (int k = 0; k < K; k++) u[k] = lload<P>(U, ((long)(blk * 4 + mu) * K + k) * Vh + h);
+  if (K == 6) {
+    // row 2 = conj(row0 x row1); the stored rows carry the antiperiodic sign s, and
+    // (s r0) x (s r1) = r0 x r1, so the reconstructed row is multiplied by s again
+    float2 a0 = u[0], a1 = u[1], a2 = u[2], b0 = u[3], b1 = u[4], b2 = u[5];
+    u[6] = cscale(cconj(csub(cmul(a1, b2), cmul(a2, b1))), sgn);
+    u[7] = cscale(cconj(csub(cmul(a2, b0), cmul(a0, b2))), sgn);
+    u[8] = cscale(cconj(csub(cmul(a0, b1), cmul(a1, b0))), sgn);
+  }
+}
+
+// Packed Hermitian blocks: 72 reals per site (block b: 6 diagonal reals, then the 15
+// complex lower-triangle entries (1,0),(2,0),(2,1),...,(5,4)), FP32 as 18 float4 / FP16 as
+// 9 uint4 at C[(blk*W + w)*Vh + h].
+template <int P>
+__device__ __forceinline__ void cload(float (&c)[72], const void *base, int blk, int h, int Vh) {
+  if (P == 32) {
+    const float4 *f = reinterpret_cast<const float4 *>(base);
+#pragma unroll
+    for (int w = 0; w < 18; w++) {
+      float4 v = __ldg(f + (long)(blk * 18 + w) * Vh + h);
+      c[4 * w] = v.x; c[4 * w + 1] = v.y; c[4 * w + 2] = v.z; c[4 * w + 3] = v.w;
+    }
+  } else {
+    const uint4 *f = reinterpret_cast<const uint4 *>(base);
+#pragma unroll
+    for (int w = 0; w < 9; w++) {
+      uint4 v = __ldg(f + (long)(blk * 9 + w) * Vh + h);
+      float2 a = h2f(v.x), b = h2f(v.y), cc = h2f(v.z), d = h2f(v.w);
+      c[8 * w + 0] = a.x; c[8 * w + 1] = a.y; c[8 * w + 2] = b.x; c[8 * w + 3] = b.y;
+      c[8 * w + 4] = cc.x; c[8 * w + 5] = cc.y; c[8 * w + 6] = d.x; c[8 * w + 7] = d.y;
+    }
+  }
+}
+
+// y = M x for the Hermitian 6x6 block b of a packed site record
+__device__ __forceinline__ void herm_apply(float2 (&y)[6], const float *c, const float2 (&x)[6]) {
+#pragma unroll
+  for (int i = 0; i < 6; i++) y[i] = cscale(x[i], c[i]);
+  int k = 6;
+#pragma unroll
+  for (int i = 1; i < 6; i++)
+#pragma unroll
+    for (int j = 0; j < i; j++, k += 2) {
+      float2 m = make_float2(c[k], c[k + 1]);      // M[i][j], and M[j][i] = conj(M[i][j])
+      cfma(y[i], m, x[j]);
+      cfmac(y[j], m, x[i]);
+    }
+}
+
+// apply both blocks: spins (0,1) use block 0, spins (2,3) block 1
+__device__ __forceinline__ void clover_packed(float2 (&out)[12], const float (&c)[72], const float2 (&s)[12]) {
+#pragma unroll
+  for (int b = 0; b < 2; b++) {
+    float2 x[6], y[6];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      x[i] = s[(2 * b) * 3 + i];
+      x[i + 3] = s[(2 * b + 1) * 3 + i];
+    }
+    herm_apply(y, c + 36 * b, x);
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      out[(2 * b) * 3 + i] = y[i];
+      out[(2 * b + 1) * 3 + i] = y[i + 3];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ the sloppy hop
+struct SHopArgs {
+  Geom g;
+  const void *src;          // hop input (sloppy spinor)
+  const float *src_norm;
+  const void *src2;         // STEP2: psi_e for the clover term
+  const float *src2_norm;
+  void *dst;
+  float *dst_norm;
+  const void *U;            // sloppy links
+  const void *C;            // packed clover blocks
+  float coeff;              // +1/2 (step 1) or -1/2 (step 2)
+  int lo, n;                // output sites [lo, lo+n): the odd block (step 1) or even (step 2)
+};
+
+// one direction: SIG = -1 forward (1 - gamma_mu), +1 backward (1 + gamma_mu); as hop_dir
+// in yg_dirac_impl.cuh (dirac.cpp:258-697)
+template <int P, int K, int MU, int SIG>
+__device__ __forceinline__ void shop_dir(float2 (&acc)[12], const SHopArgs &a, int nid, int lid, int lt) {
+  const Geom &g = a.g;
+  float2 p[12];
+  int nb = nid >= g.Vh, nh = nid - nb * g.Vh;
+  sload<P>(p, a.src, a.src_norm, nb, nh, g.Vh);
+  float2 hh[2][3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    float2 p0 = p[c], p1 = p[3 + c], p2 = p[6 + c], p3 = p[9 + c];
+    if (MU == 0) {
+      hh[0][c] = SIG < 0 ? cadd(p0, p2) : csub(p0, p2);
+      hh[1][c] = SIG < 0 ? cadd(p1, p3) : csub(p1, p3);
+    } else if (MU == 1) {
+      hh[0][c] = SIG < 0 ? cadd(p0, ctimesi(p3)) : csub(p0, ctimesi(p3));
+      hh[1][c] = SIG < 0 ? cadd(p1, ctimesi(p2)) : csub(p1, ctimesi(p2));
+    } else if (MU == 2) {
+      hh[0][c] = SIG < 0 ? cadd(p0, p3) : csub(p0, p3);
+      hh[1][c] = SIG < 0 ? csub(p1, p2) : cadd(p1, p2);
+    } else {
+      hh[0][c] = SIG < 0 ? cadd(p0, ctimesi(p2)) : csub(p0, ctimesi(p2));
+      hh[1][c] = SIG < 0 ? csub(p1, ctimesi(p3)) : cadd(p1, ctimesi(p3));
+    }
+  }
+  int lb = lid >= g.Vh, lh = lid - lb * g.Vh;
+  float sgn = (g.bc == YG_BC_ANTIPERIODIC && MU == 0 && lt == 0) ? -1.f : 1.f;
+  float2 u[9];
+  link_load<P, K>(u, a.U, lb, lh, g.Vh, MU, sgn);
+  float2 chi[2][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    float2 s0 = make_float2(0.f, 0.f), s1 = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      if (SIG > 0) { cfmac(s0, u[j * 3 + i], hh[0][j]); cfmac(s1, u[j * 3 + i], hh[1][j]); }
+      else { cfma(s0, u[i * 3 + j], hh[0][j]); cfma(s1, u[i * 3 + j], hh[1][j]); }
+    }
+    chi[0][i] = s0;
+    chi[1][i] = s1;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    acc[c] = cadd(acc[c], chi[0][c]);
+    acc[3 + c] = cadd(acc[3 + c], chi[1][c]);
+    if (MU == 0) {
+      acc[6 + c] = SIG < 0 ? cadd(acc[6 + c], chi[0][c]) : csub(acc[6 + c], chi[0][c]);
+      acc[9 + c] = SIG < 0 ? cadd(acc[9 + c], chi[1][c]) : csub(acc[9 + c], chi[1][c]);
+    } else if (MU == 1) {
+      acc[6 + c] = SIG < 0 ? cadd(acc[6 + c], ctimesmi(chi[1][c])) : cadd(acc[6 + c], ctimesi(chi[1][c]));
+      acc[9 + c] = SIG < 0 ? cadd(acc[9 + c], ctimesmi(chi[0][c])) : cadd(acc[9 + c], ctimesi(chi[0][c]));
+    } else if (MU == 2) {
+      acc[6 + c] = SIG < 0 ? csub(acc[6 + c], chi[1][c]) : cadd(acc[6 + c], chi[1][c]);
+      acc[9 + c] = SIG < 0 ? cadd(acc[9 + c], chi[0][c]) : csub(acc[9 + c], chi[0][c]);
+    } else {
+      acc[6 + c] = SIG < 0 ? cadd(acc[6 + c], ctimesmi(chi[0][c])) : cadd(acc[6 + c], ctimesi(chi[0][c]));
+      acc[9 + c] = SIG < 0 ? cadd(acc[9 + c], ctimesi(chi[1][c])) : cadd(acc[9 + c], ctimesmi(chi[1][c]));
+    }
+  }
+}
+
+// STEP 1 (odd output):  dst = M_o^-1 (coeff * hop(src))
+// STEP 2 (even output): dst = gamma5 (M_e src2 + coeff * hop(src))
+template <int P, int K, int STEP>
+__global__ void __launch_bounds__(128) k_shop(SHopArgs a) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  const Geom &g = a.g;
+  int id = a.lo + t;
+  int c[4];
+  coords_of(g, id, c);
+  int T = g.dim[0];
+  float2 acc[12];
+#pragma unroll
+  for (int k = 0; k < 12; k++) acc[k] = make_float2(0.f, 0.f);
+  int f, b;
+  f = neighbour(g, c, 0, +1); shop_dir<P, K, 0, -1>(acc, a, f, id, c[0]);
+  b = neighbour(g, c, 0, -1); shop_dir<P, K, 0, +1>(acc, a, b, b, c[0] == 0 ? T - 1 : c[0] - 1);
+  f = neighbour(g, c, 1, +1); shop_dir<P, K, 1, -1>(acc, a, f, id, c[0]);
+  b = neighbour(g, c, 1, -1); shop_dir<P, K, 1, +1>(acc, a, b, b, c[0]);
+  f = neighbour(g, c, 2, +1); shop_dir<P, K, 2, -1>(acc, a, f, id, c[0]);
+  b = neighbour(g, c, 2, -1); shop_dir<P, K, 2, +1>(acc, a, b, b, c[0]);
+  f = neighbour(g, c, 3, +1); shop_dir<P, K, 3, -1>(acc, a, f, id, c[0]);
+  b = neighbour(g, c, 3, -1); shop_dir<P, K, 3, +1>(acc, a, b, b, c[0]);
+  int blk = id >= g.Vh, h = id - blk * g.Vh;
+  float2 out[12];
+  bool bnd = spinor_zeroed(g, c[0]);
+  float cl[72];
+  cload<P>(cl, a.C, blk, h, g.Vh);
+  if (STEP == 1) {
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc[k] = cscale(acc[k], a.coeff);
+    clover_packed(out, cl, acc);
+  } else {
+    float2 s2[12];
+    sload<P>(s2, a.src2, a.src2_norm, blk, h, g.Vh);
+    clover_packed(out, cl, s2);
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+      out[k] = cadd(out[k], cscale(acc[k], a.coeff));
+      if (k >= 6) out[k] = cscale(out[k], -1.f);            // gamma5
+    }
+  }
+  if (bnd) {
+#pragma unroll
+    for (int k = 0; k < 12; k++) out[k] = make_float2(0.f, 0.f);
+  }
+  sstore<P>(a.dst, a.dst_norm, out, blk, h, g.Vh);
+}
+
+// ------------------------------------------------------------------ builds (once per gauge field / mass)
+template <int P>
+__device__ __forceinline__ void lstore(void *base, long i, double2 v) {
+  if (P == 32) reinterpret_cast<float2 *>(base)[i] = make_float2((float)v.x, (float)v.y);
+  else reinterpret_cast<unsigned *>(base)[i] = f2h(make_float2((float)v.x, (float)v.y));
+}
+
+// links: the first K complex entries (row-major) of each FP64 represented link
+template <int P, int K>
+__global__ void k_pack_links(void *dst, const double2 *links, Geom g) {
+  long r = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (r >= 4L * g.V) return;
+  int id = (int)(r >> 2), mu = (int)(r & 3);
+  int blk = id >= g.Vh, h = id - blk * g.Vh;
+  for (int k = 0; k < K; k++)
+    lstore<P>(dst, ((long)(blk * 4 + mu) * K + k) * g.Vh + h, links[fidx(g, id, mu * 9 + k, 36)]);
+}
+
+template <int P>
+__device__ __forceinline__ void cstore(void *base, const float (&c)[72], int blk, int h, int Vh) {
+  if (P == 32) {
+    float4 *f = reinterpret_cast<float4 *>(base);
+    for (int w = 0; w < 18; w++)
+      f[(long)(blk * 18 + w) * Vh + h] = make_float4(c[4 * w], c[4 * w + 1], c[4 * w + 2], c[4 * w + 3]);
+  } else {
+    uint4 *f = reinterpret_cast<uint4 *>(base);
+    for (int w = 0; w < 9; w++) {
+      uint4 v;
+      v.x = f2h(make_float2(c[8 * w], c[8 * w + 1]));
+      v.y = f2h(make_float2(c[8 * w + 2], c[8 * w + 3]));
+      v.z = f2h(make_float2(c[8 * w + 4], c[8 * w + 5]));
+      v.w = f2h(make_float2(c[8 * w + 6], c[8 * w + 7]));
+      f[(long)(blk * 9 + w) * Vh + h] = v;
+    }
+  }
+}
+
+// pack a Hermitian 6x6 block (full matrix M in double2) into 36 reals at c
+__device__ __forceinline__ void pack_block(float *c, const double2 (&M)[36]) {
+  for (int i = 0; i < 6; i++) c[i] = (float)M[i * 6 + i].x;
+  int k = 6;
+  for (int i = 1; i < 6; i++)
+    for (int j = 0; j < i; j++, k += 2) {
+      c[k] = (float)M[i * 6 + j].x;
+      c[k + 1] = (float)M[i * 6 + j].y;
+    }
+}
+
+// even sites: M_e = diag + [[A0,A1],[A1^dag,-A0]] (+) [[A2,A3],[A3^dag,-A2]] (clover_kernel,
+// dirac.cpp:25-107) with diag = 4+m+cf(t); without a clover term, diag = (4+m)^2 alone
+template <int P>
+__global__ void k_pack_clover_even(void *dst, const double2 *cl, Geom g, double diag, double cfm1, int clover) {
+  int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= g.Vh) return;
+  int id = h;
+  int c4[4];
+  coords_of(g, id, c4);
+  double dg = diag + ((clover && (c4[0] == g.Ta || c4[0] == g.Tb)) ? cfm1 : 0.0);
+  float c[72];
+  for (int b = 0; b < 2; b++) {
+    double2 M[36];
+    for (int k = 0; k < 36; k++) M[k] = make_double2(0, 0);
+    for (int i = 0; i < 6; i++) M[i * 6 + i].x = dg;
+    if (clover) {
+      int m0 = 2 * b, m1 = 2 * b + 1;
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+          double2 a0 = cl[fidx(g, id, m0 * 9 + i * 3 + j, 36)];
+          double2 a1 = cl[fidx(g, id, m1 * 9 + i * 3 + j, 36)];
+          M[i * 6 + j] = cadd(M[i * 6 + j], a0);
+          M[(i + 3) * 6 + (j + 3)] = csub(M[(i + 3) * 6 + (j + 3)], a0);
+          M[i * 6 + (j + 3)] = a1;
+          M[(j + 3) * 6 + i] = cconj(a1);
+        }
+    }
+    pack_block(c + 36 * b, M);
+  }
+  cstore<P>(dst, c, 0, h, g.Vh);
+}
+
+// odd sites: the explicit inverse M_o^-1 from the FP64 LDL factors (identity without clover)
+template <int P>
+__global__ void k_pack_clover_odd(void *dst, const double2 *ldl, Geom g, int clover) {
+  int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= g.Vh) return;
+  constexpr int N = 6, Pk = 21;
+  float c[72];
+  for (int b = 0; b < 2; b++) {
+    double2 M[36];
+    for (int k = 0; k < 36; k++) M[k] = make_double2(0, 0);
+    if (!clover) {
+      for (int i = 0; i < 6; i++) M[i * 6 + i].x = 1.0;
+    } else {
+      const double2 *Lb = ldl + (long)b * Pk * g.Vh + h;
+      for (int col = 0; col < N; col++) {
+        double2 x[N];
+        for (int i = 0; i < N; i++) x[i] = make_double2(i == col ? 1.0 : 0.0, 0.0);
+        for (int i = 1; i < N; i++)
+          for (int k = 0; k < i; k++) x[i] = csub(x[i], cmul(Lb[(long)(i * (i + 1) / 2 + k) * g.Vh], x[k]));
+        for (int i = N - 1; i >= 0; i--) {
+          x[i] = cscale(x[i], 1.0 / Lb[(long)(i * (i + 1) / 2 + i) * g.Vh].x);
+          for (int k = i + 1; k < N; k++) x[i] = csub(x[i], cmulc(Lb[(long)(k * (k + 1) / 2 + i) * g.Vh], x[k]));
+        }
+        for (int i = 0; i < N; i++) M[i * 6 + col] = x[i];
+      }
+    }
+    pack_block(c + 36 * b, M);
+  }
+  cstore<P>(dst, c, 1, h, g.Vh);
+}
+
+// ------------------------------------------------------------------ sloppy vector kernels
+// FP32 vectors x, r use the FP64 field order (complex k = spin*3+colour at [k*Vh + h],
+// even block); sloppy vectors p, q use the formats above.
+
+__device__ __forceinline__ double block_sum_d(double v) {
+  __shared__ double sh[8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  v = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+  if (w == 0) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  return v;
+}
+
+// sloppy <- FP64 block 0 (even sites)
+template <int P>
+__global__ void __launch_bounds__(256) k_s_from_d(void *dst, float *dn, const double2 *src, int Vh) {
+  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += gridDim.x * blockDim.x) {
+    float2 s[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+      double2 v = src[(long)k * Vh + h];
+      s[k] = make_float2((float)v.x, (float)v.y);
+    }
+    sstore<P>(dst, dn, s, 0, h, Vh);
+  }
+}
+
+// partial Re <p, q> over the even block
+template <int P>
+__global__ void __launch_bounds__(256) k_s_dot(double2 *partial, const void *p, const float *pn, const void *q,
+                                               const float *qn, int Vh) {
+  double acc = 0.0;
+  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += gridDim.x * blockDim.x) {
+    float2 a[12], b[12];
+    sload<P>(a, p, pn, 0, h, Vh);
+    sload<P>(b, q, qn, 0, h, Vh);
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 12; k++) s += a[k].x * b[k].x + a[k].y * b[k].y;
+    acc += s;
+  }
+  acc = block_sum_d(acc);
+  if (threadIdx.x == 0) partial[blockIdx.x] = make_double2(acc, 0.0);
+}
+
+// x += a p ; r -= a q ; partial |r|^2
+template <int P>
+__global__ void __launch_bounds__(256) k_s_cg_update(double2 *partial, float2 *x, float2 *r, const void *p,
+                                                     const float *pn, const void *q, const float *qn, float a, int Vh) {
+  double acc = 0.0;
+  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += gridDim.x * blockDim.x) {
+    float2 pp[12], qq[12];
+    sload<P>(pp, p, pn, 0, h, Vh);
+    sload<P>(qq, q, qn, 0, h, Vh);
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+      long i = (long)k * Vh + h;
+      float2 xi = x[i], ri = r[i];
+      xi.x = fmaf(a, pp[k].x, xi.x);
+      xi.y = fmaf(a, pp[k].y, xi.y);
+      ri.x = fmaf(-a, qq[k].x, ri.x);
+      ri.y = fmaf(-a, qq[k].y, ri.y);
+      x[i] = xi;
+      r[i] = ri;
+      s += ri.x * ri.x + ri.y * ri.y;
+    }
+    acc += s;
+  }
+  acc = block_sum_d(acc);
+  if (threadIdx.x == 0) partial[blockIdx.x] = make_double2(acc, 0.0);
+}
+
+// p = r + b p
+template <int P>
+__global__ void __launch_bounds__(256) k_s_xpay(void *p, float *pn, float b, const float2 *r, int Vh) {
+  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += gridDim.x * blockDim.x) {
+    float2 pp[12];
+    sload<P>(pp, p, pn, 0, h, Vh);
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+      float2 ri = r[(long)k * Vh + h];
+      pp[k] = make_float2(fmaf(b, pp[k].x, ri.x), fmaf(b, pp[k].y, ri.y));
+    }
+    sstore<P>(p, pn, pp, 0, h, Vh);
+  }
+}
+
+// ------------------------------------------------------------------ host side
+// sloppy fields live in the lattice's scratch fields (each one FP64 field in size, which
+// holds a sloppy spinor plus its norms: FP32 96 B/site, FP16 48 + 4 B/site)
+struct SField {
+  void *data;
+  float *norm;
+};
+
+static SField sfield(Lattice &L, int slot) {
+  char *base = reinterpret_cast<char *>(L.scratch_field(slot));
+  SField f;
+  f.data = base;
+  f.norm = reinterpret_cast<float *>(base + (size_t)L.V * 96);   // after the largest (FP32) payload
+  return f;
+}
+
+static int sgrid(long n) {
+  long g = (n + 255) / 256;
+  const long cap = 148 * 16;
+  return (int)(g < cap ? g : cap);
+}
+
+#define YG_SLOPPY_DISPATCH(P_, K_, ...)                                                      \
+  do {                                                                                       \
+    if (P_ == 32 && K_ == 12) { constexpr int SP = 32, SK = 6; __VA_ARGS__; }                \
+    else if (P_ == 32 && K_ == 18) { constexpr int SP = 32, SK = 9; __VA_ARGS__; }           \
+    else if (P_ == 16 && K_ == 12) { constexpr int SP = 16, SK = 6; __VA_ARGS__; }           \
+    else if (P_ == 16 && K_ == 18) { constexpr int SP = 16, SK = 9; __VA_ARGS__; }           \
+    else throw Error(YG_ERR_ARG, "inner precision must be 32 or 16 and link reals 18 or 12"); \
+  } while (0)
+
+void ensure_sloppy(Lattice &L, double mass, int prec, int reals) {
+  if ((prec != 32 && prec != 16) || (reals != 18 && reals != 12))
+    throw Error(YG_ERR_ARG, "inner precision must be 32 or 16 and link reals 18 or 12");
+  if (L.d != 3) throw Error(YG_ERR_ARG, "the compressed inner operator exists for d = 3 representations");
+  if (reals == 12 && !(L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL))
+    throw Error(YG_ERR_ARG, "12-real links need SU(3) fundamental links");
+  if (!L.p.eo) throw Error(YG_ERR_ARG, "the mixed-precision solver needs even-odd preconditioning");
+  if (L.sl_valid && L.sl_prec == prec && L.sl_reals == reals && L.sl_mass == mass) return;
+  size_t esz = prec == 32 ? 4 : 2;
+  int K = reals / 2;
+  L.sl_links.alloc(esz * 2 * K * 4 * (size_t)L.V);
+  L.sl_clover.alloc(esz * 72 * (size_t)L.V);
+  if (L.p.clover) ensure_ldl(L, 4.0 + mass);
+  int clover = L.p.clover ? 1 : 0;
+  double diag = clover ? 4.0 + mass : (4.0 + mass) * (4.0 + mass);
+  YG_SLOPPY_DISPATCH(prec, reals, {
+    k_pack_links<SP, SK><<<nblk(4 * L.V, 128), 128, 0, L.stream>>>(L.sl_links.p, L.links.as<double2>(), L.g);
+    YG_LAUNCHED();
+    k_pack_clover_even<SP><<<nblk(L.Vh, 64), 64, 0, L.stream>>>(L.sl_clover.p, L.clover.as<double2>(), L.g, diag,
+                                                                 L.p.cf - 1.0, clover);
+    YG_LAUNCHED();
+    k_pack_clover_odd<SP><<<nblk(L.Vh, 64), 64, 0, L.stream>>>(L.sl_clover.p, L.ldl.as<double2>(), L.g, clover);
+    YG_LAUNCHED();
+  });
+  L.sl_prec = prec;
+  L.sl_reals = reals;
+  L.sl_mass = mass;
+  L.sl_valid = true;
+}
+
+// dst = Hphi(src) with the compressed operator; tmp receives the odd-site intermediate
+static void sloppy_hphi(Lattice &L, SField dst, SField src, SField tmp) {
+  SHopArgs a{};
+  a.g = L.g;
+  a.U = L.sl_links.p;
+  a.C = L.sl_clover.p;
+  a.src = src.data; a.src_norm = src.norm;
+  a.dst = tmp.data; a.dst_norm = tmp.norm;
+  a.coeff = 0.5f;
+  a.lo = (int)L.Vh; a.n = (int)L.Vh;
+  SHopArgs b = a;
+  b.src = tmp.data; b.src_norm = tmp.norm;
+  b.src2 = src.data; b.src2_norm = src.norm;
+  b.dst = dst.data; b.dst_norm = dst.norm;
+  b.coeff = -0.5f;
+  b.lo = 0;
+  YG_SLOPPY_DISPATCH(L.sl_prec, L.sl_reals, {
+    k_shop<SP, SK, 1><<<nblk(a.n, 128), 128, 0, L.stream>>>(a);
+    YG_LAUNCHED();
+    k_shop<SP, SK, 2><<<nblk(b.n, 128), 128, 0, L.stream>>>(b);
+    YG_LAUNCHED();
+  });
+  L.mvm += 2;
+}
+
+static double sloppy_dot(Lattice &L, SField p, SField q) {
+  int grid = sgrid(L.Vh);
+  if (grid > L.red_blocks) grid = L.red_blocks;
+  YG_SLOPPY_DISPATCH(L.sl_prec, 18, {
+    k_s_dot<SP><<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), p.data, p.norm, q.data, q.norm, (int)L.Vh);
+    YG_LAUNCHED();
+  });
+  return reduce_partials(L, grid).x;
+}
+
+static double sloppy_cg_update(Lattice &L, float *x, float *r, SField p, SField q, float alpha) {
+  int grid = sgrid(L.Vh);
+  if (grid > L.red_blocks) grid = L.red_blocks;
+  YG_SLOPPY_DISPATCH(L.sl_prec, 18, {
+    k_s_cg_update<SP><<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (float2 *)x, (float2 *)r, p.data,
+                                                  p.norm, q.data, q.norm, alpha, (int)L.Vh);
+    YG_LAUNCHED();
+  });
+  return reduce_partials(L, grid).x;
+}
+
+static void sloppy_xpay(Lattice &L, SField p, float beta, const float *r) {
+  YG_SLOPPY_DISPATCH(L.sl_prec, 18, {
+    k_s_xpay<SP><<<sgrid(L.Vh), 256, 0, L.stream>>>(p.data, p.norm, beta, (const float2 *)r, (int)L.Vh);
+    YG_LAUNCHED();
+  });
+}
+
+static void sloppy_from_d(Lattice &L, SField dst, const double *src) {
+  YG_SLOPPY_DISPATCH(L.sl_prec, 18, {
+    k_s_from_d<SP><<<sgrid(L.Vh), 256, 0, L.stream>>>(dst.data, dst.norm, (const double2 *)src, (int)L.Vh);
+    YG_LAUNCHED();
+  });
+}
+
+// Mixed-precision CG on Hphi_sq with the compressed inner operator (see cg_mixed in
+// yg_solvers.cu for the algorithm).  x and r of the inner iterations are FP32, p and Ap
+// are in the inner storage format; reliable updates recompute b - A x with the FP64
+// operator whenever |r| fell below delta * (its value at the last update), and the solve
+// stops only on the true FP64 squared residual |b - A x|^2 < prec |b|^2.
+int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, double delta, double *x, double *b,
+                    yg_solve_stats *st);
+
+}  // namespace yg
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+
+namespace yg {
+
+int cg(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
+
+int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, double delta, double *x, double *b,
+                    yg_solve_stats *st) {
+  auto t0 = std::chrono::steady_clock::now();
+  if (par.op != YG_OP_HPHI_SQ) throw Error(YG_ERR_ARG, "cg_mixed solves Hphi_sq systems");
+  if (!(delta > 0.0 && delta < 1.0)) throw Error(YG_ERR_ARG, "reliable-update delta must lie in (0,1)");
+  ensure_sloppy(L, par.mass, prec, reals);
+  long lo, n;
+  L.view_range(YG_VIEW_DEFAULT, lo, n);
+  const long cnt = n * 4L * L.d;
+  double *r = L.scratch_field(3), *Ax = L.scratch_field(4), *xd = L.scratch_field(5);
+  float *fr = reinterpret_cast<float *>(L.scratch_field(40));
+  float *fx = reinterpret_cast<float *>(L.scratch_field(42));
+  SField p = sfield(L, 41), q = sfield(L, 43), t = sfield(L, 44), o = sfield(L, 45);
+
+  auto residual = [&]() {           // r = b - A x in FP64, returns |r|^2
+    blas_copy(L, xd, x);
+    apply_op(L, YG_OP_HPHI_SQ, par.mass, Ax, xd);
+    blas_copy(L, r, b);
+    blas_axpby(L, r, make_double2(1, 0), make_double2(-1, 0), Ax, lo, n);
+    return blas_sqnorm(L, r, lo, n);
+  };
+
+  double norm = blas_sqnorm(L, b, lo, n);
+  double rr = residual();
+  double target = norm * par.prec;
+  int it = 0, updates = 0, status = YG_OK, stall = 0;
+  double best = rr;
+  if (rr >= target) {
+    f_from_d(L, fr, r, cnt);
+    sloppy_from_d(L, p, r);
+    YG_CUDA(cudaMemsetAsync(fx, 0, sizeof(float2) * cnt, L.stream));
+    double rr_s = rr, maxrr = rr;
+    const double d2 = delta * delta;
+    while (true) {
+      if (par.maxiter > 0 && it >= par.maxiter) { status = YG_MAXITER; break; }
+      it++;
+      sloppy_hphi(L, t, p, o);
+      sloppy_hphi(L, q, t, o);
+      double pq = sloppy_dot(L, p, q);
+      if (!std::isfinite(pq)) throw Error(YG_NONFINITE, "non-finite value in cg_mixed");
+      double alpha = rr_s / pq;
+      double rr_new = sloppy_cg_update(L, fx, fr, p, q, (float)alpha);
+      if (rr_new < d2 * maxrr || rr_new < target) {
+        d_add_f(L, x, fx, cnt);
+        YG_CUDA(cudaMemsetAsync(fx, 0, sizeof(float2) * cnt, L.stream));
+        double rr_true = residual();
+        updates++;
+        if (rr_true < target) { rr = rr_true; break; }
+        if (rr_true < 0.5 * best) { best = rr_true; stall = 0; }
+        else if (++stall >= 8) { status = YG_STALL; rr = rr_true; break; }
+        f_from_d(L, fr, r, cnt);
+        sloppy_xpay(L, p, (float)(rr_true / rr_s), fr);
+        rr_s = rr_true;
+        maxrr = rr_true;
+        rr = rr_true;
+        continue;
+      }
+      sloppy_xpay(L, p, (float)(rr_new / rr_s), fr);
+      rr_s = rr_new;
+    }
+  }
+  int fallback = 0;
+  if (status != YG_OK) {
+    yg_inv_par p64 = par;
+    p64.log = 0;
+    int it64 = 0;
+    int s64 = cg(L, p64, x, b, &it64);
+    it += it64;
+    fallback = 1;
+    rr = residual();
+    status = s64;
+  }
+  YG_CUDA(cudaStreamSynchronize(L.stream));
+  if (st) {
+    st->iterations = it;
+    st->reliable_updates = updates;
+    st->fallback = fallback;
+    st->true_residual = rr / norm;
+    st->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  if (par.log)
+    fprintf(stderr, "[INVERTER][30]cg_mixed(fp%d, %d-real): iterations = %d, precision = %1.4e\n", prec, reals, it,
+            rr / norm);
+  return status;
+}
+
+}  // namespace yg
