@@ -46,7 +46,7 @@ FALLBACK_HBM_GBS = 6650.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--dims", type=int, nargs=4, default=[32, 32, 32, 32])
@@ -58,6 +58,8 @@ def parse():
                          "operator with FP32/FP16 spinors and 18/12-real links")
     ap.add_argument("--delta", type=float, default=0.1, help="reliable-update threshold")
     ap.add_argument("--variants", action="store_true", help="also time every inner operator once")
+    ap.add_argument("--solve-only", action="store_true",
+                    help="time only the mixed solve and print its time (for profiling; not the bench line)")
     return ap.parse_args()
 
 
@@ -244,6 +246,11 @@ def run_ours(a, rank, world, dist):
     launches = (yg.launch_count() - n0) // a.steps
     clocks = clk.stop()
     st = stats[-1]
+    if a.solve_only:
+        if rank == 0:
+            print(json.dumps({"solve_ms": ms_mixed, "inner": a.inner, "delta": a.delta, "launches": int(launches),
+                              "solver": st}))
+        return
     # independent check of the stopping criterion on the true residual
     xc, r = lat.field(), lat.field()
     lat.spinor_copy(xc, x)

@@ -92,9 +92,14 @@ void schur_step1(Lattice &L, double mass, double *tmp, const double *src, double
   a.U = L.links.as<double2>();
   a.dst = (double2 *)tmp;
   a.dst2 = (double2 *)clob;
-  a.ldl = L.ldl.as<double2>();
   a.coeff = 0.5;                      // dirac_kernel(sptr, sptr, ODD, -1): -(-1)/2
-  launch_hop<EPI_CLOVINV>(L, a);
+  if (L.d <= kPackedInverseMaxD) {
+    a.cpk = L.cpk64.as<double2>();
+    launch_hop<EPI_CLOVPK>(L, a);
+  } else {
+    a.ldl = L.ldl.as<double2>();
+    launch_hop<EPI_CLOVINV>(L, a);
+  }
 }
 
 void schur_step2(Lattice &L, double mass, double *dst, const double *tmp, const double *src, bool g5) {

@@ -151,6 +151,40 @@ __device__ __forceinline__ void clover_site(cplx<R> (&out)[4][D], const cplx<R> 
   }
 }
 
+// acc += A psi for the psi stored at src2 (A as in clover_site), one spin block at a time
+// so that only two spins of psi are live next to the accumulator
+template <int D, typename R>
+__device__ __forceinline__ void clover_add_site(cplx<R> (&acc)[4][D], const cplx<R> *src2, const cplx<R> *cl,
+                                                const Geom &g, int id, R diag) {
+#pragma unroll
+  for (int blk = 0; blk < 2; blk++) {
+    const int s0 = 2 * blk, s1 = 2 * blk + 1;
+    const int m0 = 2 * blk, m1 = 2 * blk + 1;
+    cplx<R> p0[D], p1[D];
+#pragma unroll
+    for (int c = 0; c < D; c++) {
+      p0[c] = ld(src2, fidx(g, id, s0 * D + c, 4 * D));
+      p1[c] = ld(src2, fidx(g, id, s1 * D + c, 4 * D));
+    }
+#pragma unroll
+    for (int i = 0; i < D; i++) {
+      cplx<R> o0 = cadd(acc[s0][i], cscale(p0[i], diag)), o1 = cadd(acc[s1][i], cscale(p1[i], diag));
+#pragma unroll
+      for (int j = 0; j < D; j++) {
+        cplx<R> a0 = ld(cl, fidx(g, id, m0 * D * D + i * D + j, 4 * D * D));
+        cplx<R> a1 = ld(cl, fidx(g, id, m1 * D * D + i * D + j, 4 * D * D));
+        cplx<R> a1t = ld(cl, fidx(g, id, m1 * D * D + j * D + i, 4 * D * D));
+        cfma(o0, a0, p0[j]);
+        cfma(o0, a1, p1[j]);
+        cfmac(o1, a1t, p0[j]);
+        o1 = csub(o1, cmul(a0, p1[j]));
+      }
+      acc[s0][i] = o0;
+      acc[s1][i] = o1;
+    }
+  }
+}
+
 // A^-1 psi through the packed LDL factors of the site: forward substitution, D^-1, back
 // substitution with conj(L) (clover_inv_kernel, dirac.cpp:135-212)
 template <int D, typename R>
@@ -161,24 +195,24 @@ __device__ __forceinline__ void ldl_site(cplx<R> (&out)[4][D], const cplx<R> (&s
   for (int blk = 0; blk < 2; blk++) {
     const double2 *Lb = ldl + (long)blk * P * Vh + h;
     double2 x[N];
-    YG_UNROLL_D
+    #pragma unroll
     for (int i = 0; i < D; i++) {
       x[i] = make_double2((double)s[2 * blk][i].x, (double)s[2 * blk][i].y);
       x[i + D] = make_double2((double)s[2 * blk + 1][i].x, (double)s[2 * blk + 1][i].y);
     }
-    YG_UNROLL_D
+    #pragma unroll
     for (int i = 1; i < N; i++) {
-      YG_UNROLL_D
+      #pragma unroll
       for (int k = 0; k < i; k++) x[i] = csub(x[i], cmul(__ldg(Lb + (long)(i * (i + 1) / 2 + k) * Vh), x[k]));
     }
-    YG_UNROLL_D
+    #pragma unroll
     for (int i = N - 1; i >= 0; i--) {
       double dii = __ldg(Lb + (long)(i * (i + 1) / 2 + i) * Vh).x;
       x[i] = cscale(x[i], 1.0 / dii);
-      YG_UNROLL_D
+      #pragma unroll
       for (int k = i + 1; k < N; k++) x[i] = csub(x[i], cmulc(__ldg(Lb + (long)(k * (k + 1) / 2 + i) * Vh), x[k]));
     }
-    YG_UNROLL_D
+    #pragma unroll
     for (int i = 0; i < D; i++) {
       out[2 * blk][i] = mk<R>((R)x[i].x, (R)x[i].y);
       out[2 * blk + 1][i] = mk<R>((R)x[i + D].x, (R)x[i + D].y);
@@ -208,10 +242,48 @@ __device__ __forceinline__ void cinv_site(cplx<R> (&out)[4][D], const cplx<R> (&
   }
 }
 
+// A^-1 psi with the packed Hermitian inverse blocks of the FP64 path: per block of
+// N = 2d rows, N real diagonal entries (two per double2 word) then the N(N-1)/2 complex
+// lower-triangle entries (1,0),(2,0),(2,1),... one per word; word w of block b of the
+// site h lives at (b*2d^2 + w)*Vh + h.  The upper triangle is the conjugate transpose.
+template <int D, typename R>
+__device__ __forceinline__ void cpk_site(cplx<R> (&out)[4][D], const cplx<R> (&s)[4][D], const double2 *cpk,
+                                         int h, int Vh) {
+  constexpr int N = 2 * D, W = 2 * D * D;
+#pragma unroll
+  for (int blk = 0; blk < 2; blk++) {
+    const double2 *Cb = cpk + (long)blk * W * Vh + h;
+    double2 x[N], y[N];
+    #pragma unroll
+    for (int i = 0; i < D; i++) {
+      x[i] = make_double2((double)s[2 * blk][i].x, (double)s[2 * blk][i].y);
+      x[i + D] = make_double2((double)s[2 * blk + 1][i].x, (double)s[2 * blk + 1][i].y);
+    }
+    #pragma unroll
+    for (int w = 0; w < D; w++) {
+      double2 dd = __ldg(Cb + (long)w * Vh);
+      y[2 * w] = cscale(x[2 * w], dd.x);
+      y[2 * w + 1] = cscale(x[2 * w + 1], dd.y);
+    }
+    #pragma unroll
+    for (int i = 1; i < N; i++) {
+      #pragma unroll
+      for (int j = 0; j < i; j++) {
+        double2 m = __ldg(Cb + (long)(D + i * (i - 1) / 2 + j) * Vh);
+        cfma(y[i], m, x[j]);
+        cfmac(y[j], m, x[i]);
+      }
+    }
+    #pragma unroll
+    for (int i = 0; i < D; i++) {
+      out[2 * blk][i] = mk<R>((R)y[i].x, (R)y[i].y);
+      out[2 * blk + 1][i] = mk<R>((R)y[i + D].x, (R)y[i + D].y);
+    }
+  }
+}
+
 template <int D, typename R, int EPI>
-__global__ void __launch_bounds__(128) k_hop(HopArgs<R> a) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.n) return;
+__device__ __forceinline__ void hop_body(const HopArgs<R> &a, int t) {
   const Geom &g = a.g;
   int id = a.lo + t;
   int c[4];
@@ -236,26 +308,21 @@ __global__ void __launch_bounds__(128) k_hop(HopArgs<R> a) {
       }
     }
     store_spinor<D, R>(a.dst, acc, g, id);
-  } else if (EPI == EPI_CLOVINV) {
+  } else if (EPI == EPI_CLOVINV || EPI == EPI_CLOVPK) {
     if (a.dst2) store_spinor<D, R>(a.dst2, acc, g, id);
     cplx<R> out[4][D];
-    if (a.ldl) ldl_site<D, R>(out, acc, a.ldl, id - g.Vh, g.Vh);
+    if (EPI == EPI_CLOVPK) cpk_site<D, R>(out, acc, a.cpk, id - g.Vh, g.Vh);
+    else if (sizeof(R) == sizeof(double)) ldl_site<D, R>(out, acc, a.ldl, id - g.Vh, g.Vh);
     else cinv_site<D, R>(out, acc, a.cinv, id - g.Vh, g.Vh);
     store_spinor<D, R>(a.dst, out, g, id);
   } else {
-    cplx<R> s2[4][D];
-    load_spinor<D, R>(s2, a.src2, g, id);
     bool zero_add = bnd && a.zero_add_at_boundary;
     if (EPI == EPI_CLOVADD) {
       R diag = a.diag + ((c[0] == g.Ta || c[0] == g.Tb) ? a.cfm1 : (R)0);
-      cplx<R> cs[4][D];
-      clover_site<D, R>(cs, s2, a.cl, g, id, diag);
-#pragma unroll
-      for (int s = 0; s < 4; s++) {
-        YG_UNROLL_D
-        for (int k = 0; k < D; k++) acc[s][k] = zero_add ? acc[s][k] : cadd(acc[s][k], cs[s][k]);
-      }
+      if (!zero_add) clover_add_site<D, R>(acc, a.src2, a.cl, g, id, diag);
     } else {
+      cplx<R> s2[4][D];
+      load_spinor<D, R>(s2, a.src2, g, id);
 #pragma unroll
       for (int s = 0; s < 4; s++) {
         YG_UNROLL_D
@@ -271,6 +338,12 @@ __global__ void __launch_bounds__(128) k_hop(HopArgs<R> a) {
     }
     store_spinor<D, R>(a.dst, acc, g, id);
   }
+}
+
+template <int D, typename R, int EPI>
+__global__ void __launch_bounds__(128) k_hop(HopArgs<R> a) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < a.n) hop_body<D, R, EPI>(a, t);
 }
 
 // clover_kernel (dirac.cpp:25-107) standalone: dst (=|+=) A psi over [lo, lo+n)
@@ -392,6 +465,33 @@ __global__ void k_cinv_float(float2 *cinv, const double2 *ldl, int Vh) {
   }
 }
 
+// packed Hermitian FP64 inverse of both clover blocks (layout of cpk_site), from the LDL
+// factors: column j of A^-1 by forward substitution, D^-1 and back substitution
+template <int D>
+__global__ void k_cinv_packed64(double2 *cpk, const double2 *ldl, int Vh) {
+  int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= Vh) return;
+  constexpr int N = 2 * D, P = D * (2 * D + 1), W = 2 * D * D;
+  for (int blk = 0; blk < 2; blk++) {
+    const double2 *Lb = ldl + (long)blk * P * Vh + h;
+    double2 *Cb = cpk + (long)blk * W * Vh + h;
+    for (int col = 0; col < N; col++) {
+      double2 x[N];
+      for (int i = 0; i < N; i++) x[i] = make_double2(i == col ? 1.0 : 0.0, 0.0);
+      for (int i = 1; i < N; i++)
+        for (int k = 0; k < i; k++) x[i] = csub(x[i], cmul(Lb[(long)(i * (i + 1) / 2 + k) * Vh], x[k]));
+      for (int i = N - 1; i >= 0; i--) {
+        x[i] = cscale(x[i], 1.0 / Lb[(long)(i * (i + 1) / 2 + i) * Vh].x);
+        for (int k = i + 1; k < N; k++) x[i] = csub(x[i], cmulc(Lb[(long)(k * (k + 1) / 2 + i) * Vh], x[k]));
+      }
+      // diagonal entry (col, col): real part into its half of word col/2
+      double *dw = reinterpret_cast<double *>(Cb + (long)(col / 2) * Vh);
+      dw[col & 1] = x[col].x;
+      for (int i = col + 1; i < N; i++) Cb[(long)(D + i * (i - 1) / 2 + col) * Vh] = x[i];
+    }
+  }
+}
+
 // log prod_n D_nn of both blocks per site (clover_logdet, clover.cpp:281-305)
 template <int D>
 __global__ void k_logdet(double *out, const double2 *ldl, int Vh) {
@@ -414,6 +514,7 @@ static void launch_hop_epi(const HopArgs<R> &a, int epi, cudaStream_t s) {
     case EPI_PLAIN: k_hop<D, R, EPI_PLAIN><<<nblk(a.n, t), t, 0, s>>>(a); break;
     case EPI_CLOVINV: k_hop<D, R, EPI_CLOVINV><<<nblk(a.n, t), t, 0, s>>>(a); break;
     case EPI_CLOVADD: k_hop<D, R, EPI_CLOVADD><<<nblk(a.n, t), t, 0, s>>>(a); break;
+    case EPI_CLOVPK: k_hop<D, R, EPI_CLOVPK><<<nblk(a.n, t), t, 0, s>>>(a); break;
     default: k_hop<D, R, EPI_AXPY><<<nblk(a.n, t), t, 0, s>>>(a); break;
   }
 }
@@ -443,6 +544,11 @@ void DK<D>::ldl(double2 *ldl, const double2 *cl, Geom g, double sigma, double cf
 template <int D>
 void DK<D>::cinv_float(float2 *cinv, const double2 *ldl, int Vh, cudaStream_t s) {
   k_cinv_float<D><<<nblk(Vh, 64), 64, 0, s>>>(cinv, ldl, Vh);
+}
+
+template <int D>
+void DK<D>::cinv_packed64(double2 *cpk, const double2 *ldl, int Vh, cudaStream_t s) {
+  k_cinv_packed64<D><<<nblk(Vh, 64), 64, 0, s>>>(cpk, ldl, Vh);
 }
 
 template <int D>

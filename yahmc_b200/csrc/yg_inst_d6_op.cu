@@ -9,5 +9,6 @@ template void DK<6>::clover(double2 *, const double2 *, const double2 *, Geom, d
 template void DK<6>::clover_inv(double2 *, const double2 *, const double2 *, Geom, int, cudaStream_t);
 template void DK<6>::ldl(double2 *, const double2 *, Geom, double, double, int, cudaStream_t);
 template void DK<6>::cinv_float(float2 *, const double2 *, int, cudaStream_t);
+template void DK<6>::cinv_packed64(double2 *, const double2 *, int, cudaStream_t);
 template void DK<6>::logdet(double *, const double2 *, int, cudaStream_t);
 }  // namespace yg

@@ -9,7 +9,9 @@
 
 namespace yg {
 
-enum { EPI_PLAIN = 0, EPI_CLOVINV = 1, EPI_CLOVADD = 2, EPI_AXPY = 3 };
+// CLOVINV applies the LDL factors (FP64) or the explicit inverse (FP32); CLOVPK the packed
+// Hermitian FP64 inverse
+enum { EPI_PLAIN = 0, EPI_CLOVINV = 1, EPI_CLOVADD = 2, EPI_AXPY = 3, EPI_CLOVPK = 4 };
 
 template <typename R>
 struct HopArgs {
@@ -22,6 +24,7 @@ struct HopArgs {
   const cplx<R> *cl;      // clover term (4 d x d per site)
   const double2 *ldl;     // LDL factors (FP64 path)
   const cplx<R> *cinv;    // explicit inverse clover blocks (FP32 path): 2 x (2d)^2 per site
+  const double2 *cpk;     // packed Hermitian inverse clover blocks (FP64 path, d <= 6): 2 x 2d^2 words per site
   R coeff;                // -sign/2
   R diag;                 // 4+m (CLOVADD) or the AXPY coefficient
   R cfm1;                 // cf-1 (Dirac boundary term at t = Ta, Tb)
@@ -41,6 +44,7 @@ struct DK {
   static void clover_inv(double2 *dst, const double2 *src, const double2 *ldl, Geom g, int assign, cudaStream_t s);
   static void ldl(double2 *ldl, const double2 *cl, Geom g, double sigma, double cf, int boundary_term, cudaStream_t s);
   static void cinv_float(float2 *cinv, const double2 *ldl, int Vh, cudaStream_t s);
+  static void cinv_packed64(double2 *cpk, const double2 *ldl, int Vh, cudaStream_t s);
   static void logdet(double *out, const double2 *ldl, int Vh, cudaStream_t s);
   static void clover_fermion_force(double2 *clf, const double2 *lhs, const double2 *rhs, Geom g, double residue,
                                    cudaStream_t s);

@@ -42,8 +42,10 @@ void DevBuf::release() {
 Lattice::~Lattice() {
   for (double *s : scratch) if (s) cudaFree(s);
   if (host_result) cudaFreeHost(host_result);
+  if (sl_hist) cudaFreeHost(sl_hist);
+  for (cudaEvent_t e : sl_ev) if (e) cudaEventDestroy(e);
   for (DevBuf *b : {&fund, &links, &clover, &ldl, &cl_force, &mom, &tables, &red_partial, &red_result, &links_f,
-                    &clover_f, &cinv_f, &sl_links, &sl_clover})
+                    &clover_f, &cinv_f, &sl_links, &sl_clover, &cpk64, &sl_part, &sl_scal})
     b->release();
 }
 
@@ -246,6 +248,13 @@ void ensure_ldl(Lattice &L, double sigma) {
   int boundary_term = (L.p.bc == YG_BC_OPEN || L.p.bc == YG_BC_SF);
   YG_DISPATCH_D(L.d, K::ldl(L.ldl.as<double2>(), L.clover.as<double2>(), L.g, sigma, L.p.cf, boundary_term, L.stream));
   YG_LAUNCHED();
+  if (L.d <= kPackedInverseMaxD) {
+    // the Schur step of the FP64 operator applies this explicit inverse (a Hermitian
+    // mat-vec) instead of the LDL substitutions: same matrix, no serial divide chain
+    L.cpk64.alloc(sizeof(double2) * 2 * 2 * (size_t)L.d * L.d * L.Vh);
+    YG_DISPATCH_D(L.d, K::cinv_packed64(L.cpk64.as<double2>(), L.ldl.as<double2>(), (int)L.Vh, L.stream));
+    YG_LAUNCHED();
+  }
   L.ldl_sigma = sigma;
   L.ldl_valid = true;
 }

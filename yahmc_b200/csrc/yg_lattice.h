@@ -59,6 +59,7 @@ struct Lattice {
   DevBuf ldl;       // LDL factors, 2 x d(2d+1) per site of block 1   (cl_ldl)
   double ldl_sigma = 0;
   bool ldl_valid = false;
+  DevBuf cpk64;     // packed Hermitian FP64 inverse of the odd-site blocks, d <= 6 (rebuilt with ldl)
   DevBuf cl_force;  // 6 x d x d per site                            (cl_force)
   DevBuf mom;       // 4 x NG per site                               (afield_momenta)
   DevBuf tables;    // basis / generators
@@ -88,6 +89,12 @@ struct Lattice {
   int sl_prec = 0, sl_reals = 0;
   double sl_mass = 0;
   bool sl_valid = false;
+  DevBuf sl_part;      // per-block partial sums of the device-scalar reductions
+  int sl_grid_nrm = 0; // blocks of the hop that forms <p, A p> (resident-grid size)
+  int sl_grid_vec = 0; // blocks of the inner vector kernels
+  DevBuf sl_scal;      // device scalars of the inner CG (rr, alpha, beta, ...) + completion counter
+  double *sl_hist = nullptr;          // mapped pinned host ring of inner |r|^2 (written by the GPU)
+  cudaEvent_t sl_ev[2] = {nullptr, nullptr};
 
   long field_doubles() const { return 8L * d * V; }
   size_t field_bytes() const { return sizeof(double) * field_doubles(); }
@@ -102,6 +109,7 @@ struct Lattice {
 Lattice *lattice_create(const yg_params &p);
 void represent_and_clover(Lattice &L);
 void ensure_ldl(Lattice &L, double sigma);
+constexpr int kPackedInverseMaxD = 6;   // largest d whose FP64 Schur step uses the packed inverse
 void gauge_upload(Lattice &L, const double *host);
 void gauge_download(Lattice &L, double *host);
 void repr_download(Lattice &L, double *host);

@@ -14,6 +14,7 @@
 //     Without a clover term M_o^-1 = 1 and M_e = (4+m)^2 (dirac.cpp:755-765).
 // Arithmetic is FP32 throughout; FP16 is a storage format only.
 #include <cuda_fp16.h>
+#include <algorithm>
 #include "yg_lattice.h"
 #include "yg_kernels.h"
 
@@ -42,8 +43,9 @@ __device__ __forceinline__ unsigned f2h(float2 f) {
   return *reinterpret_cast<unsigned *>(&h);
 }
 
+// unscaled components; FP16 words are stored divided by the site norm (snorm)
 template <int P>
-__device__ __forceinline__ void sload(float2 (&s)[12], const void *base, const float *norm, int blk, int h, int Vh) {
+__device__ __forceinline__ void sload_raw(float2 (&s)[12], const void *base, int blk, int h, int Vh) {
   if (P == 32) {
     const float4 *f = reinterpret_cast<const float4 *>(base);
 #pragma unroll
@@ -54,16 +56,29 @@ __device__ __forceinline__ void sload(float2 (&s)[12], const void *base, const f
     }
   } else {
     const uint4 *f = reinterpret_cast<const uint4 *>(base);
-    float n = __ldg(norm + (long)blk * Vh + h);
 #pragma unroll
     for (int w = 0; w < 3; w++) {
       uint4 v = __ldg(f + (long)(blk * 3 + w) * Vh + h);
-      float2 a = h2f(v.x), b = h2f(v.y), c = h2f(v.z), d = h2f(v.w);
-      s[4 * w + 0] = make_float2(a.x * n, a.y * n);
-      s[4 * w + 1] = make_float2(b.x * n, b.y * n);
-      s[4 * w + 2] = make_float2(c.x * n, c.y * n);
-      s[4 * w + 3] = make_float2(d.x * n, d.y * n);
+      s[4 * w + 0] = h2f(v.x);
+      s[4 * w + 1] = h2f(v.y);
+      s[4 * w + 2] = h2f(v.z);
+      s[4 * w + 3] = h2f(v.w);
     }
+  }
+}
+
+template <int P>
+__device__ __forceinline__ float snorm(const float *norm, int blk, int h, int Vh) {
+  return P == 32 ? 1.f : __ldg(norm + (long)blk * Vh + h);
+}
+
+template <int P>
+__device__ __forceinline__ void sload(float2 (&s)[12], const void *base, const float *norm, int blk, int h, int Vh) {
+  sload_raw<P>(s, base, blk, h, Vh);
+  if (P == 16) {
+    float n = snorm<P>(norm, blk, h, Vh);
+#pragma unroll
+    for (int k = 0; k < 12; k++) s[k] = cscale(s[k], n);
   }
 }
 
@@ -187,7 +202,43 @@ struct SHopArgs {
   const void *C;            // packed clover blocks
   float coeff;              // +1/2 (step 1) or -1/2 (step 2)
   int lo, n;                // output sites [lo, lo+n): the odd block (step 1) or even (step 2)
+  double *part;             // NRM: one partial sum of |dst|^2 per block
 };
+
+// ------------------------------------------------------------------ device-side reductions
+// Device scalars of the inner CG (sl_scal): |r|^2 in two slots that alternate between
+// iterations (iteration k reads slot k&1 and writes slot (k+1)&1, so no block overwrites
+// a value another block of the same launch still reads), and alpha, <p, A p> for
+// inspection.  Grid sums are two-phase: a producer launch stores one partial per block,
+// and every block of the consumer launch adds all of them in index order, so the result
+// is deterministic and no block ever waits for another.
+enum { S_RR0 = 0, S_RR1 = 1, S_ALPHA = 2, S_PQ = 3, S_WORDS = 8 };
+
+// block total of v, returned to every thread (blockDim a multiple of 32, at most 1024)
+__device__ __forceinline__ double block_total(double v) {
+  __shared__ double sh[33];
+  __syncthreads();                       // a previous call may still be reading sh
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[32] = v;
+  }
+  __syncthreads();
+  return sh[32];
+}
+
+// sum of n partials written by the previous launch, identical in every block
+__device__ __forceinline__ double sum_partials(const double *part, int n) {
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += part[i];
+  return block_total(acc);
+}
 
 // one direction: SIG = -1 forward (1 - gamma_mu), +1 backward (1 + gamma_mu); as hop_dir
 // in yg_dirac_impl.cuh (dirac.cpp:258-697)
@@ -196,7 +247,8 @@ __device__ __forceinline__ void shop_dir(float2 (&acc)[12], const SHopArgs &a, i
   const Geom &g = a.g;
   float2 p[12];
   int nb = nid >= g.Vh, nh = nid - nb * g.Vh;
-  sload<P>(p, a.src, a.src_norm, nb, nh, g.Vh);
+  sload_raw<P>(p, a.src, nb, nh, g.Vh);          // the site norm multiplies chi below (linear)
+  const float pn = snorm<P>(a.src_norm, nb, nh, g.Vh);
   float2 hh[2][3];
 #pragma unroll
   for (int c = 0; c < 3; c++) {
@@ -228,8 +280,8 @@ __device__ __forceinline__ void shop_dir(float2 (&acc)[12], const SHopArgs &a, i
       if (SIG > 0) { cfmac(s0, u[j * 3 + i], hh[0][j]); cfmac(s1, u[j * 3 + i], hh[1][j]); }
       else { cfma(s0, u[i * 3 + j], hh[0][j]); cfma(s1, u[i * 3 + j], hh[1][j]); }
     }
-    chi[0][i] = s0;
-    chi[1][i] = s1;
+    chi[0][i] = P == 16 ? cscale(s0, pn) : s0;
+    chi[1][i] = P == 16 ? cscale(s1, pn) : s1;
   }
 #pragma unroll
   for (int c = 0; c < 3; c++) {
@@ -253,12 +305,10 @@ __device__ __forceinline__ void shop_dir(float2 (&acc)[12], const SHopArgs &a, i
 
 // STEP 1 (odd output):  dst = M_o^-1 (coeff * hop(src))
 // STEP 2 (even output): dst = gamma5 (M_e src2 + coeff * hop(src))
+// returns |dst|^2 of the site (before FP16 rounding)
 template <int P, int K, int STEP>
-__global__ void __launch_bounds__(128) k_shop(SHopArgs a) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.n) return;
+__device__ __forceinline__ float shop_site(const SHopArgs &a, int id) {
   const Geom &g = a.g;
-  int id = a.lo + t;
   int c[4];
   coords_of(g, id, c);
   int T = g.dim[0];
@@ -293,11 +343,30 @@ __global__ void __launch_bounds__(128) k_shop(SHopArgs a) {
       if (k >= 6) out[k] = cscale(out[k], -1.f);            // gamma5
     }
   }
-  if (bnd) {
+  float n2 = 0.f;
 #pragma unroll
-    for (int k = 0; k < 12; k++) out[k] = make_float2(0.f, 0.f);
+  for (int k = 0; k < 12; k++) {
+    if (bnd) out[k] = make_float2(0.f, 0.f);
+    n2 = fmaf(out[k].x, out[k].x, fmaf(out[k].y, out[k].y, n2));
   }
   sstore<P>(a.dst, a.dst_norm, out, blk, h, g.Vh);
+  return n2;
+}
+
+// NRM = 1 (first Hphi of a CG iteration, t = Hphi p): also the per-block partials of
+// <p, A p> = |t|^2 (Hphi is Hermitian and A = Hphi^2); a grid-stride loop over a grid of
+// resident blocks keeps the number of partials small
+template <int P, int K, int STEP, int NRM>
+__global__ void __launch_bounds__(128) k_shop(SHopArgs a) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!NRM) {
+    if (t < a.n) shop_site<P, K, STEP>(a, a.lo + t);
+    return;
+  }
+  double n2 = 0.0;
+  for (; t < a.n; t += gridDim.x * blockDim.x) n2 += (double)shop_site<P, K, STEP>(a, a.lo + t);
+  n2 = block_total(n2);
+  if (threadIdx.x == 0) a.part[blockIdx.x] = n2;
 }
 
 // ------------------------------------------------------------------ builds (once per gauge field / mass)
@@ -415,21 +484,6 @@ __global__ void k_pack_clover_odd(void *dst, const double2 *ldl, Geom g, int clo
 // FP32 vectors x, r use the FP64 field order (complex k = spin*3+colour at [k*Vh + h],
 // even block); sloppy vectors p, q use the formats above.
 
-__device__ __forceinline__ double block_sum_d(double v) {
-  __shared__ double sh[8];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) sh[w] = v;
-  __syncthreads();
-  v = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
-  if (w == 0) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  }
-  return v;
-}
-
 // sloppy <- FP64 block 0 (even sites)
 template <int P>
 __global__ void __launch_bounds__(256) k_s_from_d(void *dst, float *dn, const double2 *src, int Vh) {
@@ -444,28 +498,20 @@ __global__ void __launch_bounds__(256) k_s_from_d(void *dst, float *dn, const do
   }
 }
 
-// partial Re <p, q> over the even block
+// alpha = |r|^2 / <p, A p> from the partials of the NRM hop; x += alpha p ; r -= alpha q ;
+// per-block partials of the new |r|^2 into part_r
 template <int P>
-__global__ void __launch_bounds__(256) k_s_dot(double2 *partial, const void *p, const float *pn, const void *q,
-                                               const float *qn, int Vh) {
-  double acc = 0.0;
-  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += gridDim.x * blockDim.x) {
-    float2 a[12], b[12];
-    sload<P>(a, p, pn, 0, h, Vh);
-    sload<P>(b, q, qn, 0, h, Vh);
-    float s = 0.f;
-#pragma unroll
-    for (int k = 0; k < 12; k++) s += a[k].x * b[k].x + a[k].y * b[k].y;
-    acc += s;
+__global__ void __launch_bounds__(256) k_s_cg_update(float2 *x, float2 *r, const void *p, const float *pn,
+                                                     const void *q, const float *qn, double *scal,
+                                                     const double *part_pq, int n_pq, double *part_r, int par,
+                                                     int Vh) {
+  const double pq = sum_partials(part_pq, n_pq);
+  const double alpha = scal[S_RR0 + par] / pq;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    scal[S_PQ] = pq;
+    scal[S_ALPHA] = alpha;
   }
-  acc = block_sum_d(acc);
-  if (threadIdx.x == 0) partial[blockIdx.x] = make_double2(acc, 0.0);
-}
-
-// x += a p ; r -= a q ; partial |r|^2
-template <int P>
-__global__ void __launch_bounds__(256) k_s_cg_update(double2 *partial, float2 *x, float2 *r, const void *p,
-                                                     const float *pn, const void *q, const float *qn, float a, int Vh) {
+  const float a = (float)alpha;
   double acc = 0.0;
   for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += gridDim.x * blockDim.x) {
     float2 pp[12], qq[12];
@@ -482,17 +528,26 @@ __global__ void __launch_bounds__(256) k_s_cg_update(double2 *partial, float2 *x
       ri.y = fmaf(-a, qq[k].y, ri.y);
       x[i] = xi;
       r[i] = ri;
-      s += ri.x * ri.x + ri.y * ri.y;
+      s = fmaf(ri.x, ri.x, fmaf(ri.y, ri.y, s));
     }
     acc += s;
   }
-  acc = block_sum_d(acc);
-  if (threadIdx.x == 0) partial[blockIdx.x] = make_double2(acc, 0.0);
+  acc = block_total(acc);
+  if (threadIdx.x == 0) part_r[blockIdx.x] = acc;
 }
 
-// p = r + b p
+// |r|^2 from the update's partials, beta = |r|^2 / |r_old|^2, p = r + beta p; block 0
+// stores |r|^2 for the next iteration and into *hist (mapped host memory the host reads
+// one iteration later)
 template <int P>
-__global__ void __launch_bounds__(256) k_s_xpay(void *p, float *pn, float b, const float2 *r, int Vh) {
+__global__ void __launch_bounds__(256) k_s_xpay(void *p, float *pn, double *scal, const double *part_r, int n_r,
+                                                int par, double *hist, const float2 *r, int Vh) {
+  const double rr = sum_partials(part_r, n_r);
+  const float b = (float)(rr / scal[S_RR0 + par]);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    scal[S_RR0 + (par ^ 1)] = rr;
+    *hist = rr;
+  }
   for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += gridDim.x * blockDim.x) {
     float2 pp[12];
     sload<P>(pp, p, pn, 0, h, Vh);
@@ -504,6 +559,8 @@ __global__ void __launch_bounds__(256) k_s_xpay(void *p, float *pn, float b, con
     sstore<P>(p, pn, pp, 0, h, Vh);
   }
 }
+
+__global__ void k_s_set(double *scal, int i, double v) { scal[i] = v; }
 
 // ------------------------------------------------------------------ host side
 // sloppy fields live in the lattice's scratch fields (each one FP64 field in size, which
@@ -543,7 +600,26 @@ void ensure_sloppy(Lattice &L, double mass, int prec, int reals) {
   if (reals == 12 && !(L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL))
     throw Error(YG_ERR_ARG, "12-real links need SU(3) fundamental links");
   if (!L.p.eo) throw Error(YG_ERR_ARG, "the mixed-precision solver needs even-odd preconditioning");
+  if (!L.sl_hist) {
+    YG_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&L.sl_hist), 4 * sizeof(double), cudaHostAllocMapped));
+    for (cudaEvent_t &e : L.sl_ev) YG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    L.sl_scal.alloc(S_WORDS * sizeof(double));
+    YG_CUDA(cudaMemsetAsync(L.sl_scal.p, 0, S_WORDS * sizeof(double), L.stream));
+  }
   if (L.sl_valid && L.sl_prec == prec && L.sl_reals == reals && L.sl_mass == mass) return;
+  {
+    // resident-grid sizes of the reduction kernels, and room for their partials
+    int dev = 0, sms = 0, per_nrm = 0, per_vec = 0;
+    YG_CUDA(cudaGetDevice(&dev));
+    YG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    YG_SLOPPY_DISPATCH(prec, reals, {
+      YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_nrm, k_shop<SP, SK, 2, 1>, 128, 0));
+      YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_vec, k_s_cg_update<SP>, 256, 0));
+    });
+    L.sl_grid_nrm = (int)std::min<long>((long)sms * std::max(per_nrm, 1), nblk(L.Vh, 128));
+    L.sl_grid_vec = (int)std::min<long>((long)sms * std::max(per_vec, 1), nblk(L.Vh, 256));
+    L.sl_part.alloc(sizeof(double) * (size_t)(L.sl_grid_nrm + L.sl_grid_vec));
+  }
   size_t esz = prec == 32 ? 4 : 2;
   int K = reals / 2;
   L.sl_links.alloc(esz * 2 * K * 4 * (size_t)L.V);
@@ -566,8 +642,13 @@ void ensure_sloppy(Lattice &L, double mass, int prec, int reals) {
   L.sl_valid = true;
 }
 
-// dst = Hphi(src) with the compressed operator; tmp receives the odd-site intermediate
-static void sloppy_hphi(Lattice &L, SField dst, SField src, SField tmp) {
+static double *dscal(Lattice &L) { return L.sl_scal.as<double>(); }
+static double *part_pq(Lattice &L) { return L.sl_part.as<double>(); }
+static double *part_r(Lattice &L) { return L.sl_part.as<double>() + L.sl_grid_nrm; }
+
+// dst = Hphi(src) with the compressed operator; tmp receives the odd-site intermediate.
+// nrm: also the partials of |dst|^2 = <p, A p> (the first Hphi of a CG iteration)
+static void sloppy_hphi(Lattice &L, SField dst, SField src, SField tmp, bool nrm) {
   SHopArgs a{};
   a.g = L.g;
   a.U = L.sl_links.p;
@@ -582,39 +663,31 @@ static void sloppy_hphi(Lattice &L, SField dst, SField src, SField tmp) {
   b.dst = dst.data; b.dst_norm = dst.norm;
   b.coeff = -0.5f;
   b.lo = 0;
+  b.part = part_pq(L);
   YG_SLOPPY_DISPATCH(L.sl_prec, L.sl_reals, {
-    k_shop<SP, SK, 1><<<nblk(a.n, 128), 128, 0, L.stream>>>(a);
+    k_shop<SP, SK, 1, 0><<<nblk(a.n, 128), 128, 0, L.stream>>>(a);
     YG_LAUNCHED();
-    k_shop<SP, SK, 2><<<nblk(b.n, 128), 128, 0, L.stream>>>(b);
+    if (nrm) k_shop<SP, SK, 2, 1><<<L.sl_grid_nrm, 128, 0, L.stream>>>(b);
+    else k_shop<SP, SK, 2, 0><<<nblk(b.n, 128), 128, 0, L.stream>>>(b);
     YG_LAUNCHED();
   });
   L.mvm += 2;
 }
 
-static double sloppy_dot(Lattice &L, SField p, SField q) {
-  int grid = sgrid(L.Vh);
-  if (grid > L.red_blocks) grid = L.red_blocks;
+// par = iteration parity (selects the |r|^2 slot)
+static void sloppy_cg_update(Lattice &L, float *x, float *r, SField p, SField q, int par) {
   YG_SLOPPY_DISPATCH(L.sl_prec, 18, {
-    k_s_dot<SP><<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), p.data, p.norm, q.data, q.norm, (int)L.Vh);
+    k_s_cg_update<SP><<<L.sl_grid_vec, 256, 0, L.stream>>>((float2 *)x, (float2 *)r, p.data, p.norm, q.data, q.norm,
+                                                           dscal(L), part_pq(L), L.sl_grid_nrm, part_r(L), par,
+                                                           (int)L.Vh);
     YG_LAUNCHED();
   });
-  return reduce_partials(L, grid).x;
 }
 
-static double sloppy_cg_update(Lattice &L, float *x, float *r, SField p, SField q, float alpha) {
-  int grid = sgrid(L.Vh);
-  if (grid > L.red_blocks) grid = L.red_blocks;
+static void sloppy_xpay(Lattice &L, SField p, const float *r, int par, double *hist) {
   YG_SLOPPY_DISPATCH(L.sl_prec, 18, {
-    k_s_cg_update<SP><<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (float2 *)x, (float2 *)r, p.data,
-                                                  p.norm, q.data, q.norm, alpha, (int)L.Vh);
-    YG_LAUNCHED();
-  });
-  return reduce_partials(L, grid).x;
-}
-
-static void sloppy_xpay(Lattice &L, SField p, float beta, const float *r) {
-  YG_SLOPPY_DISPATCH(L.sl_prec, 18, {
-    k_s_xpay<SP><<<sgrid(L.Vh), 256, 0, L.stream>>>(p.data, p.norm, beta, (const float2 *)r, (int)L.Vh);
+    k_s_xpay<SP><<<L.sl_grid_vec, 256, 0, L.stream>>>(p.data, p.norm, dscal(L), part_r(L), L.sl_grid_vec, par, hist,
+                                                      (const float2 *)r, (int)L.Vh);
     YG_LAUNCHED();
   });
 }
@@ -626,11 +699,19 @@ static void sloppy_from_d(Lattice &L, SField dst, const double *src) {
   });
 }
 
-// Mixed-precision CG on Hphi_sq with the compressed inner operator (see cg_mixed in
-// yg_solvers.cu for the algorithm).  x and r of the inner iterations are FP32, p and Ap
-// are in the inner storage format; reliable updates recompute b - A x with the FP64
-// operator whenever |r| fell below delta * (its value at the last update), and the solve
-// stops only on the true FP64 squared residual |b - A x|^2 < prec |b|^2.
+static void set_scalar(Lattice &L, int i, double v) {
+  k_s_set<<<1, 1, 0, L.stream>>>(dscal(L), i, v);
+  YG_LAUNCHED();
+}
+
+// Mixed-precision CG on Hphi_sq with the compressed inner operator.  x and r of the inner
+// iterations are FP32, p and A p are in the inner storage format.  alpha and beta live on
+// the device, so an inner iteration is six launches and no host synchronisation; the host
+// reads each iteration's |r|^2 one iteration late (while the next one runs) and then
+// decides on a reliable update: b - A x is recomputed with the FP64 operator whenever the
+// iterated |r| fell below delta times its value at the last update, r is replaced by it
+// and the search direction is kept.  The solve stops only on the true FP64 squared
+// residual |b - A x|^2 < prec |b|^2; a stall falls back to the FP64 CG.
 int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, double delta, double *x, double *b,
                     yg_solve_stats *st);
 
@@ -657,6 +738,7 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, doub
   float *fr = reinterpret_cast<float *>(L.scratch_field(40));
   float *fx = reinterpret_cast<float *>(L.scratch_field(42));
   SField p = sfield(L, 41), q = sfield(L, 43), t = sfield(L, 44), o = sfield(L, 45);
+  volatile double *hist = L.sl_hist;
 
   auto residual = [&]() {           // r = b - A x in FP64, returns |r|^2
     blas_copy(L, xd, x);
@@ -675,34 +757,43 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, doub
     f_from_d(L, fr, r, cnt);
     sloppy_from_d(L, p, r);
     YG_CUDA(cudaMemsetAsync(fx, 0, sizeof(float2) * cnt, L.stream));
-    double rr_s = rr, maxrr = rr;
+    set_scalar(L, S_RR0, rr);                 // iteration 0 reads slot 0
+    double maxrr = rr;
     const double d2 = delta * delta;
+    bool pending = false;           // an enqueued iteration whose |r|^2 is still to be read
     while (true) {
-      if (par.maxiter > 0 && it >= par.maxiter) { status = YG_MAXITER; break; }
+      if (par.maxiter > 0 && it >= par.maxiter) {
+        status = YG_MAXITER;
+        d_add_f(L, x, fx, cnt);     // keep the progress of the inner iterations
+        break;
+      }
+      int slot = it & 1;
+      sloppy_hphi(L, t, p, o, true);
+      sloppy_hphi(L, q, t, o, false);
+      sloppy_cg_update(L, fx, fr, p, q, slot);
+      sloppy_xpay(L, p, fr, slot, const_cast<double *>(hist) + slot);
+      YG_CUDA(cudaEventRecord(L.sl_ev[slot], L.stream));
       it++;
-      sloppy_hphi(L, t, p, o);
-      sloppy_hphi(L, q, t, o);
-      double pq = sloppy_dot(L, p, q);
-      if (!std::isfinite(pq)) throw Error(YG_NONFINITE, "non-finite value in cg_mixed");
-      double alpha = rr_s / pq;
-      double rr_new = sloppy_cg_update(L, fx, fr, p, q, (float)alpha);
-      if (rr_new < d2 * maxrr || rr_new < target) {
+      if (!pending) { pending = true; continue; }
+      // the previous iteration's |r|^2, read while this one runs
+      YG_CUDA(cudaEventSynchronize(L.sl_ev[slot ^ 1]));
+      double rr_prev = hist[slot ^ 1];
+      if (!std::isfinite(rr_prev)) throw Error(YG_NONFINITE, "non-finite value in cg_mixed");
+      if (rr_prev < d2 * maxrr || rr_prev < target) {
+        // reliable update on the state after the iteration just enqueued
         d_add_f(L, x, fx, cnt);
         YG_CUDA(cudaMemsetAsync(fx, 0, sizeof(float2) * cnt, L.stream));
         double rr_true = residual();
         updates++;
-        if (rr_true < target) { rr = rr_true; break; }
-        if (rr_true < 0.5 * best) { best = rr_true; stall = 0; }
-        else if (++stall >= 8) { status = YG_STALL; rr = rr_true; break; }
-        f_from_d(L, fr, r, cnt);
-        sloppy_xpay(L, p, (float)(rr_true / rr_s), fr);
-        rr_s = rr_true;
-        maxrr = rr_true;
         rr = rr_true;
-        continue;
+        if (rr_true < target) break;
+        if (rr_true < 0.5 * best) { best = rr_true; stall = 0; }
+        else if (++stall >= 8) { status = YG_STALL; break; }
+        f_from_d(L, fr, r, cnt);
+        set_scalar(L, S_RR0 + (it & 1), rr_true); // the slot the next iteration reads
+        maxrr = rr_true;
+        pending = false;            // the enqueued |r|^2 predates the update
       }
-      sloppy_xpay(L, p, (float)(rr_new / rr_s), fr);
-      rr_s = rr_new;
     }
   }
   int fallback = 0;
