@@ -203,6 +203,25 @@ int yg_clover_logdet_force(yg_lattice *lat, double mass, double residue);       
 int yg_wilson_gauge_force(yg_lattice *lat, double dt, double beta);                                 /* forces.cpp:262-283 */
 int yg_avr_plaquette(yg_lattice *lat, double *out);                                                 /* wilsonloop.cpp:116-133 (1x1) */
 
+/* ---- molecular dynamics on the fundamental links (update.cpp, forces.cpp, wilsonloop.cpp) ----
+ * Momenta stay on the device between these calls (yg_momenta_upload/download move them). */
+int yg_improved_gauge_force(yg_lattice *lat, double dt, double beta, double c0, double c1);        /* forces.cpp:285-309 */
+int yg_avr_wilson(yg_lattice *lat, int height, int width, double *out);                            /* wilsonloop.cpp:116-133 */
+int yg_gauge_action(yg_lattice *lat, double beta, double c0, double *out);                         /* monomials/gauge.cpp:21-40 */
+/* update.cpp:228-247: U <- exp(eps P) U with the momentum and link boundary conditions; like
+ * the reference it changes the fundamental links only, the represented field (and the clover
+ * term) follow at yg_represent_gauge_field */
+int yg_update_links(yg_lattice *lat, double eps);
+int yg_represent_gauge_field(yg_lattice *lat);                                                     /* repr.cpp:265-280 */
+int yg_reunitarize(yg_lattice *lat);                                                               /* update.cpp:269-279 */
+/* reset_variables, momentum part (update.cpp:254-267): Gaussian algebra components with the
+ * reference's standard deviation 1/sqrt(2) (random.h:15), drawn from a Philox4x32-10 stream
+ * keyed by seed (the reference's ranlux stream is not reproduced) */
+int yg_momenta_gaussian(yg_lattice *lat, unsigned long long seed);
+int yg_momenta_action(yg_lattice *lat, double *out);                /* hamiltonian(), momentum part: update.cpp:201-220 */
+int yg_gauge_backup(yg_lattice *lat);                                                              /* gaugefield.cpp:32-36 */
+int yg_gauge_restore(yg_lattice *lat);                                                             /* gaugefield.cpp:38-42 */
+
 /* ---- allocation-free reduction ------------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot allocate device memory (no
  * lattice handle needed): sum of |a_i|^2 over n_words complex FP64 words at dev_words,

@@ -86,7 +86,7 @@ class RefLattice:
         self.csw = csw
         self.cf = cf
         for fn in ("yref_spinor_sqnorm", "yref_spinor_product_re", "yref_clover_logdet",
-                   "yref_timestamp", "yref_avr_wilson"):
+                   "yref_timestamp", "yref_avr_wilson", "yref_hamiltonian"):
             getattr(lib, fn).restype = _D
         for fn, args in {
             "yref_Dphi_ee": [_D, _P, _P], "yref_Dphi_oo": [_D, _P, _P], "yref_Dphi_oo_inv": [_D, _P, _P],
@@ -106,6 +106,8 @@ class RefLattice:
             "yref_wilson_gauge_force": [_D, _D],
             "yref_improved_gauge_force": [_D, _D, _D, _D],
             "yref_avr_wilson": [_I, _I],
+            "yref_update_links": [_D], "yref_reunitarize": [], "yref_represent_gauge_field": [],
+            "yref_hamiltonian": [],
             "yref_represent": [_P, _P, _I],
         }.items():
             getattr(lib, fn).argtypes = args

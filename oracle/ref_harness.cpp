@@ -43,6 +43,11 @@
 #include <wilsonloop.h>
 #include <checks.h>
 #include <timing.h>
+#include <update.h>
+
+/* defined in library/update.cpp without a header declaration */
+double hamiltonian();
+void reunitarize();
 
 static int harness_ready = 0;
 
@@ -386,6 +391,12 @@ void yref_clover_logdet_force(double mass, double residue) { clover_logdet_force
 void yref_wilson_gauge_force(double dt, double beta) { wilson_gauge_force(dt, beta); }
 void yref_improved_gauge_force(double dt, double beta, double c0, double c1) { improved_gauge_force(dt, beta, c0, c1); }
 double yref_avr_wilson(int h, int w) { return avr_wilson(h, w); }
+
+/* ---- molecular-dynamics support (update.h) ---- */
+void yref_update_links(double eps) { update_links(eps); }
+void yref_reunitarize(void) { reunitarize(); }
+void yref_represent_gauge_field(void) { represent_gauge_field(); }
+double yref_hamiltonian(void) { return hamiltonian(); }     /* no monomials: the momentum part */
 
 /* ---- the reference's own self-checks (checks/check.cpp:4-26) ---- */
 int yref_check_group(void) { return check_group(); }

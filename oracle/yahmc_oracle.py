@@ -235,19 +235,20 @@ def represent(u: np.ndarray, nc: int, rep: str) -> np.ndarray:
 
 
 def exp_algebra(nc: int, alg: np.ndarray, coeff: float = 1.0) -> np.ndarray:
-    """exp(suNa, coeff): Taylor series to |X^k/k!|^2 < 1e-24 then reunitarize, suNa.cpp:113-134.
-    (Vectorised: the series runs until every matrix of the batch meets the bound.)"""
+    """exp(suNa, coeff): Taylor series then reunitarize, suNa.cpp:113-134.  Each matrix adds
+    terms (coeff/k) X^k / ... until the last added term has squared norm <= 1e-24, exactly
+    as the reference's loop does per matrix (the batch keeps a mask of unfinished ones)."""
     x = su_generator(nc, alg)
     xk = np.broadcast_to(np.eye(nc, dtype=complex), x.shape).copy()
     ret = xk.copy()
+    active = np.ones(x.shape[:-2], dtype=bool)
     k = 1
-    while True:
+    while np.any(active):
         xk = (coeff / k) * (xk @ x)
-        ret = ret + xk
+        ret[active] += xk[active]
         err = np.sum(np.abs(xk) ** 2, axis=(-1, -2))
+        active &= err > 1e-24
         k += 1
-        if np.all(err <= 1e-24):
-            break
     return reunitarize(ret)
 
 
@@ -1019,10 +1020,45 @@ class Oracle:
         if self.p.clover:
             self.clover_force_core(dt)
 
-    # ---- gauge support (staples.cpp, wilsonloop.cpp, forces.cpp:262-309)
+    # ---- gauge support (bcs.cpp, staples.cpp, wilsonloop.cpp, forces.cpp:262-309, update.cpp)
+    def plaq_weights(self):
+        """plaq_weight(id,mu,nu) as a (V, 4, 4) array, bcs.cpp:29-133: 1 everywhere except
+        0.5 on the spatial planes of t = 0 and t = T-1 (open) or t = 0 and t = T-2 (sf)."""
+        w = np.ones((self.V, 4, 4))
+        T = self.dims[0]
+        slices = {"open": [0, T - 1], "sf": [0, T - 2]}.get(self.p.bc, [])
+        for tt in slices:
+            for mu in (1, 2, 3):
+                for nu in (1, 2, 3):
+                    if mu != nu:
+                        w[self.t == tt, mu, nu] = 0.5
+        return w
+
+    def rect_weights(self):
+        """rect_weight(id,mu,nu), bcs.cpp:29-133: the plaquette weights (open: same array),
+        or for sf 0 on the planes (1,2),(1,3),(2,3) of t = 0 and T-2 and 1.5 on (0,1),(0,2),
+        (0,3) of t = 0 and T-3."""
+        if self.p.bc != "sf":
+            return self.plaq_weights()
+        w = np.ones((self.V, 4, 4))
+        T = self.dims[0]
+        for tt in (0, T - 2):
+            for (mu, nu) in ((1, 2), (1, 3), (2, 3)):
+                w[self.t == tt, mu, nu] = 0.0
+        for tt in (0, T - 3):
+            for nu in (1, 2, 3):
+                w[self.t == tt, 0, nu] = 1.5
+        return w
+
+    def volume(self):
+        """the global `volume` of the gauge action: V, (T-1) V3 for open, (T-2) V3 for sf
+        (bcs.cpp:32, 76)."""
+        v3 = self.V // self.dims[0]
+        return {"open": (self.dims[0] - 1) * v3, "sf": (self.dims[0] - 2) * v3}.get(self.p.bc, self.V)
+
     def staples_wilson(self, mu):
-        """staples_wilson, staples.cpp:83-107 (periodic/antiperiodic plaquette weights = 1)."""
-        U = self.fund
+        """staples_wilson, staples.cpp:83-107."""
+        U, pw = self.fund, self.plaq_weights()
         x = np.arange(self.V)
         st = np.zeros((self.V, self.nc, self.nc), dtype=complex)
         for nu in range(4):
@@ -1030,10 +1066,38 @@ class Oracle:
                 continue
             o1 = self.fw[x, mu]
             o2 = self.fw[x, nu]
-            st += U[o1, nu] @ dagger(U[x, nu] @ U[o2, mu])
+            st += pw[x, mu, nu][:, None, None] * (U[o1, nu] @ dagger(U[x, nu] @ U[o2, mu]))
             o1 = self.bk[x, nu]
             o2 = self.fw[o1, mu]
-            st += dagger(U[o1, mu] @ U[o2, nu]) @ U[o1, nu]
+            st += pw[o1, nu, mu][:, None, None] * (dagger(U[o1, mu] @ U[o2, nu]) @ U[o1, nu])
+        return st
+
+    def staples_symanzik(self, mu):
+        """staples_symanzik, staples.cpp:7-81: the six 2x1 rectangles through link (x,mu)
+        for each nu != mu."""
+        U, rw = self.fund, self.rect_weights()
+        fw, bk = self.fw, self.bk
+        x = np.arange(self.V)
+        st = np.zeros((self.V, self.nc, self.nc), dtype=complex)
+
+        def w(site, a, b):
+            return rw[site, a, b][:, None, None]
+
+        for nu in range(4):
+            if nu == mu:
+                continue
+            o1 = fw[x, mu]; o2 = fw[o1, nu]; o3 = fw[x, nu]; o4 = fw[o3, nu]
+            st += w(x, mu, nu) * (U[o1, nu] @ U[o2, nu] @ dagger(U[x, nu] @ U[o3, nu] @ U[o4, mu]))
+            o1 = bk[x, nu]; o2 = bk[o1, nu]; o3 = fw[o2, mu]; o4 = fw[o3, nu]
+            st += w(o2, mu, nu) * (dagger(U[o2, mu] @ U[o3, nu] @ U[o4, nu]) @ U[o2, nu] @ U[o1, nu])
+            o1 = bk[x, nu]; o2 = fw[o1, mu]; o3 = fw[o2, mu]; o4 = fw[x, mu]
+            st += w(o1, nu, mu) * (U[o4, mu] @ dagger(U[o1, mu] @ U[o2, mu] @ U[o3, nu]) @ U[o1, nu])
+            o1 = fw[x, mu]; o2 = fw[o1, mu]; o3 = fw[x, nu]; o4 = fw[o3, mu]
+            st += w(x, nu, mu) * (U[o1, mu] @ U[o2, nu] @ dagger(U[x, nu] @ U[o3, mu] @ U[o4, mu]))
+            o1 = bk[x, mu]; o2 = bk[o1, nu]; o3 = fw[o2, mu]; o4 = fw[o3, mu]
+            st += w(o2, nu, mu) * (dagger(U[o2, mu] @ U[o3, mu] @ U[o4, nu]) @ U[o2, nu] @ U[o1, mu])
+            o1 = bk[x, mu]; o2 = fw[o1, nu]; o3 = fw[o2, mu]; o4 = fw[x, mu]
+            st += w(o1, nu, mu) * (U[o4, nu] @ dagger(U[o1, nu] @ U[o2, mu] @ U[o3, mu]) @ U[o1, mu])
         return st
 
     def wilson_gauge_force(self, dt, beta):
@@ -1043,15 +1107,118 @@ class Oracle:
             f = self.fund[:, mu] @ self.staples_wilson(mu)
             self.mom[:, mu] -= algebra_project(f, self.itfund, coeff)
 
-    def plaquette(self):
-        """avr_wilson(1,1), wilsonloop.cpp:116-133 (weights 1)."""
-        U = self.fund
+    def improved_gauge_force(self, dt, beta, c0, c1):
+        """forces.cpp:285-309"""
+        coeff = dt * (beta / self.nc)
+        for mu in range(4):
+            f = c0 * (self.fund[:, mu] @ self.staples_wilson(mu)) + c1 * (self.fund[:, mu] @ self.staples_symanzik(mu))
+            self.mom[:, mu] -= algebra_project(f, self.itfund, coeff)
+
+    def wilson_loop(self, mu, nu, height, width):
+        """wilson_loop(id,mu,nu,height,width) for every site, wilsonloop.cpp:56-114."""
+        U, fw = self.fund, self.fw
         x = np.arange(self.V)
+        one = U[x, mu].copy()
+        two = U[x, nu].copy()
+        pos = x
+        for _ in range(1, height):
+            pos = fw[pos, mu]
+            one = one @ U[pos, mu]
+        pos = fw[pos, mu]
+        one = one @ U[pos, nu]
+        for _ in range(1, width):
+            pos = fw[pos, nu]
+            one = one @ U[pos, nu]
+        pos = x
+        for _ in range(1, width):
+            pos = fw[pos, nu]
+            two = two @ U[pos, nu]
+        pos = fw[pos, nu]
+        two = two @ U[pos, mu]
+        for _ in range(1, height):
+            pos = fw[pos, mu]
+            two = two @ U[pos, mu]
+        tr = np.einsum("vij,vji->v", one, dagger(two)).real
+        if (height, width) == (1, 1):
+            tr = tr * self.plaq_weights()[x, mu, nu]
+        elif (height, width) == (1, 2):
+            tr = tr * self.rect_weights()[x, mu, nu]
+        elif (height, width) == (2, 1):
+            tr = tr * self.rect_weights()[x, nu, mu]
+        return tr
+
+    def avr_wilson(self, height, width):
+        """wilsonloop.cpp:116-133"""
         s = 0.0
         for (mu, nu) in [(1, 0), (2, 0), (2, 1), (3, 0), (3, 1), (3, 2)]:
-            a = self.fw[x, mu]
-            b = self.fw[x, nu]
-            one = U[x, mu] @ U[a, nu]
-            two = U[x, nu] @ U[b, mu]
-            s += np.einsum("vij,vji->", one, dagger(two)).real
-        return s / (self.nc * 6 * self.V)
+            s += self.wilson_loop(mu, nu, height, width).sum()
+        return s / (self.nc * 6 * self.volume())
+
+    def plaquette(self):
+        """avr_wilson(1,1)"""
+        return self.avr_wilson(1, 1)
+
+    def gauge_action(self, beta, c0):
+        """MonomialGauge::action, monomials/gauge.cpp:21-40 (c1 = (1-c0)/8)."""
+        c1 = (1.0 - c0) / 8.0
+        if abs(c1) > 1e-8:
+            v = c0 * self.avr_wilson(1, 1) + c1 * (self.avr_wilson(2, 1) + self.avr_wilson(1, 2))
+        else:
+            v = self.avr_wilson(1, 1)
+        return -beta * v * 6 * self.volume()
+
+    def bcs_on_momenta(self):
+        """apply_bcs_on_momentum_field, bcs.cpp:166-199"""
+        T = self.dims[0]
+        if self.p.bc == "open":
+            self.mom[self.t == T - 1, 0] = 0
+        elif self.p.bc == "sf":
+            self.mom[self.t == 0, 1:] = 0
+            self.mom[self.t == T - 2] = 0
+            self.mom[self.t == T - 1] = 0
+
+    def sf_boundary_links(self):
+        """C1, C2 of apply_bcs_on_gauge_field (bcs.cpp:211-245): diag exp(i v_k / L)."""
+        nc = self.nc
+        if nc == 2:
+            v1, v2, L = [-math.pi, math.pi], [-3 * math.pi, 3 * math.pi], 4 * self.dims[1]
+        elif nc == 3:
+            v1, v2, L = [-math.pi, 0, math.pi], [-5 * math.pi, 2 * math.pi, 3 * math.pi], 6 * self.dims[1]
+        else:
+            raise ValueError("sf boundary fields exist for SU(2) and SU(3)")
+        c1 = np.diag(np.exp(1j * np.array(v1) / L))
+        c2 = np.diag(np.exp(1j * np.array(v2) / L))
+        return c1, c2
+
+    def bcs_on_gauge(self):
+        """apply_bcs_on_gauge_field, bcs.cpp:201-262"""
+        T = self.dims[0]
+        if self.p.bc == "open":
+            self.fund[self.t == T - 1, 0] = 0
+        elif self.p.bc == "sf":
+            c1, c2 = self.sf_boundary_links()
+            self.fund[self.t == 0, 1:] = c1
+            self.fund[self.t == T - 2, 0] = 0
+            self.fund[self.t == T - 2, 1:] = c2
+            self.fund[self.t == T - 1] = 0
+
+    def update_links(self, eps):
+        """update.cpp:228-247: U <- exp(eps P) U with the boundary conditions.  As there, the
+        represented field is rebuilt only by represent_gauge_field()."""
+        self.bcs_on_momenta()
+        self.fund = exp_algebra(self.nc, self.mom, eps) @ self.fund
+        self.bcs_on_gauge()
+
+    def represent_gauge_field(self):
+        """repr.cpp:265-280 (with the clover term and the antiperiodic sign)"""
+        self.set_links(self.fund)
+
+    def reunitarize_links(self):
+        """update.cpp:269-279 (the represented field is rebuilt by the caller, as there)."""
+        self.fund = reunitarize(self.fund)
+
+    def hamiltonian_momenta(self):
+        """the momentum part of hamiltonian(), update.cpp:201-226: (TF/2) sum |P|^2 after the
+        momentum boundary conditions."""
+        self.bcs_on_momenta()
+        return TF / 2.0 * float(np.sum(self.mom ** 2))

@@ -153,3 +153,36 @@ def test_reference_self_checks_pass():
     assert R.call("check_group") == 0
     assert R.call("check_dirac") == 0
     assert R.call("check_inverters") == 0
+
+
+@pytest.mark.parametrize("name", ["su3_fund_ap", "su3_fund_per", "su3_fund_open", "su3_fund_sf", "su2_fund_ap",
+                                  "su4_fund_ap"])
+def test_md_support(name):
+    """Weighted Wilson loops, the Symanzik force, the momentum part of hamiltonian(),
+    update_links (exp, momentum and link boundary conditions) and reunitarize."""
+    R, O, rng, src = _setup(name, 6)
+    V, nc = O.V, O.nc
+    mom = rng.normal(0.0, 2 ** -0.5, (V, 4, nc * nc - 1))
+    R.lib.yref_set_momenta(ref._ptr(np.ascontiguousarray(mom.reshape(-1))))
+    O.mom[:] = mom
+    for h, w in [(1, 1), (1, 2), (2, 1)]:
+        assert abs(R.call("avr_wilson", h, w) - O.avr_wilson(h, w)) < 1e-14
+    c0 = 5.0 / 3.0
+    R.call("improved_gauge_force", 0.1, 5.6, c0, (1 - c0) / 8)
+    O.improved_gauge_force(0.1, 5.6, c0, (1 - c0) / 8)
+    assert _rel(R.momenta().reshape(V, 4, -1), O.mom) < TOL
+    h_ref = R.call("hamiltonian")
+    assert abs(h_ref - O.hamiltonian_momenta()) < 1e-13 * abs(h_ref)
+    assert _rel(R.momenta().reshape(V, 4, -1), O.mom) < TOL
+    R.call("update_links", 0.13)
+    O.update_links(0.13)
+    assert _rel(yo.mat_from_raw(R.get_links(), nc).reshape(V, 4, nc, nc), O.fund) < 1e-13
+    R.call("represent_gauge_field")
+    O.represent_gauge_field()
+    assert _rel(yo.mat_from_raw(R.repr_links(), O.d).reshape(V, 4, O.d, O.d), O.links) < 1e-13
+    Up = O.fund + 1e-3 * (rng.normal(size=O.fund.shape) + 1j * rng.normal(size=O.fund.shape))
+    R.set_links(fields.complex_to_raw(Up))
+    O.fund = Up.copy()
+    R.call("reunitarize")
+    O.reunitarize_links()
+    assert _rel(yo.mat_from_raw(R.get_links(), nc).reshape(V, 4, nc, nc), O.fund) < 1e-12

@@ -106,6 +106,10 @@ _SIGNATURES = {
     "yg_wilson_fermion_force": [_P, _D, _D, _D, _P, _P], "yg_wilson_fermion_force_q": [_P, _D, _D, _D, _P],
     "yg_clover_fermion_force": [_P, _D, _P, _P], "yg_clover_logdet_force": [_P, _D, _D],
     "yg_wilson_gauge_force": [_P, _D, _D], "yg_avr_plaquette": [_P, _P],
+    "yg_improved_gauge_force": [_P, _D, _D, _D, _D], "yg_avr_wilson": [_P, _I, _I, _P],
+    "yg_gauge_action": [_P, _D, _D, _P], "yg_update_links": [_P, _D], "yg_represent_gauge_field": [_P],
+    "yg_reunitarize": [_P], "yg_momenta_gaussian": [_P, ctypes.c_ulonglong], "yg_momenta_action": [_P, _P],
+    "yg_gauge_backup": [_P], "yg_gauge_restore": [_P],
     "yg_field_sqnorm_noalloc": [_P, ctypes.c_long, _P, _P],
 }
 
@@ -407,3 +411,40 @@ class Lattice:
         out = ctypes.c_double()
         self._check(self.lib.yg_avr_plaquette(self.h, ctypes.byref(out)))
         return out.value
+
+    # ---- molecular dynamics (update.cpp, forces.cpp:262-309, wilsonloop.cpp)
+    def improved_gauge_force(self, dt, beta, c0, c1):
+        self._check(self.lib.yg_improved_gauge_force(self.h, dt, beta, c0, c1))
+
+    def avr_wilson(self, height, width):
+        out = ctypes.c_double()
+        self._check(self.lib.yg_avr_wilson(self.h, int(height), int(width), ctypes.byref(out)))
+        return out.value
+
+    def gauge_action(self, beta, c0=1.0):
+        """MonomialGauge::action with c1 = (1 - c0)/8"""
+        out = ctypes.c_double()
+        self._check(self.lib.yg_gauge_action(self.h, beta, c0, ctypes.byref(out)))
+        return out.value
+
+    def update_links(self, eps):
+        """U <- exp(eps P) U on the fundamental links; call represent_gauge_field() before
+        the Dirac operator sees them, as in the reference"""
+        self._check(self.lib.yg_update_links(self.h, eps))
+
+    def represent_gauge_field(self): self._check(self.lib.yg_represent_gauge_field(self.h))
+
+    def reunitarize(self): self._check(self.lib.yg_reunitarize(self.h))
+
+    def momenta_gaussian(self, seed):
+        self._check(self.lib.yg_momenta_gaussian(self.h, int(seed) & 0xFFFFFFFFFFFFFFFF))
+
+    def momenta_action(self):
+        """(TF/2) sum P^2 after the momentum boundary conditions (applied in place)"""
+        out = ctypes.c_double()
+        self._check(self.lib.yg_momenta_action(self.h, ctypes.byref(out)))
+        return out.value
+
+    def gauge_backup(self): self._check(self.lib.yg_gauge_backup(self.h))
+
+    def gauge_restore(self): self._check(self.lib.yg_gauge_restore(self.h))

@@ -271,4 +271,26 @@ int yg_clover_logdet_force(yg_lattice *l, double m, double res) { return guard([
 int yg_wilson_gauge_force(yg_lattice *l, double dt, double beta) { return guard([&] { yg::wilson_gauge_force(lat(l), dt, beta); }); }
 int yg_avr_plaquette(yg_lattice *l, double *out) { return guard([&] { need(out, "out"); *out = yg::avr_plaquette(lat(l)); }); }
 
+// ---- molecular dynamics
+int yg_improved_gauge_force(yg_lattice *l, double dt, double beta, double c0, double c1) {
+  return guard([&] { yg::improved_gauge_force(lat(l), dt, beta, c0, c1); });
+}
+int yg_avr_wilson(yg_lattice *l, int h, int w, double *out) {
+  return guard([&] { need(out, "out"); *out = yg::avr_wilson(lat(l), h, w); });
+}
+int yg_gauge_action(yg_lattice *l, double beta, double c0, double *out) {
+  return guard([&] { need(out, "out"); *out = yg::gauge_action(lat(l), beta, c0); });
+}
+int yg_update_links(yg_lattice *l, double eps) { return guard([&] { yg::update_links(lat(l), eps); }); }
+int yg_represent_gauge_field(yg_lattice *l) {
+  return guard([&] { yg::Lattice &L = lat(l); yg::represent_and_clover(L); YG_CUDA(cudaStreamSynchronize(L.stream)); });
+}
+int yg_reunitarize(yg_lattice *l) { return guard([&] { yg::reunitarize(lat(l)); }); }
+int yg_momenta_gaussian(yg_lattice *l, unsigned long long seed) { return guard([&] { yg::momenta_gaussian(lat(l), seed); }); }
+int yg_momenta_action(yg_lattice *l, double *out) {
+  return guard([&] { need(out, "out"); *out = yg::momenta_action(lat(l)); });
+}
+int yg_gauge_backup(yg_lattice *l) { return guard([&] { yg::gauge_backup(lat(l)); }); }
+int yg_gauge_restore(yg_lattice *l) { return guard([&] { yg::gauge_restore(lat(l)); }); }
+
 }  // extern "C"

@@ -59,14 +59,6 @@ void end_fermion_force(Lattice &L, double dt) {
   YG_LAUNCHED();
 }
 
-void wilson_gauge_force(Lattice &L, double dt, double beta) {
-  if (L.p.bc == YG_BC_OPEN || L.p.bc == YG_BC_SF)
-    throw Error(YG_ERR_ARG, "gauge force with open/SF plaquette weights is not provided");
-  double coeff = dt * (beta / L.nc);
-  YG_DISPATCH_N(L.nc, K::gauge_force(L.mom.as<double>(), L.fund.as<double2>(), L.g, L.rt.itfund, coeff, L.stream));
-  YG_LAUNCHED();
-}
-
 double clover_logdet(Lattice &L, double mass) {
   if (!L.p.clover) return 0.0;
   ensure_ldl(L, 4.0 + mass);
@@ -74,15 +66,6 @@ double clover_logdet(Lattice &L, double mass) {
   YG_DISPATCH_D(L.d, K::logdet(tmp, L.ldl.as<double2>(), (int)L.Vh, L.stream));
   YG_LAUNCHED();
   return sum_device(L, tmp, L.Vh);
-}
-
-double avr_plaquette(Lattice &L) {
-  if (L.p.bc == YG_BC_OPEN || L.p.bc == YG_BC_SF)
-    throw Error(YG_ERR_ARG, "plaquette with open/SF weights is not provided");
-  double *tmp = L.scratch_field(0);
-  YG_DISPATCH_N(L.nc, K::plaquette(tmp, L.fund.as<double2>(), L.g, L.stream));
-  YG_LAUNCHED();
-  return sum_device(L, tmp, L.V) / (L.nc * 6.0 * L.V);
 }
 
 }  // namespace yg

@@ -280,62 +280,6 @@ __global__ void k_clover_force_core(double *mom, const double2 *clf, const doubl
   }
 }
 
-// ---- wilson_gauge_force, forces.cpp:262-283 with staples_wilson, staples.cpp:83-107
-template <int NC>
-__global__ void k_wilson_gauge_force(double *mom, const double2 *fund, Geom g, const double2 *itfund, double coeff) {
-  constexpr int D = NC;
-  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (t >= 4L * g.V) return;
-  int id = (int)(t >> 2), mu = (int)(t & 3);
-  int c[4], cc[4];
-  coords_of(g, id, c);
-  double2 st[D * D], A[D * D], B[D * D], P[D * D], Q[D * D];
-  for (int k = 0; k < D * D; k++) st[k] = make_double2(0, 0);
-  for (int nu = 0; nu < 4; nu++) {
-    if (nu == mu) continue;
-    int o1 = neighbour(g, c, mu, +1), o2 = neighbour(g, c, nu, +1);
-    ld_mat<D>(A, fund, g, id, nu, 4); ld_mat<D>(B, fund, g, o2, mu, 4); mat_mul<D>(P, A, B);
-    dag<D>(Q, P);
-    ld_mat<D>(A, fund, g, o1, nu, 4); mat_mul<D>(P, A, Q);
-    for (int k = 0; k < D * D; k++) st[k] = cadd(st[k], P[k]);
-    int b1 = neighbour(g, c, nu, -1);
-    coords_of(g, b1, cc);
-    int b2 = neighbour(g, cc, mu, +1);
-    ld_mat<D>(A, fund, g, b1, mu, 4); ld_mat<D>(B, fund, g, b2, nu, 4); mat_mul<D>(P, A, B);
-    dag<D>(Q, P);
-    ld_mat<D>(A, fund, g, b1, nu, 4); mat_mul<D>(P, Q, A);
-    for (int k = 0; k < D * D; k++) st[k] = cadd(st[k], P[k]);
-  }
-  ld_mat<D>(A, fund, g, id, mu, 4);
-  mat_mul<D>(P, A, st);
-  project_add<D>(mom + (4L * id + mu) * (NC * NC - 1), P, itfund, NC * NC - 1, -coeff);
-}
-
-// per-site sum of Re tr(plaquette) over the six planes (avr_wilson(1,1), wilsonloop.cpp:116-133)
-template <int NC>
-__global__ void k_plaquette(double *out, const double2 *fund, Geom g) {
-  constexpr int D = NC;
-  int id = blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= g.V) return;
-  int c[4];
-  coords_of(g, id, c);
-  const int pl[6][2] = {{1, 0}, {2, 0}, {2, 1}, {3, 0}, {3, 1}, {3, 2}};
-  double s = 0;
-  double2 A[D * D], B[D * D], P[D * D], Q[D * D];
-  for (int q = 0; q < 6; q++) {
-    int mu = pl[q][0], nu = pl[q][1];
-    int a = neighbour(g, c, mu, +1), b = neighbour(g, c, nu, +1);
-    ld_mat<D>(A, fund, g, id, mu, 4); ld_mat<D>(B, fund, g, a, nu, 4); mat_mul<D>(P, A, B);
-    ld_mat<D>(A, fund, g, id, nu, 4); ld_mat<D>(B, fund, g, b, mu, 4); mat_mul<D>(Q, A, B);
-    for (int i = 0; i < NC; i++)
-      for (int k = 0; k < NC; k++) {
-        double2 x = P[i * NC + k], y = Q[i * NC + k];    // tr(P Q^dag) = sum P_ik conj(Q_ik)
-        s += x.x * y.x + x.y * y.y;
-      }
-  }
-  out[id] = s;
-}
-
 // ------------------------------------------------------------------ launchers
 template <int D>
 void DK<D>::clover_fermion_force(double2 *clf, const double2 *lhs, const double2 *rhs, Geom g, double residue,
@@ -358,16 +302,6 @@ template <int D>
 void DK<D>::clover_force_core(double *mom, const double2 *clf, const double2 *U, Geom g, const double2 *itrepr, int ng,
                               double coeff, cudaStream_t s) {
   k_clover_force_core<D><<<nblk(4L * g.V, 64), 64, 0, s>>>(mom, clf, U, g, itrepr, ng, coeff);
-}
-
-template <int NC>
-void GK<NC>::gauge_force(double *mom, const double2 *fund, Geom g, const double2 *itfund, double coeff, cudaStream_t s) {
-  k_wilson_gauge_force<NC><<<nblk(4L * g.V, 64), 64, 0, s>>>(mom, fund, g, itfund, coeff);
-}
-
-template <int NC>
-void GK<NC>::plaquette(double *out, const double2 *fund, Geom g, cudaStream_t s) {
-  k_plaquette<NC><<<nblk(g.V, 128), 128, 0, s>>>(out, fund, g);
 }
 
 }  // namespace yg

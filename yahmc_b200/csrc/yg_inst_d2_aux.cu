@@ -9,5 +9,4 @@ template void DK<2>::hopping_force(double *, const double2 *, const double2 *, c
 template void DK<2>::clover_ldl_force(double2 *, const double2 *, Geom, double, cudaStream_t);
 template void DK<2>::clover_force_core(double *, const double2 *, const double2 *, Geom, const double2 *, int, double, cudaStream_t);
 template struct RK<2, 2>;
-template struct GK<2>;
 }  // namespace yg

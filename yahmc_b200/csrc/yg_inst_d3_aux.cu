@@ -10,5 +10,4 @@ template void DK<3>::clover_ldl_force(double2 *, const double2 *, Geom, double, 
 template void DK<3>::clover_force_core(double *, const double2 *, const double2 *, Geom, const double2 *, int, double, cudaStream_t);
 template struct RK<2, 3>;
 template struct RK<3, 3>;
-template struct GK<3>;
 }  // namespace yg

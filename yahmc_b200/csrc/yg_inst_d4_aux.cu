@@ -9,5 +9,4 @@ template void DK<4>::hopping_force(double *, const double2 *, const double2 *, c
 template void DK<4>::clover_ldl_force(double2 *, const double2 *, Geom, double, cudaStream_t);
 template void DK<4>::clover_force_core(double *, const double2 *, const double2 *, Geom, const double2 *, int, double, cudaStream_t);
 template struct RK<4, 4>;
-template struct GK<4>;
 }  // namespace yg

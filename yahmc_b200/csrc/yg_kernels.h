@@ -63,13 +63,6 @@ struct RK {
                           cudaStream_t s);
 };
 
-// Gauge-side kernels on the fundamental links
-template <int NC>
-struct GK {
-  static void gauge_force(double *mom, const double2 *fund, Geom g, const double2 *itfund, double coeff,
-                          cudaStream_t s);
-  static void plaquette(double *out, const double2 *fund, Geom g, cudaStream_t s);
-};
 
 // run-time D -> DK<D>
 #define YG_DISPATCH_D(DV, CALL)                                                              \
@@ -101,16 +94,6 @@ struct GK {
     else if (NCV == 4 && DV == 10) { using K = ::yg::RK<4, 10>; CALL; }                      \
     else if (NCV == 4 && DV == 15) { using K = ::yg::RK<4, 15>; CALL; }                      \
     else throw ::yg::Error(YG_ERR_ARG, "unsupported (N, representation) pair");              \
-  } while (0)
-
-#define YG_DISPATCH_N(NCV, CALL)                                                             \
-  do {                                                                                       \
-    switch (NCV) {                                                                           \
-      case 2: { using K = ::yg::GK<2>; CALL; } break;                                        \
-      case 3: { using K = ::yg::GK<3>; CALL; } break;                                        \
-      case 4: { using K = ::yg::GK<4>; CALL; } break;                                        \
-      default: throw ::yg::Error(YG_ERR_ARG, "unsupported N");                               \
-    }                                                                                        \
   } while (0)
 
 static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }

@@ -45,7 +45,7 @@ Lattice::~Lattice() {
   if (sl_hist) cudaFreeHost(sl_hist);
   for (cudaEvent_t e : sl_ev) if (e) cudaEventDestroy(e);
   for (DevBuf *b : {&fund, &links, &clover, &ldl, &cl_force, &mom, &tables, &red_partial, &red_result, &links_f,
-                    &clover_f, &cinv_f, &sl_links, &sl_clover, &cpk64, &sl_part, &sl_scal})
+                    &clover_f, &cinv_f, &sl_links, &sl_clover, &cpk64, &sl_part, &sl_scal, &fund_backup})
     b->release();
 }
 

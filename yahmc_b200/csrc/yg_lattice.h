@@ -54,6 +54,7 @@ struct Lattice {
   int mvm = 0;
 
   DevBuf fund;      // fundamental links, 4 x N x N per site        (gfield_fund)
+  DevBuf fund_backup;  // gauge_field_backup copy of fund
   DevBuf links;     // represented links with the AP sign, 4 x d x d (gfield_repr)
   DevBuf clover;    // clover term, 4 x d x d per site                (cl_term)
   DevBuf ldl;       // LDL factors, 2 x d(2d+1) per site of block 1   (cl_ldl)
@@ -180,5 +181,16 @@ void clover_logdet_force(Lattice &L, double mass, double residue);
 void wilson_gauge_force(Lattice &L, double dt, double beta);
 double clover_logdet(Lattice &L, double mass);
 double avr_plaquette(Lattice &L);
+
+// molecular-dynamics support on the fundamental links (yg_gauge.cu)
+void improved_gauge_force(Lattice &L, double dt, double beta, double c0, double c1);
+double avr_wilson(Lattice &L, int height, int width);
+double gauge_action(Lattice &L, double beta, double c0);
+void update_links(Lattice &L, double eps);
+void reunitarize(Lattice &L);
+void momenta_gaussian(Lattice &L, unsigned long long seed);
+double momenta_action(Lattice &L);
+void gauge_backup(Lattice &L);
+void gauge_restore(Lattice &L);
 
 }  // namespace yg
