@@ -4,7 +4,8 @@ Workload (defaults): 32^4 SU(3) fundamental, even-odd preconditioned Wilson-clov
 m = -0.75, csw = 1.0, periodic space / antiperiodic time.  One step = one solve of
 Hphi_sq x = b (the D^dag D system of cg_inverter, cg.cpp:132-202) to a TRUE FP64
 relative residual of 1e-12 (prec = 1e-24 in the reference's squared convention), with
-the mixed-precision solver (FP32 inner iterations, FP64 reliable updates).
+the mixed-precision solver (compressed FP32 inner operator with 12-real links, FP64
+reliable updates and stopping test).
 
 Reported beside it: the same solve with the plain FP64 CG (the reference's algorithm on
 the GPU), the FP64 Dslash (Dphi_oe) bandwidth against the measured HBM peak, the same
@@ -12,11 +13,11 @@ metric end to end through the public API with the source uploaded from pinned ho
 memory and the solution downloaded every step, and the reference's own CPU code
 (oracle/_ref, built from the reference sources) timed on this host's cores.
 
-Synthetic inputs: links are the reference's random start (exp of a Gaussian su(3)
-algebra element per link, library/suNg.cpp:375-380) from a fixed seed, standing in for
-a thermalised beta=5.6 field; the source is a complex Gaussian, unit variance per
-component.  Every input (links 604 MB, clover 604 MB, fields 201 MB each) is larger than
-the 126 MB L2, so no flush is needed between timed steps.
+Synthetic inputs: a thermalised beta = 5.6 field made on the GPU before timing: pure-gauge
+HMC (Wilson action, o2mn integrator, 150 trajectories from a cold start) on 16^3x32, tiled
+2x2x2x1 to 32^4 (a periodic field with the same local action density); the source is a
+complex Gaussian, unit variance per component.  Every input (links 604 MB, clover 604 MB,
+fields 201 MB each) is larger than the 126 MB L2, so no flush is needed between steps.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                        [--dims T X Y Z] [--no-cpu-baseline]
@@ -39,6 +40,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 MASS, CSW, PREC = -0.75, 1.0, 1e-24
+CPU_SAMPLE_PREC = 1e-8      # squared relative residual of the bounded CPU-baseline sample
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
@@ -53,10 +55,10 @@ def parse():
     ap.add_argument("--seed", type=int, default=20241203)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dslash-iters", type=int, default=50)
-    ap.add_argument("--inner", default="f16-l12", choices=list(INNER),
+    ap.add_argument("--inner", default="f32-l12", choices=list(INNER),
                     help="inner operator of the mixed solver: generic FP32, or the compressed d = 3 "
                          "operator with FP32/FP16 spinors and 18/12-real links")
-    ap.add_argument("--delta", type=float, default=0.1, help="reliable-update threshold")
+    ap.add_argument("--delta", type=float, default=0.003, help="reliable-update threshold")
     ap.add_argument("--variants", action="store_true", help="also time every inner operator once")
     ap.add_argument("--solve-only", action="store_true",
                     help="time only the mixed solve and print its time (for profiling; not the bench line)")
@@ -65,7 +67,7 @@ def parse():
 
 # inner operator of the mixed-precision solver: None = generic FP32 (every representation),
 # (spinor bits, link reals) = the compressed d = 3 operator
-INNER = {"generic-f32": None, "f32-l18": (32, 18), "f32-l12": (32, 12), "f16-l18": (16, 18), "f16-l12": (16, 12)}
+INNER = {"generic-f32": (0, 18), "f32-l18": (32, 18), "f32-l12": (32, 12), "f16-l18": (16, 18), "f16-l12": (16, 12)}
 
 
 DTYPE = {"generic-f32": "f32 inner / f64 reliable updates and residual",
@@ -77,8 +79,6 @@ DTYPE = {"generic-f32": "f32 inner / f64 reliable updates and residual",
 
 def solve_mixed(lat, x, b, inner, delta):
     spec = INNER[inner]
-    if spec is None:
-        return lat.cg_mixed("Hphi_sq", MASS, PREC, x, b)
     return lat.cg_mixed("Hphi_sq", MASS, PREC, x, b, inner_precision=spec[0], link_reals=spec[1], delta=delta)
 
 
@@ -90,14 +90,44 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+THERM = {"beta": 5.6, "c0": 1.0, "trajectories": 150, "warmup_md": 10, "steps": 100, "length": 1.0,
+         "integrator": "o2mn", "start": "cold"}
+
+
+def thermalised_links(dims, seed):
+    """A thermalised SU(3) field for the workload: pure-gauge HMC (Wilson action, beta 5.6)
+    on the lattice with the spatial extents halved, from a cold start, then tiled 1x2x2x2
+    (for 32^4: a thermalised 16^3x32 field tiled 2x2x2x1, again a periodic field).
+    Generated on the GPU by the engine's molecular-dynamics kernels; returns (U, plaquette)."""
+    import yahmc_b200 as yg
+    from yahmc_b200 import thermalize as th
+    small = (dims[0],) + tuple(d // 2 if d % 4 == 0 else d for d in dims[1:])
+    lat = yg.Lattice(small, nc=3, repr="fundamental", bc="periodic", clover=False, eo=True)
+    lat.set_links(np.broadcast_to(np.eye(3, dtype=complex), (lat.V, 4, 3, 3)).copy())
+    hist = th.thermalize(lat, THERM["beta"], THERM["trajectories"], steps=THERM["steps"], length=THERM["length"],
+                         c0=THERM["c0"], seed=seed, integrator=THERM["integrator"], n_warm=THERM["warmup_md"])
+    acc = float(np.mean([h[0] for h in hist[THERM["warmup_md"]:]]))
+    U = th.tile(lat.get_links(), small, tuple(dims))
+    plaq = float(hist[-1][2])
+    del lat
+    return U, plaq, acc
+
+
 def make_inputs(dims, seed, rank=0):
     from yahmc_b200 import fields
+    U, plaq, acc = thermalised_links(dims, seed)
     T, X, Y, Z = dims
     V = T * X * Y * Z
     rng = np.random.default_rng(seed + 7919 * rank)
-    U = fields.random_start_su(3, 4 * V, rng).reshape(V, 4, 3, 3)
     b = fields.gaussian_spinor(V, 3, rng)
-    return U, b
+    return U, b, {"plaquette": plaq, "acceptance": acc}
+
+
+def links_desc(info):
+    return (f"thermalised: {THERM['trajectories']} pure-gauge HMC trajectories (Wilson action, beta "
+            f"{THERM['beta']}, {THERM['integrator']} {THERM['steps']} steps, length {THERM['length']}, first "
+            f"{THERM['warmup_md']} without accept/reject) from a cold start on the lattice with halved spatial "
+            f"extents, tiled 1x2x2x2; plaquette {info['plaquette']:.5f}, acceptance {info['acceptance']:.2f}")
 
 
 def workload_name(dims):
@@ -146,9 +176,10 @@ class Clocks:
 
 
 # ------------------------------------------------------------------ reference (CPU) arm
-def reference_solve_ms(dims, U, b, steps, threads):
+def reference_solve_ms(dims, U, b, steps, threads, prec=PREC):
     """The reference's own cg_inverter (oracle/_ref, compiled from the reference sources) on
-    Hphi_sq with the same links, source and squared precision; returns (ms per solve, iters)."""
+    Hphi_sq with the same links and source to squared precision prec; returns (ms per
+    solve, iterations)."""
     from oracle import ref as oref
     from oracle import yahmc_oracle as yo
     from yahmc_b200 import fields
@@ -161,7 +192,7 @@ def reference_solve_ms(dims, U, b, steps, threads):
         x = R.spinor()
         bb = braw.copy()
         t0 = time.perf_counter()
-        it = R.call("cg", 2, MASS, PREC, x, bb)
+        it = R.call("cg", 2, MASS, prec, x, bb)
         times.append((time.perf_counter() - t0) * 1e3)
         its.append(it)
     return float(np.median(times)), int(its[-1])
@@ -175,19 +206,22 @@ def run_reference(a, rank, world):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (no reference sources on this host)"}))
         return
     threads = os.cpu_count() or 1
-    U, b = make_inputs(a.dims, a.seed)
-    steps = max(1, min(a.steps, 3))
-    warm = min(a.warmup, 1)
-    if warm:
-        reference_solve_ms(a.dims, U, b, warm, threads)
+    import yahmc_b200 as yg
+    yg.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    U, b, info = make_inputs(a.dims, a.seed)        # input preparation only (GPU thermalisation)
+    # one full solve is the bounded sample: about a minute on 16 host cores at 32^4; the
+    # reference code has no warm-up effect worth a second minute
+    steps, warm = 1, 0
     ms, it = reference_solve_ms(a.dims, U, b, steps, threads)
     line = {
         "impl": "reference", "metric": "CG time-to-solution (true rel. residual 1e-12)", "value": ms, "unit": "ms",
         "n_gpus": a.gpus, "steps": steps, "warmup": warm, "ms_per_step": ms, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(a.dims), "iterations": it, "threads": threads},
+        "config": {"workload": workload_name(a.dims), "iterations": it, "threads": threads,
+                   "links": links_desc(info)},
         "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
-                         "sample": f"{steps} full reference cg_inverter solves (prec 1e-24) on {threads} OpenMP threads"},
+                         "sample": f"{steps} full reference cg_inverter solve (prec 1e-24, {it} iterations) on "
+                                   f"{threads} OpenMP threads"},
         "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -199,7 +233,8 @@ def run_ours(a, rank, world, dist):
     import yahmc_b200 as yg
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
     dev = torch.cuda.current_device()
-    U, b = make_inputs(a.dims, a.seed, rank)
+    yg.set_device(dev)
+    U, b, info = make_inputs(a.dims, a.seed, rank)
     lat = yg.Lattice(a.dims, nc=3, repr="fundamental", bc="antiperiodic", clover=True, eo=True, csw=CSW)
     lat.set_links(U)
     V, d = lat.V, lat.d
@@ -309,10 +344,12 @@ def run_ours(a, rank, world, dist):
             from oracle import ref as oref
             if oref.available("su3_fund_ap"):
                 threads = os.cpu_count() or 1
-                cms, cit = reference_solve_ms(a.dims, U, b, 1, threads)
-                cpu = {"value": cms, "unit": "ms", "cores": threads, "kind": "reference",
-                       "sample": f"1 full reference cg_inverter solve (prec 1e-24, {cit} iterations) of the same "
-                                 f"system on {threads} OpenMP threads"}
+                cms, cit = reference_solve_ms(a.dims, U, b, 1, threads, prec=CPU_SAMPLE_PREC)
+                cpu = {"value": cms / cit * it_fp64, "unit": "ms", "cores": threads, "kind": "reference",
+                       "sample": f"reference cg_inverter on the same system stopped at prec {CPU_SAMPLE_PREC:g} "
+                                 f"({cit} iterations, {cms / 1e3:.1f} s on {threads} OpenMP threads), scaled to the "
+                                 f"{it_fp64} iterations of the full solve (the FP64 CG on the GPU runs the "
+                                 f"reference's iteration)"}
             else:
                 cpu = {"value": None, "unit": "ms", "cores": 0, "kind": "reference",
                        "sample": "oracle/_ref not built on this host"}
@@ -328,7 +365,7 @@ def run_ours(a, rank, world, dist):
         "ms_per_step": ms_mixed, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": DTYPE[a.inner], "data": "synthetic",
         "config": {"workload": workload_name(a.dims), "mass": MASS, "csw": CSW, "prec_squared": PREC,
-                   "links": "random start exp(Gaussian su(3) algebra), seeded",
+                   "links": links_desc(info),
                    "l2": "inputs larger than L2 (links 604 MB, clover 604 MB), no flush",
                    "parallelism": f"replicas x{world}"},
         "solver": {"inner": a.inner, "delta": a.delta, "iterations": st["iterations"],

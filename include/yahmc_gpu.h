@@ -100,6 +100,10 @@ typedef struct {
  * (programs/hmc.cpp:94-117; geometry.cpp:1032-1191, repr.cpp:17-105,
  * bcs.cpp:11-137, clover.cpp:349-361, gaugefield.cpp:15-30) */
 int yg_lattice_create(const yg_params *p, yg_lattice **out);
+/* No reference counterpart (the reference is CPU/MPI): selects the CUDA device on which the
+ * calling thread's next yg_lattice_create places its state (one process per GPU: call it
+ * with the local rank first).  Each lattice keeps the device it was created on. */
+int yg_set_device(int device);
 void yg_lattice_destroy(yg_lattice *lat);
 int yg_lattice_query(const yg_lattice *lat, yg_info *out);
 int yg_set_stream(yg_lattice *lat, void *cuda_stream);
@@ -172,11 +176,14 @@ int yg_cg_mshift(yg_lattice *lat, const yg_inv_par *par, int num, const double *
 int yg_rational_calc(yg_lattice *lat, const yg_inv_par *par, double a0, int order, const double *poles,
                      const double *residues, double *x, double *b, int *iters);
 /* No reference counterpart: CG on the same operator with FP32 inner iterations and FP64
- * reliable updates; stops on the TRUE FP64 squared residual |b-Ax|^2 < prec*|b|^2. */
+ * reliable updates; stops on the TRUE FP64 squared residual |b-Ax|^2 < prec*|b|^2.  Uses
+ * the compressed FP32 inner operator (12-real links for SU(3) fundamental) for d = 3 and
+ * the generic FP32 operator otherwise. */
 int yg_cg_mixed(yg_lattice *lat, const yg_inv_par *par, double *x, double *b, yg_solve_stats *stats);
 
 /* No reference counterpart: options of the mixed-precision solver.
- *   inner_precision  32 (FP32 storage) or 16 (FP16 storage with per-site norms); FP32 arithmetic
+ *   inner_precision  32 (FP32 storage) or 16 (FP16 storage with per-site norms), FP32
+ *                    arithmetic; 0 selects the generic FP32 operator of yg_cg_mixed (any d)
  *   link_reals       18, or 12 (two rows, third rebuilt; SU(3) fundamental only)
  *   delta            reliable update when |r| falls below delta * |r| at the last update
  * The compressed inner operator exists for d = 3 representations with even-odd

@@ -25,7 +25,8 @@ def _true_residual(lat, op, mass, x, b):
 
 CASES = [("su3_fund_ap", 32, 12), ("su3_fund_ap", 32, 18), ("su3_fund_ap", 16, 12), ("su3_fund_ap", 16, 18),
          ("su3_fund_open", 16, 12), ("su3_fund_sf", 32, 12), ("su3_fund_per", 16, 12),
-         ("su3_fund_ap_nocl", 16, 12), ("su2_adj_ap", 32, 18), ("su2_adj_ap", 16, 18)]
+         ("su3_fund_ap_nocl", 16, 12), ("su2_adj_ap", 32, 18), ("su2_adj_ap", 16, 18),
+         ("su3_fund_ap", 0, 18), ("su2_adj_ap", 0, 18)]          # 0: the generic FP32 inner operator
 
 
 @pytest.mark.parametrize("name,inner,reals", CASES)
@@ -47,13 +48,18 @@ def test_compressed_inner_cg(name, inner, reals):
             assert st["iterations"] <= 1.5 * it64 + 10, (st, it64)
 
 
-@pytest.mark.parametrize("delta", [0.01, 0.3])
+@pytest.mark.parametrize("delta", [0.01, 0.3, 1e-4])
 def test_compressed_inner_delta(delta):
+    """delta = 1e-4 lies below what FP16 storage can resolve: the iterated residual levels
+    off, the stagnation guard forces reliable updates and the solve still ends (possibly
+    through the FP64 fallback) with the true residual below prec."""
     lat, O, rng = make_pair("su3_fund_ap", (8, 8, 8, 8), seed=32)
     b = lat.field(source(O, rng))
     x = lat.field()
     st = lat.cg_mixed("Hphi_sq", -0.4, 1e-26, x, b, inner_precision=16, link_reals=12, delta=delta)
-    assert st["status"] == 0 and st["fallback"] == 0, st
+    assert st["status"] == 0, st
+    if delta >= 0.01:
+        assert st["fallback"] == 0, st
     assert _true_residual(lat, "Hphi_sq", -0.4, x, b) < 1e-26
 
 

@@ -74,7 +74,7 @@ _I = ctypes.c_int
 _P = ctypes.c_void_p
 
 _SIGNATURES = {
-    "yg_lattice_create": [ctypes.POINTER(_Params), ctypes.POINTER(_P)],
+    "yg_lattice_create": [ctypes.POINTER(_Params), ctypes.POINTER(_P)], "yg_set_device": [_I],
     "yg_lattice_destroy": [_P], "yg_lattice_query": [_P, ctypes.POINTER(_Info)],
     "yg_set_stream": [_P, _P], "yg_synchronize": [_P],
     "yg_field_alloc": [_P, ctypes.POINTER(_P)], "yg_field_free": [_P, _P],
@@ -132,6 +132,13 @@ def load_library(path: Path | str | None = None):
         fn.restype = None if name in ("yg_lattice_destroy", "yg_mvm_reset") else ctypes.c_int
     _lib = lib
     return lib
+
+
+def set_device(device: int) -> None:
+    """CUDA device of the lattices this thread creates next (one process per GPU)."""
+    lib = load_library()
+    if lib.yg_set_device(int(device)) != 0:
+        raise YGError(1, lib.yg_last_error().decode())
 
 
 def launch_count() -> int:
@@ -358,8 +365,9 @@ class Lattice:
 
     def cg_mixed(self, op, mass, prec, x, b, log=0, maxiter=0, inner_precision=None, link_reals=18, delta=0.1):
         """Mixed-precision CG (true FP64 stopping criterion).  inner_precision None: the
-        generic FP32 inner operator; 32 or 16: the compressed d = 3 inner operator with
-        link_reals 18 or 12 and reliable-update threshold delta."""
+        library's choice (yg_cg_mixed); 0: the generic FP32 inner operator; 32 or 16: the
+        compressed d = 3 inner operator with link_reals 18 or 12 and reliable-update
+        threshold delta."""
         st = SolveStats()
         par = self._par(op, mass, prec, log, maxiter)
         if inner_precision is None:

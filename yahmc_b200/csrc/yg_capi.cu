@@ -61,6 +61,15 @@ const char *yg_last_error(void) { return g_last_error.c_str(); }
 
 long yg_launch_count(void) { return yg::g_launch_count; }
 
+int yg_set_device(int device) {
+  return guard([&] {
+    int n = 0;
+    YG_CUDA(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) throw yg::Error(YG_ERR_ARG, "no such CUDA device");
+    YG_CUDA(cudaSetDevice(device));
+  });
+}
+
 int yg_lattice_create(const yg_params *p, yg_lattice **out) {
   return guard([&] {
     need(p, "params");
@@ -242,11 +251,21 @@ int yg_cg_mixed_opts(yg_lattice *l, const yg_inv_par *p, const yg_mixed_opts *o,
                      yg_solve_stats *st) {
   return guard_status([&] {
     check_par(p); need(o, "opts"); need(x, "x"); need(b, "b");
+    if (o->inner_precision == 0) return yg::cg_mixed(lat(l), *p, x, b, st);
     return yg::cg_mixed_sloppy(lat(l), *p, o->inner_precision, o->link_reals, o->delta, x, b, st);
   });
 }
 int yg_cg_mixed(yg_lattice *l, const yg_inv_par *p, double *x, double *b, yg_solve_stats *st) {
-  return guard_status([&] { check_par(p); need(x, "x"); need(b, "b"); return yg::cg_mixed(lat(l), *p, x, b, st); });
+  return guard_status([&] {
+    check_par(p); need(x, "x"); need(b, "b");
+    yg::Lattice &L = lat(l);
+    // the compressed FP32 inner operator where it exists (d = 3, even-odd), else the generic one
+    if (L.d == 3 && L.p.eo) {
+      int reals = (L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL) ? 12 : 18;
+      return yg::cg_mixed_sloppy(L, *p, 32, reals, 0.003, x, b, st);
+    }
+    return yg::cg_mixed(L, *p, x, b, st);
+  });
 }
 
 // ---- forces

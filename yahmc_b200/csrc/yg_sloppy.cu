@@ -753,6 +753,8 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, doub
   double target = norm * par.prec;
   int it = 0, updates = 0, status = YG_OK, stall = 0;
   double best = rr;
+  double *xbest = L.scratch_field(46);      // the iterate with the smallest true residual
+  blas_copy(L, xbest, x);
   if (rr >= target) {
     f_from_d(L, fr, r, cnt);
     sloppy_from_d(L, p, r);
@@ -761,6 +763,12 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, doub
     double maxrr = rr;
     const double d2 = delta * delta;
     bool pending = false;           // an enqueued iteration whose |r|^2 is still to be read
+    // The iterated |r| of a low-precision inner solve levels off near the storage precision
+    // times |r| at the last update; if it has not halved for kStagnate iterations a
+    // reliable update is forced, so a delta below that floor cannot keep the loop going.
+    constexpr int kStagnate = 100;
+    double min_cycle = rr;
+    int since_min = 0;
     while (true) {
       if (par.maxiter > 0 && it >= par.maxiter) {
         status = YG_MAXITER;
@@ -779,7 +787,9 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, doub
       YG_CUDA(cudaEventSynchronize(L.sl_ev[slot ^ 1]));
       double rr_prev = hist[slot ^ 1];
       if (!std::isfinite(rr_prev)) throw Error(YG_NONFINITE, "non-finite value in cg_mixed");
-      if (rr_prev < d2 * maxrr || rr_prev < target) {
+      if (rr_prev < 0.25 * min_cycle) { min_cycle = rr_prev; since_min = 0; }
+      else since_min++;
+      if (rr_prev < d2 * maxrr || rr_prev < target || since_min >= kStagnate) {
         // reliable update on the state after the iteration just enqueued
         d_add_f(L, x, fx, cnt);
         YG_CUDA(cudaMemsetAsync(fx, 0, sizeof(float2) * cnt, L.stream));
@@ -787,25 +797,36 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, doub
         updates++;
         rr = rr_true;
         if (rr_true < target) break;
-        if (rr_true < 0.5 * best) { best = rr_true; stall = 0; }
+        if (rr_true < best) blas_copy(L, xbest, x);
+        if (rr_true > 100.0 * best) { status = YG_STALL; break; }       // the inner solve diverged
+        if (rr_true < 0.5 * best) stall = 0;
         else if (++stall >= 8) { status = YG_STALL; break; }
+        best = std::min(best, rr_true);
         f_from_d(L, fr, r, cnt);
         set_scalar(L, S_RR0 + (it & 1), rr_true); // the slot the next iteration reads
         maxrr = rr_true;
+        min_cycle = rr_true;
+        since_min = 0;
         pending = false;            // the enqueued |r|^2 predates the update
       }
     }
   }
   int fallback = 0;
   if (status != YG_OK) {
+    // plain FP64 CG (the reference's solver) from the best iterate; its recursive residual
+    // can stop above the true one, so it restarts until the true residual meets prec
+    blas_copy(L, x, xbest);
     yg_inv_par p64 = par;
     p64.log = 0;
-    int it64 = 0;
-    int s64 = cg(L, p64, x, b, &it64);
-    it += it64;
     fallback = 1;
-    rr = residual();
-    status = s64;
+    for (int attempt = 0; attempt < 3; attempt++) {
+      int it64 = 0;
+      status = cg(L, p64, x, b, &it64);
+      it += it64;
+      rr = residual();
+      if (status != YG_OK || rr < target) break;
+    }
+    if (status == YG_OK && rr >= target) status = YG_STALL;
   }
   YG_CUDA(cudaStreamSynchronize(L.stream));
   if (st) {

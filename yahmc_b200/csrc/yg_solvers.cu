@@ -5,6 +5,7 @@
 // and solutions match the reference to rounding; the device work per step is the fused
 // operator (yg_dirac.cu) and streaming BLAS passes (yg_blas.cu).  Scalars come back to
 // the host once per reduction, as the reference's control flow needs them.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -311,13 +312,22 @@ int cg_mixed(Lattice &L, const yg_inv_par &par, double *x, double *b, yg_solve_s
   int it = 0, updates = 0, status = YG_OK;
   double best = rr;
   int stall = 0;
+  double *xbest = L.scratch_field(46);      // the iterate with the smallest true residual
+  c.copy(xbest, x);
   if (rr >= target) {
     f_from_d(L, fr, r, cnt);
     f_from_d(L, fp, r, cnt);
     YG_CUDA(cudaMemsetAsync(fx, 0, sizeof(float2) * cnt, L.stream));
     double rr_s = rr, maxrr = rr;
+    constexpr int kStagnate = 100;    // forced reliable update when |r| stops falling
+    double min_cycle = rr;
+    int since_min = 0;
     while (true) {
-      if (par.maxiter > 0 && it >= par.maxiter) { status = YG_MAXITER; break; }
+      if (par.maxiter > 0 && it >= par.maxiter) {
+        status = YG_MAXITER;
+        d_add_f(L, x, fx, cnt);       // keep the progress of the inner iterations
+        break;
+      }
       it++;
       hphi_float(L, par.mass, (float2 *)ft, (float2 *)fp, (float2 *)fo);
       hphi_float(L, par.mass, (float2 *)fq, (float2 *)ft, (float2 *)fo);
@@ -325,7 +335,9 @@ int cg_mixed(Lattice &L, const yg_inv_par &par, double *x, double *b, yg_solve_s
       check_finite(pq, "cg_mixed");
       double alpha = rr_s / pq;
       double rr_new = f_cg_update(L, fx, fr, fp, fq, (float)alpha, cnt);
-      bool update = rr_new < delta * delta * maxrr || rr_new < target;
+      if (rr_new < 0.25 * min_cycle) { min_cycle = rr_new; since_min = 0; }
+      else since_min++;
+      bool update = rr_new < delta * delta * maxrr || rr_new < target || since_min >= kStagnate;
       if (update) {
         // fold the FP32 increment into x and recompute the true residual in FP64
         d_add_f(L, x, fx, cnt);
@@ -337,13 +349,18 @@ int cg_mixed(Lattice &L, const yg_inv_par &par, double *x, double *b, yg_solve_s
         double rr_true = c.sqnorm(r);
         updates++;
         if (rr_true < target) { rr = rr_true; break; }
-        if (rr_true < 0.5 * best) { best = rr_true; stall = 0; }
+        if (rr_true < best) c.copy(xbest, x);
+        if (rr_true > 100.0 * best) { status = YG_STALL; rr = rr_true; break; }   // diverged
+        if (rr_true < 0.5 * best) stall = 0;
         else if (++stall >= 8) { status = YG_STALL; rr = rr_true; break; }
+        best = std::min(best, rr_true);
         f_from_d(L, fr, r, cnt);
         double beta = rr_true / rr_s;
         f_xpay(L, fp, (float)beta, fr, cnt);
         rr_s = rr_true;
         maxrr = rr_true;
+        min_cycle = rr_true;
+        since_min = 0;
         rr = rr_true;
         continue;
       }
@@ -354,19 +371,24 @@ int cg_mixed(Lattice &L, const yg_inv_par &par, double *x, double *b, yg_solve_s
   }
   int fallback = 0;
   if (status != YG_OK) {
-    // plain FP64 CG from the current x (the reference's solver) guarantees the criterion
+    // plain FP64 CG (the reference's solver) from the best iterate, restarted until the
+    // true residual meets prec (its recursive residual can stop above the true one)
+    c.copy(x, xbest);
     yg_inv_par p64 = par;
     p64.log = 0;
-    int it64 = 0;
-    int s64 = cg(L, p64, x, b, &it64);
-    it += it64;
     fallback = 1;
-    c.copy(xd, x);
-    apply_op(L, YG_OP_HPHI_SQ, par.mass, Ax, xd);
-    c.copy(r, b);
-    c.axpby(r, {1, 0}, {-1, 0}, Ax);
-    rr = c.sqnorm(r);
-    status = s64;
+    for (int attempt = 0; attempt < 3; attempt++) {
+      int it64 = 0;
+      status = cg(L, p64, x, b, &it64);
+      it += it64;
+      c.copy(xd, x);
+      apply_op(L, YG_OP_HPHI_SQ, par.mass, Ax, xd);
+      c.copy(r, b);
+      c.axpby(r, {1, 0}, {-1, 0}, Ax);
+      rr = c.sqnorm(r);
+      if (status != YG_OK || rr < target) break;
+    }
+    if (status == YG_OK && rr >= target) status = YG_STALL;
   }
   YG_CUDA(cudaStreamSynchronize(L.stream));
   if (st) {
