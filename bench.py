@@ -60,6 +60,8 @@ def parse():
                          "operator with FP32/FP16 spinors and 18/12-real links")
     ap.add_argument("--delta", type=float, default=0.003, help="reliable-update threshold")
     ap.add_argument("--variants", action="store_true", help="also time every inner operator once")
+    ap.add_argument("--therm-trajectories", type=int, default=THERM["trajectories"],
+                    help="HMC trajectories of the field generation (fewer only to profile a few launches)")
     ap.add_argument("--solve-only", action="store_true",
                     help="time only the mixed solve and print its time (for profiling; not the bench line)")
     return ap.parse_args()
@@ -94,7 +96,7 @@ THERM = {"beta": 5.6, "c0": 1.0, "trajectories": 150, "warmup_md": 10, "steps": 
          "integrator": "o2mn", "start": "cold"}
 
 
-def thermalised_links(dims, seed):
+def thermalised_links(dims, seed, trajectories=None):
     """A thermalised SU(3) field for the workload: pure-gauge HMC (Wilson action, beta 5.6)
     on the lattice with the spatial extents halved, from a cold start, then tiled 1x2x2x2
     (for 32^4: a thermalised 16^3x32 field tiled 2x2x2x1, again a periodic field).
@@ -104,27 +106,29 @@ def thermalised_links(dims, seed):
     small = (dims[0],) + tuple(d // 2 if d % 4 == 0 else d for d in dims[1:])
     lat = yg.Lattice(small, nc=3, repr="fundamental", bc="periodic", clover=False, eo=True)
     lat.set_links(np.broadcast_to(np.eye(3, dtype=complex), (lat.V, 4, 3, 3)).copy())
-    hist = th.thermalize(lat, THERM["beta"], THERM["trajectories"], steps=THERM["steps"], length=THERM["length"],
-                         c0=THERM["c0"], seed=seed, integrator=THERM["integrator"], n_warm=THERM["warmup_md"])
-    acc = float(np.mean([h[0] for h in hist[THERM["warmup_md"]:]]))
+    n_traj = THERM["trajectories"] if trajectories is None else trajectories
+    hist = th.thermalize(lat, THERM["beta"], n_traj, steps=THERM["steps"], length=THERM["length"], c0=THERM["c0"],
+                         seed=seed, integrator=THERM["integrator"], n_warm=min(THERM["warmup_md"], n_traj))
+    acc = float(np.mean([h[0] for h in hist[THERM["warmup_md"]:]])) if n_traj > THERM["warmup_md"] else 1.0
     U = th.tile(lat.get_links(), small, tuple(dims))
     plaq = float(hist[-1][2])
     del lat
     return U, plaq, acc
 
 
-def make_inputs(dims, seed, rank=0):
+def make_inputs(dims, seed, rank=0, trajectories=None):
     from yahmc_b200 import fields
-    U, plaq, acc = thermalised_links(dims, seed)
+    U, plaq, acc = thermalised_links(dims, seed, trajectories)
     T, X, Y, Z = dims
     V = T * X * Y * Z
     rng = np.random.default_rng(seed + 7919 * rank)
     b = fields.gaussian_spinor(V, 3, rng)
-    return U, b, {"plaquette": plaq, "acceptance": acc}
+    return U, b, {"plaquette": plaq, "acceptance": acc,
+                  "trajectories": THERM["trajectories"] if trajectories is None else trajectories}
 
 
 def links_desc(info):
-    return (f"thermalised: {THERM['trajectories']} pure-gauge HMC trajectories (Wilson action, beta "
+    return (f"thermalised: {info['trajectories']} pure-gauge HMC trajectories (Wilson action, beta "
             f"{THERM['beta']}, {THERM['integrator']} {THERM['steps']} steps, length {THERM['length']}, first "
             f"{THERM['warmup_md']} without accept/reject) from a cold start on the lattice with halved spatial "
             f"extents, tiled 1x2x2x2; plaquette {info['plaquette']:.5f}, acceptance {info['acceptance']:.2f}")
@@ -208,7 +212,7 @@ def run_reference(a, rank, world):
     threads = os.cpu_count() or 1
     import yahmc_b200 as yg
     yg.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    U, b, info = make_inputs(a.dims, a.seed)        # input preparation only (GPU thermalisation)
+    U, b, info = make_inputs(a.dims, a.seed, 0, a.therm_trajectories)   # input preparation (GPU HMC)
     # one full solve is the bounded sample: about a minute on 16 host cores at 32^4; the
     # reference code has no warm-up effect worth a second minute
     steps, warm = 1, 0
@@ -234,7 +238,7 @@ def run_ours(a, rank, world, dist):
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
     dev = torch.cuda.current_device()
     yg.set_device(dev)
-    U, b, info = make_inputs(a.dims, a.seed, rank)
+    U, b, info = make_inputs(a.dims, a.seed, rank, a.therm_trajectories)
     lat = yg.Lattice(a.dims, nc=3, repr="fundamental", bc="antiperiodic", clover=True, eo=True, csw=CSW)
     lat.set_links(U)
     V, d = lat.V, lat.d
