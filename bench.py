@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--variants", action="store_true", help="also time every inner operator once")
     ap.add_argument("--therm-trajectories", type=int, default=THERM["trajectories"],
                     help="HMC trajectories of the field generation (fewer only to profile a few launches)")
+    ap.add_argument("--nrhs", type=int, default=12, help="systems of the batched-CG measurement (<= 1: skip)")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="time only the batched CG of --nrhs systems (for profiling; not the bench line)")
     ap.add_argument("--solve-only", action="store_true",
                     help="time only the mixed solve and print its time (for profiling; not the bench line)")
     return ap.parse_args()
@@ -276,6 +279,24 @@ def run_ours(a, rank, world, dist):
         lat.spinor_zero(x)
         return lat.cg_inverter("Hphi_sq", MASS, PREC, x, bf)
 
+    if a.batched_only:
+        rng_b = np.random.default_rng(a.seed + 17)
+        from yahmc_b200 import fields as yf
+        bsrc = [lat.field(yf.gaussian_spinor(V, 3, rng_b)) for _ in range(a.nrhs)]
+        bx = [lat.field() for _ in range(a.nrhs)]
+
+        def multi_only():
+            for f in bx:
+                lat.spinor_zero(f)
+            return lat.cg_inverter_multi("Hphi_sq", MASS, PREC, bx, bsrc)
+
+        for _ in range(max(1, a.warmup)):
+            multi_only()
+        ms_b, its_b = timed(multi_only, a.steps)
+        if rank == 0:
+            print(json.dumps({"batched_ms": ms_b, "nrhs": a.nrhs, "iterations": its_b[-1]}))
+        return
+
     # warm-up (W >= 3 solves), then the timed mixed-precision solves with clocks sampled
     for _ in range(max(3, a.warmup)):
         mixed()
@@ -328,6 +349,27 @@ def run_ours(a, rank, world, dist):
 
     e2e()
     ms_e2e, _ = timed(e2e, a.steps)
+
+    # several right-hand sides at once: 12 sources (the point-source count of a meson
+    # measurement) through the batched FP64 CG, per-system results identical to cg_inverter
+    batched = None
+    if a.nrhs > 1:
+        rng_b = np.random.default_rng(a.seed + 17)
+        from yahmc_b200 import fields as yf
+        bsrc = [lat.field(yf.gaussian_spinor(V, 3, rng_b)) for _ in range(a.nrhs)]
+        bx = [lat.field() for _ in range(a.nrhs)]
+
+        def multi():
+            for f in bx:
+                lat.spinor_zero(f)
+            return lat.cg_inverter_multi("Hphi_sq", MASS, PREC, bx, bsrc)
+
+        multi()
+        ms_multi, its_multi = timed(multi, 1)
+        batched = {"nrhs": a.nrhs, "solver": "FP64 CG, all systems per operator launch", "ms_total": ms_multi,
+                   "ms_per_rhs": ms_multi / a.nrhs, "iterations": its_multi[-1],
+                   "speedup_per_rhs_vs_fp64_cg": ms_fp64 / (ms_multi / a.nrhs)}
+        del bsrc, bx
 
     variants = None
     if a.variants:
@@ -387,6 +429,8 @@ def run_ours(a, rank, world, dist):
     }
     if variants is not None:
         line["inner_variants"] = variants
+    if batched is not None:
+        line["batched"] = batched
     print(json.dumps(line))
 
 

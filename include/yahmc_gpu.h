@@ -181,6 +181,15 @@ int yg_rational_calc(yg_lattice *lat, const yg_inv_par *par, double a0, int orde
  * the generic FP32 operator otherwise. */
 int yg_cg_mixed(yg_lattice *lat, const yg_inv_par *par, double *x, double *b, yg_solve_stats *stats);
 
+/* No reference counterpart: nrhs cg_inverter solves (cg.cpp:132-202) of the same operator
+ * (Hphi or Hphi_sq) advanced together.  Every system follows the reference's recurrence,
+ * initial guess (xs[i] on entry), stopping rule |r_i|^2 < prec |b_i|^2 and iteration count
+ * (iters[i]); the operator is applied to all systems in one launch per step, so the links
+ * and the clover term are read once for all of them.  1 <= nrhs <= 16, d = 3, even-odd.
+ * Sources must vanish on the open/SF boundary slices, as spinor_random's do. */
+int yg_cg_inverter_multi(yg_lattice *lat, const yg_inv_par *par, int nrhs, double *const *xs, double *const *bs,
+                         int *iters);
+
 /* No reference counterpart: options of the mixed-precision solver.
  *   inner_precision  32 (FP32 storage) or 16 (FP16 storage with per-site norms), FP32
  *                    arithmetic; 0 selects the generic FP32 operator of yg_cg_mixed (any d)

@@ -101,6 +101,7 @@ _SIGNATURES = {
     "yg_rational_calc": [_P, ctypes.POINTER(InvPar), _D, _I, _P, _P, _P, _P, ctypes.POINTER(_I)],
     "yg_cg_mixed": [_P, ctypes.POINTER(InvPar), _P, _P, ctypes.POINTER(SolveStats)],
     "yg_cg_mixed_opts": [_P, ctypes.POINTER(InvPar), ctypes.POINTER(MixedOpts), _P, _P, ctypes.POINTER(SolveStats)],
+    "yg_cg_inverter_multi": [_P, _P, _I, _P, _P, _P],
     "yg_momenta_upload": [_P, _P], "yg_momenta_download": [_P, _P], "yg_momenta_zero": [_P],
     "yg_clover_force_download": [_P, _P], "yg_begin_fermion_force": [_P], "yg_end_fermion_force": [_P, _D],
     "yg_wilson_fermion_force": [_P, _D, _D, _D, _P, _P], "yg_wilson_fermion_force_q": [_P, _D, _D, _D, _P],
@@ -362,6 +363,22 @@ class Lattice:
         self._check(self.lib.yg_rational_calc(self.h, ctypes.byref(par), a0, len(po), _ptr(po), _ptr(re),
                                               x.ptr, b.ptr, ctypes.byref(it)))
         return it.value
+
+    def cg_inverter_multi(self, op, mass, prec, xs, bs, log=0, maxiter=0):
+        """len(xs) cg_inverter solves sharing every operator application; returns the
+        iteration count of each system"""
+        n = len(xs)
+        if n != len(bs):
+            raise ValueError("xs and bs differ in length")
+        par = self._par(op, mass, prec, log, maxiter)
+        px = (ctypes.c_void_p * n)(*[x.ptr for x in xs])
+        pb = (ctypes.c_void_p * n)(*[b.ptr for b in bs])
+        its = (ctypes.c_int * n)()
+        rc = self.lib.yg_cg_inverter_multi(self.h, ctypes.byref(par), n, px, pb, its)
+        self.last_status = rc
+        if rc not in (0, 4):
+            self._check(rc)
+        return list(its)
 
     def cg_mixed(self, op, mass, prec, x, b, log=0, maxiter=0, inner_precision=None, link_reals=18, delta=0.1):
         """Mixed-precision CG (true FP64 stopping criterion).  inner_precision None: the

@@ -301,4 +301,89 @@ void f_xpay(Lattice &L, float *p, float b, const float *r, long cnt) {
   YG_LAUNCHED();
 }
 
+// ---- cg_mshift updates of all shifts in one pass each (cg.cpp:62-116)
+// Launch parameters carry the per-shift fields and coefficients of the active shifts.
+struct MshiftArgs {
+  double2 *x[kMaxShifts];
+  double2 *k[kMaxShifts];
+  double c_x[kMaxShifts];     // x_n -= c_x[n] k_n
+  double c_kk[kMaxShifts];    // k_n = c_kk[n] k_n + c_kr[n] r
+  double c_kr[kMaxShifts];
+  int num;
+};
+
+// r += beta q (partial |r|^2) and x_n -= bt_n k_n for every active shift, one pass
+__global__ void __launch_bounds__(256) k_mshift_xr(double2 *partial, double2 *r, const double2 *q, double beta,
+                                                   MshiftArgs a, long n) {
+  double acc = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double2 v = r[i], w = q[i];
+    v.x = fma(beta, w.x, v.x);
+    v.y = fma(beta, w.y, v.y);
+    r[i] = v;
+    acc = fma(v.x, v.x, fma(v.y, v.y, acc));
+    for (int s = 0; s < a.num; s++) {
+      double2 xv = a.x[s][i], kv = a.k[s][i];
+      xv.x = fma(-a.c_x[s], kv.x, xv.x);
+      xv.y = fma(-a.c_x[s], kv.y, xv.y);
+      a.x[s][i] = xv;
+    }
+  }
+  double2 t = block_sum2(make_double2(acc, 0.0));
+  if (threadIdx.x == 0) partial[blockIdx.x] = t;
+}
+
+// k_n = at_n k_n + c3_n r for every active shift, and p = alpha p + r, one pass
+__global__ void __launch_bounds__(256) k_mshift_kp(double2 *p, const double2 *r, double alpha, MshiftArgs a, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double2 rv = r[i];
+    for (int s = 0; s < a.num; s++) {
+      double2 kv = a.k[s][i];
+      kv.x = fma(a.c_kr[s], rv.x, a.c_kk[s] * kv.x);
+      kv.y = fma(a.c_kr[s], rv.y, a.c_kk[s] * kv.y);
+      a.k[s][i] = kv;
+    }
+    if (p) {
+      double2 pv = p[i];
+      p[i] = make_double2(fma(alpha, pv.x, rv.x), fma(alpha, pv.y, rv.y));
+    }
+  }
+}
+
+static MshiftArgs mshift_args(const Lattice &L, int num, double *const *x, double *const *k, const double *c1,
+                              const double *c2, const double *c3, long lo) {
+  if (num < 0 || num > kMaxShifts) throw Error(YG_ERR_ARG, "too many shifts");
+  MshiftArgs a{};
+  a.num = num;
+  const long o = woff(L, lo);
+  for (int s = 0; s < num; s++) {
+    a.x[s] = x ? (double2 *)x[s] + o : nullptr;
+    a.k[s] = (double2 *)k[s] + o;
+    a.c_x[s] = c1 ? c1[s] : 0.0;
+    a.c_kk[s] = c2 ? c2[s] : 0.0;
+    a.c_kr[s] = c3 ? c3[s] : 0.0;
+  }
+  return a;
+}
+
+double blas_mshift_xr(Lattice &L, double *r, const double *q, double beta, int num, double *const *x,
+                      double *const *k, const double *bt, long lo, long n) {
+  long cnt = wcnt(L, n);
+  int grid = red_grid(L, cnt);
+  MshiftArgs a = mshift_args(L, num, x, k, bt, nullptr, nullptr, lo);
+  k_mshift_xr<<<grid, 256, 0, L.stream>>>(L.red_partial.as<double2>(), (double2 *)r + woff(L, lo),
+                                           (const double2 *)q + woff(L, lo), beta, a, cnt);
+  YG_LAUNCHED();
+  return reduce_partials(L, grid).x;
+}
+
+void blas_mshift_kp(Lattice &L, double *p, const double *r, double alpha, int num, double *const *k,
+                    const double *at, const double *c3, long lo, long n) {
+  long cnt = wcnt(L, n);
+  MshiftArgs a = mshift_args(L, num, nullptr, k, nullptr, at, c3, lo);
+  k_mshift_kp<<<stream_grid(cnt), 256, 0, L.stream>>>(p ? (double2 *)p + woff(L, lo) : nullptr,
+                                                       (const double2 *)r + woff(L, lo), alpha, a, cnt);
+  YG_LAUNCHED();
+}
+
 }  // namespace yg

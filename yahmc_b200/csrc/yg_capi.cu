@@ -255,6 +255,14 @@ int yg_cg_mixed_opts(yg_lattice *l, const yg_inv_par *p, const yg_mixed_opts *o,
     return yg::cg_mixed_sloppy(lat(l), *p, o->inner_precision, o->link_reals, o->delta, x, b, st);
   });
 }
+int yg_cg_inverter_multi(yg_lattice *l, const yg_inv_par *p, int nrhs, double *const *xs, double *const *bs,
+                         int *iters) {
+  return guard_status([&] {
+    check_par(p); need(xs, "xs"); need(bs, "bs"); need(iters, "iters");
+    for (int i = 0; i < nrhs; i++) { need(xs[i], "xs[i]"); need(bs[i], "bs[i]"); }
+    return yg::cg_multi(lat(l), *p, nrhs, xs, bs, iters);
+  });
+}
 int yg_cg_mixed(yg_lattice *l, const yg_inv_par *p, double *x, double *b, yg_solve_stats *st) {
   return guard_status([&] {
     check_par(p); need(x, "x"); need(b, "b");

@@ -151,6 +151,13 @@ double blas_cg_update(Lattice &L, double *x, double *r, const double *p, const d
 double sum_device(Lattice &L, const double *v, long n);
 // sum the first `grid` double2 partials in L.red_partial (deterministic), to the host
 double2 reduce_partials(Lattice &L, int grid);
+constexpr int kMaxShifts = 50;          // MAX of cg.cpp:5
+// cg_mshift passes over all active shifts at once: r += beta q, x_n -= bt_n k_n (returns
+// |r|^2); and k_n = at_n k_n + c3_n r, p = alpha p + r (p may be null)
+double blas_mshift_xr(Lattice &L, double *r, const double *q, double beta, int num, double *const *x,
+                      double *const *k, const double *bt, long lo, long n);
+void blas_mshift_kp(Lattice &L, double *p, const double *r, double alpha, int num, double *const *k,
+                    const double *at, const double *c3, long lo, long n);
 // FP32 helpers of the mixed-precision solver (counts in complex words)
 void f_from_d(Lattice &L, float *dst, const double *src, long cnt);
 void d_add_f(Lattice &L, double *dst, const float *src, long cnt);
@@ -192,5 +199,8 @@ void momenta_gaussian(Lattice &L, unsigned long long seed);
 double momenta_action(Lattice &L);
 void gauge_backup(Lattice &L);
 void gauge_restore(Lattice &L);
+
+// several cg_inverter solves sharing every operator application (yg_multi.cu)
+int cg_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, double *const *bs, int *iters);
 
 }  // namespace yg

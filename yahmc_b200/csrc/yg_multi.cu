@@ -1,0 +1,486 @@
+// Several right-hand sides of the same operator advanced together.
+//
+// cg_inverter (cg.cpp:132-202) solves one system at a time and reads the links and the
+// clover term once per right-hand side and operator application.  Here nrhs systems share
+// every operator application: a batched field stores the right-hand-side index fastest,
+//   B[((blk*4d + k)*Vh + h)*nrhs + i]   (complex word k of site (blk,h) of system i),
+// one thread handles one (site, system) pair, and the nrhs threads of a site sit next to
+// each other in a warp, so the site's links and clover blocks are fetched once for all of
+// them while each thread gathers its own neighbour spinors (contiguous across the site's
+// threads).  Every system keeps the reference's CG recurrence, stopping rule and iteration
+// count; a converged system stops being updated.
+#include <algorithm>
+#include <cstdio>
+#include <vector>
+#include "yg_dirac_impl.cuh"
+#include "yg_lattice.h"
+
+namespace yg {
+
+constexpr int kMaxRhs = 16;
+
+// batched index of complex word k of site id, system i
+__device__ __forceinline__ long bidx(const Geom &g, int id, int k, int ncomp, int nb, int i) {
+  return fidx(g, id, k, ncomp) * nb + i;
+}
+
+template <int D, int MU, int SIG>
+__device__ __forceinline__ void bhop_dir(double2 (&acc)[4][D], const double2 *src, const double2 *U, const Geom &g,
+                                         int nid, int lid, int nb, int i) {
+  double2 h[2][D];
+#pragma unroll
+  for (int c = 0; c < D; c++) {
+    double2 p0 = __ldg(src + bidx(g, nid, 0 * D + c, 4 * D, nb, i));
+    double2 p1 = __ldg(src + bidx(g, nid, 1 * D + c, 4 * D, nb, i));
+    double2 p2 = __ldg(src + bidx(g, nid, 2 * D + c, 4 * D, nb, i));
+    double2 p3 = __ldg(src + bidx(g, nid, 3 * D + c, 4 * D, nb, i));
+    if (MU == 0) {
+      h[0][c] = SIG < 0 ? cadd(p0, p2) : csub(p0, p2);
+      h[1][c] = SIG < 0 ? cadd(p1, p3) : csub(p1, p3);
+    } else if (MU == 1) {
+      h[0][c] = SIG < 0 ? cadd(p0, ctimesi(p3)) : csub(p0, ctimesi(p3));
+      h[1][c] = SIG < 0 ? cadd(p1, ctimesi(p2)) : csub(p1, ctimesi(p2));
+    } else if (MU == 2) {
+      h[0][c] = SIG < 0 ? cadd(p0, p3) : csub(p0, p3);
+      h[1][c] = SIG < 0 ? csub(p1, p2) : cadd(p1, p2);
+    } else {
+      h[0][c] = SIG < 0 ? cadd(p0, ctimesi(p2)) : csub(p0, ctimesi(p2));
+      h[1][c] = SIG < 0 ? csub(p1, ctimesi(p3)) : cadd(p1, ctimesi(p3));
+    }
+  }
+  double2 chi[2][D];
+  link_mul<D, double, (SIG > 0)>(chi, h, U, g, lid, MU);
+#pragma unroll
+  for (int c = 0; c < D; c++) {
+    acc[0][c] = cadd(acc[0][c], chi[0][c]);
+    acc[1][c] = cadd(acc[1][c], chi[1][c]);
+    if (MU == 0) {
+      acc[2][c] = SIG < 0 ? cadd(acc[2][c], chi[0][c]) : csub(acc[2][c], chi[0][c]);
+      acc[3][c] = SIG < 0 ? cadd(acc[3][c], chi[1][c]) : csub(acc[3][c], chi[1][c]);
+    } else if (MU == 1) {
+      acc[2][c] = SIG < 0 ? cadd(acc[2][c], ctimesmi(chi[1][c])) : cadd(acc[2][c], ctimesi(chi[1][c]));
+      acc[3][c] = SIG < 0 ? cadd(acc[3][c], ctimesmi(chi[0][c])) : cadd(acc[3][c], ctimesi(chi[0][c]));
+    } else if (MU == 2) {
+      acc[2][c] = SIG < 0 ? csub(acc[2][c], chi[1][c]) : cadd(acc[2][c], chi[1][c]);
+      acc[3][c] = SIG < 0 ? cadd(acc[3][c], chi[0][c]) : csub(acc[3][c], chi[0][c]);
+    } else {
+      acc[2][c] = SIG < 0 ? cadd(acc[2][c], ctimesmi(chi[0][c])) : cadd(acc[2][c], ctimesi(chi[0][c]));
+      acc[3][c] = SIG < 0 ? cadd(acc[3][c], ctimesi(chi[1][c])) : cadd(acc[3][c], ctimesmi(chi[1][c]));
+    }
+  }
+}
+
+struct MultiHopArgs {
+  Geom g;
+  const double2 *src;     // batched hop input
+  const double2 *src2;    // STEP 2: batched psi_e
+  double2 *dst;
+  const double2 *U;
+  const double2 *cpk;     // STEP 1 with clover: packed Hermitian inverse of the odd-site blocks
+  const double2 *cl;      // STEP 2 with clover: clover term
+  double diag;            // STEP 2: 4+m (clover) or (4+m)^2 (no clover)
+  double cfm1;
+  double coeff;           // +1/2 (step 1), -1/2 (step 2)
+  int lo, n, nb;          // output sites [lo, lo+n), nb systems
+  int clover;
+  int g5;
+};
+
+// STEP 1 (odd sites): dst = A_oo^-1 (coeff hop src)            (no clover: coeff hop src)
+// STEP 2 (even sites): dst = [g5] (A_ee src2 + coeff hop src)   (no clover: diag src2 + ...)
+// as schur_step1 / schur_step2 of the single-system operator (dirac.cpp:738-765)
+template <int D, int STEP>
+__global__ void __launch_bounds__(128) k_hop_multi(MultiHopArgs a) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= (long)a.n * a.nb) return;
+  const int i = (int)(t % a.nb);
+  const int id = a.lo + (int)(t / a.nb);
+  const Geom &g = a.g;
+  int c[4];
+  coords_of(g, id, c);
+  double2 acc[4][D];
+#pragma unroll
+  for (int s = 0; s < 4; s++)
+#pragma unroll
+    for (int k = 0; k < D; k++) acc[s][k] = make_double2(0, 0);
+  int f, b;
+  f = neighbour(g, c, 0, +1); bhop_dir<D, 0, -1>(acc, a.src, a.U, g, f, id, a.nb, i);
+  b = neighbour(g, c, 0, -1); bhop_dir<D, 0, +1>(acc, a.src, a.U, g, b, b, a.nb, i);
+  f = neighbour(g, c, 1, +1); bhop_dir<D, 1, -1>(acc, a.src, a.U, g, f, id, a.nb, i);
+  b = neighbour(g, c, 1, -1); bhop_dir<D, 1, +1>(acc, a.src, a.U, g, b, b, a.nb, i);
+  f = neighbour(g, c, 2, +1); bhop_dir<D, 2, -1>(acc, a.src, a.U, g, f, id, a.nb, i);
+  b = neighbour(g, c, 2, -1); bhop_dir<D, 2, +1>(acc, a.src, a.U, g, b, b, a.nb, i);
+  f = neighbour(g, c, 3, +1); bhop_dir<D, 3, -1>(acc, a.src, a.U, g, f, id, a.nb, i);
+  b = neighbour(g, c, 3, -1); bhop_dir<D, 3, +1>(acc, a.src, a.U, g, b, b, a.nb, i);
+  const bool bnd = spinor_zeroed(g, c[0]);
+#pragma unroll
+  for (int s = 0; s < 4; s++)
+#pragma unroll
+    for (int k = 0; k < D; k++) acc[s][k] = bnd ? make_double2(0, 0) : cscale(acc[s][k], a.coeff);
+  double2 out[4][D];
+  if (STEP == 1) {
+    if (a.clover) cpk_site<D, double>(out, acc, a.cpk, id - g.Vh, g.Vh);
+    else {
+#pragma unroll
+      for (int s = 0; s < 4; s++)
+#pragma unroll
+        for (int k = 0; k < D; k++) out[s][k] = acc[s][k];
+    }
+  } else {
+    // the diagonal and clover terms are skipped at zeroed boundary slices, as the
+    // single-system operator does (zero_add_at_boundary)
+    if (!bnd) {
+      if (a.clover) {
+        const double diag = a.diag + ((c[0] == g.Ta || c[0] == g.Tb) ? a.cfm1 : 0.0);
+#pragma unroll
+        for (int blk = 0; blk < 2; blk++) {
+          const int s0 = 2 * blk, s1 = 2 * blk + 1;
+          double2 p0[D], p1[D];
+#pragma unroll
+          for (int q = 0; q < D; q++) {
+            p0[q] = __ldg(a.src2 + bidx(g, id, s0 * D + q, 4 * D, a.nb, i));
+            p1[q] = __ldg(a.src2 + bidx(g, id, s1 * D + q, 4 * D, a.nb, i));
+          }
+#pragma unroll
+          for (int r = 0; r < D; r++) {
+            double2 o0 = cadd(acc[s0][r], cscale(p0[r], diag)), o1 = cadd(acc[s1][r], cscale(p1[r], diag));
+#pragma unroll
+            for (int q = 0; q < D; q++) {
+              double2 a0 = __ldg(a.cl + fidx(g, id, s0 * D * D + r * D + q, 4 * D * D));
+              double2 a1 = __ldg(a.cl + fidx(g, id, s1 * D * D + r * D + q, 4 * D * D));
+              double2 a1t = __ldg(a.cl + fidx(g, id, s1 * D * D + q * D + r, 4 * D * D));
+              cfma(o0, a0, p0[q]);
+              cfma(o0, a1, p1[q]);
+              cfmac(o1, a1t, p0[q]);
+              o1 = csub(o1, cmul(a0, p1[q]));
+            }
+            acc[s0][r] = o0;
+            acc[s1][r] = o1;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int s = 0; s < 4; s++)
+#pragma unroll
+          for (int k = 0; k < D; k++) {
+            double2 v = __ldg(a.src2 + bidx(g, id, s * D + k, 4 * D, a.nb, i));
+            acc[s][k] = cadd(acc[s][k], cscale(v, a.diag));
+          }
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+#pragma unroll
+      for (int k = 0; k < D; k++) out[s][k] = (a.g5 && s >= 2) ? cscale(acc[s][k], -1.0) : acc[s][k];
+  }
+#pragma unroll
+  for (int s = 0; s < 4; s++)
+#pragma unroll
+    for (int k = 0; k < D; k++) a.dst[bidx(g, id, s * D + k, 4 * D, a.nb, i)] = out[s][k];
+}
+
+// ---- batched BLAS over the words [w0, w0 + cnt) of every system.  Block size 32*nb, so a
+// thread's system index threadIdx.x % nb is the same for all the elements it visits.
+struct MultiScalars {
+  double a[kMaxRhs];
+};
+
+// deterministic per-system block sums: thread t holds the partial of system t % nb
+__device__ __forceinline__ void block_partials(double v, double *part, int nb) {
+  __shared__ double sh[32 * kMaxRhs];
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  if (threadIdx.x < nb) {
+    double s = 0;
+    for (int k = threadIdx.x; k < (int)blockDim.x; k += nb) s += sh[k];
+    part[(long)blockIdx.x * nb + threadIdx.x] = s;
+  }
+}
+
+// KIND 0: Re <a_i, b_i> ; 1: |a_i|^2
+template <int KIND>
+__global__ void k_multi_reduce(double *part, const double2 *a, const double2 *b, long w0, long cnt, int nb) {
+  const long n = cnt * nb, base = w0 * nb;
+  double acc = 0;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    double2 x = a[base + e];
+    if (KIND == 0) {
+      double2 y = b[base + e];
+      acc = fma(x.x, y.x, fma(x.y, y.y, acc));
+    } else {
+      acc = fma(x.x, x.x, fma(x.y, x.y, acc));
+    }
+  }
+  block_partials(acc, part, nb);
+}
+
+// x_i += alpha_i p_i ; r_i -= alpha_i q_i ; partials of |r_i|^2
+__global__ void k_multi_cg_update(double *part, double2 *x, double2 *r, const double2 *p, const double2 *q,
+                                  MultiScalars al, long w0, long cnt, int nb) {
+  const long n = cnt * nb, base = w0 * nb;
+  const double a = al.a[threadIdx.x % nb];
+  double acc = 0;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    double2 xv = x[base + e], rv = r[base + e], pv = p[base + e], qv = q[base + e];
+    xv.x = fma(a, pv.x, xv.x);
+    xv.y = fma(a, pv.y, xv.y);
+    rv.x = fma(-a, qv.x, rv.x);
+    rv.y = fma(-a, qv.y, rv.y);
+    x[base + e] = xv;
+    r[base + e] = rv;
+    acc = fma(rv.x, rv.x, fma(rv.y, rv.y, acc));
+  }
+  block_partials(acc, part, nb);
+}
+
+// p_i = beta_i p_i + r_i for the systems with beta_i != 0 flagged in `on`
+__global__ void k_multi_xpay(double2 *p, const double2 *r, MultiScalars be, MultiScalars on, long w0, long cnt,
+                             int nb) {
+  const long n = cnt * nb, base = w0 * nb;
+  const int i = threadIdx.x % nb;
+  if (on.a[i] == 0.0) return;
+  const double b = be.a[i];
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    double2 pv = p[base + e], rv = r[base + e];
+    p[base + e] = make_double2(fma(b, pv.x, rv.x), fma(b, pv.y, rv.y));
+  }
+}
+
+// dst_i = b_i - a_i on the words [w0, w0+cnt)
+__global__ void k_multi_sub(double2 *dst, const double2 *bvec, const double2 *avec, long w0, long cnt, int nb) {
+  const long n = cnt * nb, base = w0 * nb;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    double2 x = bvec[base + e], y = avec[base + e];
+    dst[base + e] = make_double2(x.x - y.x, x.y - y.y);
+  }
+}
+
+// pack (dir = 0) or unpack (dir = 1) the words [w0, w0+cnt) of nb single-system fields
+struct FieldPtrs {
+  double2 *f[kMaxRhs];
+};
+
+__global__ void k_multi_pack(double2 *batch, FieldPtrs fp, long w0, long cnt, int nb, int dir) {
+  const long n = cnt * nb;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const long w = w0 + e / nb;
+    const int i = (int)(e % nb);
+    if (dir == 0) batch[w * nb + i] = fp.f[i][w];
+    else fp.f[i][w] = batch[w * nb + i];
+  }
+}
+
+// zero the spinors of the boundary slices (open / SF) of a batched field, both parities:
+// the side effect of the single-system operator on its input (bc_zero_field)
+__global__ void k_multi_bc_zero(double2 *batch, Geom g, int words, int nb) {
+  const long n = (long)g.V * words * nb;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const long w = e / nb;                        // word index in the single-system layout
+    const int blk = (int)(w / ((long)words * g.Vh));
+    const int h = (int)(w % g.Vh);
+    int c[4];
+    coords_of(g, blk * g.Vh + h, c);
+    if (spinor_zeroed(g, c[0])) batch[e] = make_double2(0, 0);
+  }
+}
+
+// ------------------------------------------------------------------ host side
+namespace {
+
+struct Multi {
+  Lattice &L;
+  int nb;
+  long w0, cnt;            // complex words of the default view (per system)
+  int grid, threads;       // batched BLAS launch shape
+  DevBuf part;
+  std::vector<double> host;
+
+  Multi(Lattice &l, int n) : L(l), nb(n) {
+    long lo, ns;
+    L.view_range(YG_VIEW_DEFAULT, lo, ns);
+    w0 = lo * 4L * L.d;
+    cnt = ns * 4L * L.d;
+    threads = 32 * nb;
+    long g = (cnt * nb + threads - 1) / threads;
+    grid = (int)std::min<long>(g, 148L * 8);
+    part.alloc(sizeof(double) * (size_t)grid * nb);
+    host.resize((size_t)grid * nb);
+  }
+
+  double2 *field() {
+    double2 *p = nullptr;
+    YG_CUDA(cudaMalloc(&p, sizeof(double2) * (size_t)L.V * 4 * L.d * nb));
+    YG_CUDA(cudaMemsetAsync(p, 0, sizeof(double2) * (size_t)L.V * 4 * L.d * nb, L.stream));
+    return p;
+  }
+
+  // sums of the block partials per system, in block order
+  std::vector<double> sums() {
+    YG_CUDA(cudaMemcpyAsync(host.data(), part.p, sizeof(double) * (size_t)grid * nb, cudaMemcpyDeviceToHost,
+                            L.stream));
+    YG_CUDA(cudaStreamSynchronize(L.stream));
+    std::vector<double> s(nb, 0.0);
+    for (int b = 0; b < grid; b++)
+      for (int i = 0; i < nb; i++) s[i] += host[(size_t)b * nb + i];
+    return s;
+  }
+
+  std::vector<double> dot_re(const double2 *a, const double2 *b) {
+    k_multi_reduce<0><<<grid, threads, 0, L.stream>>>(part.as<double>(), a, b, w0, cnt, nb);
+    YG_LAUNCHED();
+    return sums();
+  }
+  std::vector<double> sqnorm(const double2 *a) {
+    k_multi_reduce<1><<<grid, threads, 0, L.stream>>>(part.as<double>(), a, nullptr, w0, cnt, nb);
+    YG_LAUNCHED();
+    return sums();
+  }
+};
+
+}  // namespace
+
+// dst = Hphi src (one Schur operator with gamma5) on batched fields; tmp takes the odd sites
+static void hphi_multi(Lattice &L, int nb, double mass, double2 *dst, const double2 *src, double2 *tmp) {
+  if (L.d != 3) throw Error(YG_ERR_ARG, "the batched operator is built for d = 3");
+  MultiHopArgs a{};
+  a.g = L.g;
+  a.U = L.links.as<double2>();
+  a.nb = nb;
+  a.cfm1 = L.p.cf - 1.0;
+  a.clover = L.p.clover ? 1 : 0;
+  if (a.clover) {
+    ensure_ldl(L, 4.0 + mass);
+    a.cpk = L.cpk64.as<double2>();
+    a.cl = L.clover.as<double2>();
+  }
+  MultiHopArgs s1 = a;
+  s1.src = src;
+  s1.dst = tmp;
+  s1.coeff = 0.5;
+  s1.lo = (int)L.Vh;
+  s1.n = (int)L.Vh;
+  MultiHopArgs s2 = a;
+  s2.src = tmp;
+  s2.src2 = src;
+  s2.dst = dst;
+  s2.coeff = -0.5;
+  s2.lo = 0;
+  s2.n = (int)L.Vh;
+  s2.g5 = 1;
+  s2.diag = a.clover ? 4.0 + mass : (4.0 + mass) * (4.0 + mass);
+  const long n = (long)L.Vh * nb;
+  k_hop_multi<3, 1><<<nblk(n, 128), 128, 0, L.stream>>>(s1);
+  YG_LAUNCHED();
+  k_hop_multi<3, 2><<<nblk(n, 128), 128, 0, L.stream>>>(s2);
+  YG_LAUNCHED();
+  L.mvm += 2;
+}
+
+static void bc_zero_multi(Lattice &L, int nb, double2 *f) {
+  if (L.p.bc != YG_BC_OPEN && L.p.bc != YG_BC_SF) return;
+  const long n = L.V * 4L * L.d * nb;
+  k_multi_bc_zero<<<(int)std::min<long>(nblk(n, 256), 148L * 16), 256, 0, L.stream>>>(f, L.g, 4 * L.d, nb);
+  YG_LAUNCHED();
+}
+
+// dst = op(src); like the single-system operator it zeroes the boundary slices of its
+// input (dirac.cpp:738-765 with apply_bcs_on_spinor_field)
+static void op_multi(Lattice &L, int op, int nb, double mass, double2 *dst, double2 *src, double2 *tmp,
+                     double2 *mid) {
+  if (op == YG_OP_HPHI) {
+    hphi_multi(L, nb, mass, dst, src, tmp);
+    bc_zero_multi(L, nb, src);
+  } else if (op == YG_OP_HPHI_SQ) {
+    hphi_multi(L, nb, mass, mid, src, tmp);
+    bc_zero_multi(L, nb, src);
+    hphi_multi(L, nb, mass, dst, mid, tmp);
+  } else {
+    throw Error(YG_ERR_ARG, "the batched CG runs on Hphi or Hphi_sq");
+  }
+}
+
+// nrhs cg_inverter solves (cg.cpp:132-202) sharing every operator application
+int cg_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, double *const *bs, int *iters) {
+  if (nrhs < 1 || nrhs > kMaxRhs) throw Error(YG_ERR_ARG, "1..16 right-hand sides");
+  if (!L.p.eo) throw Error(YG_ERR_ARG, "the batched CG needs even-odd preconditioning");
+  if (L.d != 3) throw Error(YG_ERR_ARG, "the batched operator is built for d = 3");
+  Multi m(L, nrhs);
+  const int nb = nrhs;
+  double2 *X = m.field(), *B = m.field(), *R = m.field(), *P = m.field(), *Q = m.field(), *T = m.field(),
+          *M = m.field();
+  std::vector<double2 *> bufs = {X, B, R, P, Q, T, M};
+  int status = YG_OK;
+  try {
+    FieldPtrs fx{}, fb{};
+    for (int i = 0; i < nb; i++) {
+      fx.f[i] = (double2 *)xs[i];
+      fb.f[i] = (double2 *)bs[i];
+    }
+    const long wall = (long)L.V * 4 * L.d;        // both blocks: the operator reads odd sites of its input
+    k_multi_pack<<<nblk(wall * nb, 256), 256, 0, L.stream>>>(X, fx, 0, wall, nb, 0);
+    YG_LAUNCHED();
+    k_multi_pack<<<nblk(wall * nb, 256), 256, 0, L.stream>>>(B, fb, 0, wall, nb, 0);
+    YG_LAUNCHED();
+    // r = b - A x ; p = r
+    YG_CUDA(cudaMemcpyAsync(P, X, sizeof(double2) * (size_t)wall * nb, cudaMemcpyDeviceToDevice, L.stream));
+    op_multi(L, par.op, nb, par.mass, Q, P, T, M);
+    k_multi_sub<<<m.grid, m.threads, 0, L.stream>>>(R, B, Q, m.w0, m.cnt, nb);
+    YG_LAUNCHED();
+    YG_CUDA(cudaMemcpyAsync(P, R, sizeof(double2) * (size_t)wall * nb, cudaMemcpyDeviceToDevice, L.stream));
+    std::vector<double> norm = m.sqnorm(B), rr = m.sqnorm(R);
+    std::vector<int> active(nb), it(nb, 0);
+    int nactive = 0;
+    for (int i = 0; i < nb; i++) {
+      active[i] = !(rr[i] < norm[i] * par.prec);   // already converged: 0 iterations
+      nactive += active[i];
+    }
+    int k = 0;
+    while (nactive > 0) {
+      k++;
+      if (par.maxiter > 0 && k > par.maxiter) { status = YG_MAXITER; break; }
+      op_multi(L, par.op, nb, par.mass, Q, P, T, M);
+      std::vector<double> pq = m.dot_re(P, Q);
+      MultiScalars al{}, be{}, on{};
+      for (int i = 0; i < nb; i++) {
+        if (!active[i]) continue;
+        if (!std::isfinite(pq[i])) throw Error(YG_NONFINITE, "non-finite value in cg_multi");
+        al.a[i] = rr[i] / pq[i];
+      }
+      k_multi_cg_update<<<m.grid, m.threads, 0, L.stream>>>(m.part.as<double>(), X, R, P, Q, al, m.w0, m.cnt, nb);
+      YG_LAUNCHED();
+      std::vector<double> rn = m.sums();
+      for (int i = 0; i < nb; i++) {
+        if (!active[i]) continue;
+        it[i] = k;
+        be.a[i] = rn[i] / rr[i];
+        rr[i] = rn[i];
+        if (rn[i] < norm[i] * par.prec) {      // cg.cpp:186-189: stop before the p update
+          active[i] = 0;
+          nactive--;
+        } else {
+          on.a[i] = 1.0;
+        }
+      }
+      if (nactive > 0) {
+        k_multi_xpay<<<m.grid, m.threads, 0, L.stream>>>(P, R, be, on, m.w0, m.cnt, nb);
+        YG_LAUNCHED();
+      }
+    }
+    // x_i (default view) back into the caller's fields
+    k_multi_pack<<<nblk(m.cnt * nb, 256), 256, 0, L.stream>>>(X, fx, m.w0, m.cnt, nb, 1);
+    YG_LAUNCHED();
+    YG_CUDA(cudaStreamSynchronize(L.stream));
+    for (int i = 0; i < nb; i++) iters[i] = it[i];
+    if (par.log)
+      for (int i = 0; i < nb; i++)
+        fprintf(stderr, "[INVERTER][30]cg_multi[%d]: iterations = %d, precision = %1.4e\n", i, it[i],
+                rr[i] / norm[i]);
+  } catch (...) {
+    for (double2 *b : bufs) cudaFree(b);
+    throw;
+  }
+  for (double2 *b : bufs) cudaFree(b);
+  return status;
+}
+
+}  // namespace yg

@@ -104,35 +104,47 @@ int cg_mshift(Lattice &L, const yg_inv_par &par, int num, const double *shift, d
   double atmp = c.sqnorm(r);
   int it = 0;
   int status = YG_OK;
+  // the per-shift x and k updates of one iteration run as one pass each over all active
+  // shifts (blas_mshift_xr / _kp); scalars follow cg.cpp:62-116 in the same order
+  std::vector<double *> ax(num), ak(num);
+  std::vector<double> abt(num), aat(num), ac3(num);
   while (++it) {
     apply_op(L, par.op, par.mass, q, p);
     double pq = c.prod_re(p, q);
     check_finite(pq, "cg_mshift");
     double beta_old = beta;
     beta = -(atmp / pq);
+    int na = 0;
     for (int n = 0; n < num; n++) {
       if (flag[n]) continue;
       c3[n] = c2[n] * c1[n] * beta_old;
       c3[n] /= (beta * alpha * (c1[n] - c2[n])) + (c1[n] * beta_old * (1 - shift[n] * beta));
-      double bt = beta * (c3[n] / c2[n]);
-      c.axpby(xs[n], {1, 0}, {-bt, 0}, k[n]);
+      ax[na] = xs[n];
+      ak[na] = k[n];
+      abt[na] = beta * (c3[n] / c2[n]);
+      na++;
     }
-    c.axpby(r, {1, 0}, {beta, 0}, q);
-    btmp = c.sqnorm(r);
+    btmp = blas_mshift_xr(L, r, q, beta, na, ax.data(), ak.data(), abt.data(), c.lo, c.n);
     alpha = btmp / atmp;
     int notconverged = 0;
+    na = 0;
     for (int n = 0; n < num; n++) {
       if (flag[n]) continue;
-      double at = alpha * (c3[n] * c3[n]) / (c2[n] * c2[n]);
-      c.axpby(k[n], {at, 0}, {c3[n], 0}, r);
+      aat[na] = alpha * (c3[n] * c3[n]) / (c2[n] * c2[n]);
+      ac3[na] = c3[n];
+      ak[na] = k[n];
+      na++;
       if (btmp * c3[n] * c3[n] < norm * par.prec) flag[n] = 1;
       else notconverged++;
       c1[n] = c2[n];
       c2[n] = c3[n];
     }
+    // k_n = at k_n + c3 r for the shifts active in this iteration; p = alpha p + r is only
+    // needed when the loop goes on
+    bool more = notconverged > 0 && !(par.maxiter > 0 && it >= par.maxiter);
+    blas_mshift_kp(L, more ? p : nullptr, r, alpha, na, ak.data(), aat.data(), ac3.data(), c.lo, c.n);
     if (notconverged == 0) break;
     if (par.maxiter > 0 && it >= par.maxiter) { status = YG_MAXITER; break; }
-    c.axpby(p, {alpha, 0}, {1, 0}, r);
     atmp = btmp;
   }
   log_line(par, "cg_mshift", it, btmp / norm);
