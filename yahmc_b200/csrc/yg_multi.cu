@@ -24,9 +24,34 @@ __device__ __forceinline__ long bidx(const Geom &g, int id, int k, int ncomp, in
   return fidx(g, id, k, ncomp) * nb + i;
 }
 
+struct MultiHopArgs {
+  Geom g;
+  const double2 *src;     // batched hop input
+  const double2 *src2;    // STEP 2: batched psi_e
+  double2 *dst;
+  const double2 *U;
+  const double2 *cpk;     // STEP 1 with clover: packed Hermitian inverse of the odd-site blocks
+  const double2 *cl;      // STEP 2 with clover: clover term
+  double diag;            // STEP 2: 4+m (clover) or (4+m)^2 (no clover)
+  double cfm1;
+  double coeff;           // +1/2 (step 1), -1/2 (step 2)
+  int lo, n, nb;          // output sites [lo, lo+n), nb systems
+  int sites;              // sites per block (blockDim = sites * nb)
+  int clover;
+  int g5;
+};
+
+// Shared memory of a block of S sites, entry-major so that the S sites of one entry are
+// consecutive (no bank conflicts between sites; the nb threads of a site broadcast):
+//   links  L[(slot*D*D + k)*S + j], slot 0..3 = U(x,mu), 4..7 = U(x-mu,mu)
+//   matrix M[e*S + j], e < 4*D*D: packed inverse words (step 1) or clover entries (step 2)
+//   nbr    N[slot*S + j]: neighbour site of slot (x+mu for 0..3, x-mu for 4..7)
+template <int D>
+__host__ __device__ constexpr int multi_smem_entries() { return 12 * D * D; }
+
 template <int D, int MU, int SIG>
-__device__ __forceinline__ void bhop_dir(double2 (&acc)[4][D], const double2 *src, const double2 *U, const Geom &g,
-                                         int nid, int lid, int nb, int i) {
+__device__ __forceinline__ void bhop_dir_s(double2 (&acc)[4][D], const double2 *src, const double2 *Ls,
+                                           const Geom &g, int nid, int S, int j, int nb, int i) {
   double2 h[2][D];
 #pragma unroll
   for (int c = 0; c < D; c++) {
@@ -48,8 +73,27 @@ __device__ __forceinline__ void bhop_dir(double2 (&acc)[4][D], const double2 *sr
       h[1][c] = SIG < 0 ? csub(p1, ctimesi(p3)) : cadd(p1, ctimesi(p3));
     }
   }
+  const int slot = SIG < 0 ? MU : 4 + MU;
+  const double2 *Lp = Ls + (long)slot * D * D * S + j;
   double2 chi[2][D];
-  link_mul<D, double, (SIG > 0)>(chi, h, U, g, lid, MU);
+#pragma unroll
+  for (int r = 0; r < D; r++) {
+    double2 s0 = make_double2(0, 0), s1 = make_double2(0, 0);
+#pragma unroll
+    for (int q = 0; q < D; q++) {
+      if (SIG > 0) {                                   // U^dag: element (q, r)
+        const double2 u = Lp[(q * D + r) * S];
+        cfmac(s0, u, h[0][q]);
+        cfmac(s1, u, h[1][q]);
+      } else {
+        const double2 u = Lp[(r * D + q) * S];
+        cfma(s0, u, h[0][q]);
+        cfma(s1, u, h[1][q]);
+      }
+    }
+    chi[0][r] = s0;
+    chi[1][r] = s1;
+  }
 #pragma unroll
   for (int c = 0; c < D; c++) {
     acc[0][c] = cadd(acc[0][c], chi[0][c]);
@@ -70,48 +114,61 @@ __device__ __forceinline__ void bhop_dir(double2 (&acc)[4][D], const double2 *sr
   }
 }
 
-struct MultiHopArgs {
-  Geom g;
-  const double2 *src;     // batched hop input
-  const double2 *src2;    // STEP 2: batched psi_e
-  double2 *dst;
-  const double2 *U;
-  const double2 *cpk;     // STEP 1 with clover: packed Hermitian inverse of the odd-site blocks
-  const double2 *cl;      // STEP 2 with clover: clover term
-  double diag;            // STEP 2: 4+m (clover) or (4+m)^2 (no clover)
-  double cfm1;
-  double coeff;           // +1/2 (step 1), -1/2 (step 2)
-  int lo, n, nb;          // output sites [lo, lo+n), nb systems
-  int clover;
-  int g5;
-};
-
 // STEP 1 (odd sites): dst = A_oo^-1 (coeff hop src)            (no clover: coeff hop src)
 // STEP 2 (even sites): dst = [g5] (A_ee src2 + coeff hop src)   (no clover: diag src2 + ...)
 // as schur_step1 / schur_step2 of the single-system operator (dirac.cpp:738-765)
 template <int D, int STEP>
-__global__ void __launch_bounds__(128) k_hop_multi(MultiHopArgs a) {
-  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (t >= (long)a.n * a.nb) return;
-  const int i = (int)(t % a.nb);
-  const int id = a.lo + (int)(t / a.nb);
+__global__ void __launch_bounds__(192) k_hop_multi(MultiHopArgs a) {
+  extern __shared__ double2 smem[];
+  const int S = a.sites, nb = a.nb;
+  double2 *Ls = smem;                                  // 8*D*D*S
+  double2 *Ms = smem + 8 * D * D * S;                  // 4*D*D*S
+  int *Ns = reinterpret_cast<int *>(smem + 12 * D * D * S);   // 8*S
   const Geom &g = a.g;
-  int c[4];
-  coords_of(g, id, c);
+  const int j = threadIdx.x / nb, i = threadIdx.x % nb;
+  const int s0 = blockIdx.x * S;
+  const bool active = s0 + j < a.n;
+  const int id = a.lo + s0 + j;
+  int c[4] = {0, 0, 0, 0};
+  if (active) {
+    coords_of(g, id, c);
+    for (int slot = i; slot < 8; slot += nb) Ns[slot * S + j] = neighbour(g, c, slot & 3, slot < 4 ? +1 : -1);
+  }
+  __syncthreads();
+  // stage the links and the site matrices of the block's sites, coalesced over sites
+  const int nsites = min(S, a.n - s0);
+  const int nent = a.clover ? 12 * D * D : 8 * D * D;
+  for (int q = threadIdx.x; q < nent * S; q += blockDim.x) {
+    const int e = q / S, jj = q - e * S;
+    if (jj >= nsites) continue;
+    const int sid = a.lo + s0 + jj;
+    double2 v;
+    if (e < 8 * D * D) {
+      const int slot = e / (D * D), k = e - slot * D * D;
+      const int lid = slot < 4 ? sid : Ns[slot * S + jj];
+      v = __ldg(a.U + fidx(g, lid, (slot & 3) * D * D + k, 4 * D * D));
+    } else {
+      const int w = e - 8 * D * D;
+      if (STEP == 1) v = __ldg(a.cpk + (long)w * g.Vh + (sid - g.Vh));
+      else v = __ldg(a.cl + fidx(g, sid, w, 4 * D * D));
+    }
+    smem[(long)e * S + jj] = v;
+  }
+  __syncthreads();
+  if (!active) return;
   double2 acc[4][D];
 #pragma unroll
   for (int s = 0; s < 4; s++)
 #pragma unroll
     for (int k = 0; k < D; k++) acc[s][k] = make_double2(0, 0);
-  int f, b;
-  f = neighbour(g, c, 0, +1); bhop_dir<D, 0, -1>(acc, a.src, a.U, g, f, id, a.nb, i);
-  b = neighbour(g, c, 0, -1); bhop_dir<D, 0, +1>(acc, a.src, a.U, g, b, b, a.nb, i);
-  f = neighbour(g, c, 1, +1); bhop_dir<D, 1, -1>(acc, a.src, a.U, g, f, id, a.nb, i);
-  b = neighbour(g, c, 1, -1); bhop_dir<D, 1, +1>(acc, a.src, a.U, g, b, b, a.nb, i);
-  f = neighbour(g, c, 2, +1); bhop_dir<D, 2, -1>(acc, a.src, a.U, g, f, id, a.nb, i);
-  b = neighbour(g, c, 2, -1); bhop_dir<D, 2, +1>(acc, a.src, a.U, g, b, b, a.nb, i);
-  f = neighbour(g, c, 3, +1); bhop_dir<D, 3, -1>(acc, a.src, a.U, g, f, id, a.nb, i);
-  b = neighbour(g, c, 3, -1); bhop_dir<D, 3, +1>(acc, a.src, a.U, g, b, b, a.nb, i);
+  bhop_dir_s<D, 0, -1>(acc, a.src, Ls, g, Ns[0 * S + j], S, j, nb, i);
+  bhop_dir_s<D, 0, +1>(acc, a.src, Ls, g, Ns[4 * S + j], S, j, nb, i);
+  bhop_dir_s<D, 1, -1>(acc, a.src, Ls, g, Ns[1 * S + j], S, j, nb, i);
+  bhop_dir_s<D, 1, +1>(acc, a.src, Ls, g, Ns[5 * S + j], S, j, nb, i);
+  bhop_dir_s<D, 2, -1>(acc, a.src, Ls, g, Ns[2 * S + j], S, j, nb, i);
+  bhop_dir_s<D, 2, +1>(acc, a.src, Ls, g, Ns[6 * S + j], S, j, nb, i);
+  bhop_dir_s<D, 3, -1>(acc, a.src, Ls, g, Ns[3 * S + j], S, j, nb, i);
+  bhop_dir_s<D, 3, +1>(acc, a.src, Ls, g, Ns[7 * S + j], S, j, nb, i);
   const bool bnd = spinor_zeroed(g, c[0]);
 #pragma unroll
   for (int s = 0; s < 4; s++)
@@ -119,8 +176,39 @@ __global__ void __launch_bounds__(128) k_hop_multi(MultiHopArgs a) {
     for (int k = 0; k < D; k++) acc[s][k] = bnd ? make_double2(0, 0) : cscale(acc[s][k], a.coeff);
   double2 out[4][D];
   if (STEP == 1) {
-    if (a.clover) cpk_site<D, double>(out, acc, a.cpk, id - g.Vh, g.Vh);
-    else {
+    if (a.clover) {
+      // packed Hermitian blocks (layout of cpk_site) from shared memory
+      constexpr int N = 2 * D, W = 2 * D * D;
+#pragma unroll
+      for (int blk = 0; blk < 2; blk++) {
+        const double2 *Cb = Ms + (long)blk * W * S + j;
+        double2 x[N], y[N];
+#pragma unroll
+        for (int r = 0; r < D; r++) {
+          x[r] = acc[2 * blk][r];
+          x[r + D] = acc[2 * blk + 1][r];
+        }
+#pragma unroll
+        for (int w = 0; w < D; w++) {
+          const double2 dd = Cb[w * S];
+          y[2 * w] = cscale(x[2 * w], dd.x);
+          y[2 * w + 1] = cscale(x[2 * w + 1], dd.y);
+        }
+#pragma unroll
+        for (int r = 1; r < N; r++)
+#pragma unroll
+          for (int q = 0; q < r; q++) {
+            const double2 m = Cb[(D + r * (r - 1) / 2 + q) * S];
+            cfma(y[r], m, x[q]);
+            cfmac(y[q], m, x[r]);
+          }
+#pragma unroll
+        for (int r = 0; r < D; r++) {
+          out[2 * blk][r] = y[r];
+          out[2 * blk + 1][r] = y[r + D];
+        }
+      }
+    } else {
 #pragma unroll
       for (int s = 0; s < 4; s++)
 #pragma unroll
@@ -134,28 +222,28 @@ __global__ void __launch_bounds__(128) k_hop_multi(MultiHopArgs a) {
         const double diag = a.diag + ((c[0] == g.Ta || c[0] == g.Tb) ? a.cfm1 : 0.0);
 #pragma unroll
         for (int blk = 0; blk < 2; blk++) {
-          const int s0 = 2 * blk, s1 = 2 * blk + 1;
+          const int s0b = 2 * blk, s1b = 2 * blk + 1;
           double2 p0[D], p1[D];
 #pragma unroll
           for (int q = 0; q < D; q++) {
-            p0[q] = __ldg(a.src2 + bidx(g, id, s0 * D + q, 4 * D, a.nb, i));
-            p1[q] = __ldg(a.src2 + bidx(g, id, s1 * D + q, 4 * D, a.nb, i));
+            p0[q] = __ldg(a.src2 + bidx(g, id, s0b * D + q, 4 * D, nb, i));
+            p1[q] = __ldg(a.src2 + bidx(g, id, s1b * D + q, 4 * D, nb, i));
           }
 #pragma unroll
           for (int r = 0; r < D; r++) {
-            double2 o0 = cadd(acc[s0][r], cscale(p0[r], diag)), o1 = cadd(acc[s1][r], cscale(p1[r], diag));
+            double2 o0 = cadd(acc[s0b][r], cscale(p0[r], diag)), o1 = cadd(acc[s1b][r], cscale(p1[r], diag));
 #pragma unroll
             for (int q = 0; q < D; q++) {
-              double2 a0 = __ldg(a.cl + fidx(g, id, s0 * D * D + r * D + q, 4 * D * D));
-              double2 a1 = __ldg(a.cl + fidx(g, id, s1 * D * D + r * D + q, 4 * D * D));
-              double2 a1t = __ldg(a.cl + fidx(g, id, s1 * D * D + q * D + r, 4 * D * D));
+              const double2 a0 = Ms[(s0b * D * D + r * D + q) * S + j];
+              const double2 a1 = Ms[(s1b * D * D + r * D + q) * S + j];
+              const double2 a1t = Ms[(s1b * D * D + q * D + r) * S + j];
               cfma(o0, a0, p0[q]);
               cfma(o0, a1, p1[q]);
               cfmac(o1, a1t, p0[q]);
               o1 = csub(o1, cmul(a0, p1[q]));
             }
-            acc[s0][r] = o0;
-            acc[s1][r] = o1;
+            acc[s0b][r] = o0;
+            acc[s1b][r] = o1;
           }
         }
       } else {
@@ -163,7 +251,7 @@ __global__ void __launch_bounds__(128) k_hop_multi(MultiHopArgs a) {
         for (int s = 0; s < 4; s++)
 #pragma unroll
           for (int k = 0; k < D; k++) {
-            double2 v = __ldg(a.src2 + bidx(g, id, s * D + k, 4 * D, a.nb, i));
+            double2 v = __ldg(a.src2 + bidx(g, id, s * D + k, 4 * D, nb, i));
             acc[s][k] = cadd(acc[s][k], cscale(v, a.diag));
           }
       }
@@ -176,7 +264,7 @@ __global__ void __launch_bounds__(128) k_hop_multi(MultiHopArgs a) {
 #pragma unroll
   for (int s = 0; s < 4; s++)
 #pragma unroll
-    for (int k = 0; k < D; k++) a.dst[bidx(g, id, s * D + k, 4 * D, a.nb, i)] = out[s][k];
+    for (int k = 0; k < D; k++) a.dst[bidx(g, id, s * D + k, 4 * D, nb, i)] = out[s][k];
 }
 
 // ---- batched BLAS over the words [w0, w0 + cnt) of every system.  Block size 32*nb, so a
@@ -368,10 +456,14 @@ static void hphi_multi(Lattice &L, int nb, double mass, double2 *dst, const doub
   s2.n = (int)L.Vh;
   s2.g5 = 1;
   s2.diag = a.clover ? 4.0 + mass : (4.0 + mass) * (4.0 + mass);
-  const long n = (long)L.Vh * nb;
-  k_hop_multi<3, 1><<<nblk(n, 128), 128, 0, L.stream>>>(s1);
+  // blocks of S sites x nb systems (about 192 threads), shared memory for S sites
+  const int S = std::min(24, std::max(1, 192 / nb));      // <= 24 sites: 42 KB of shared memory
+  s1.sites = s2.sites = S;
+  const size_t smem = sizeof(double2) * (size_t)multi_smem_entries<3>() * S + sizeof(int) * 8 * S;
+  const int blocks = nblk(L.Vh, S);
+  k_hop_multi<3, 1><<<blocks, S * nb, smem, L.stream>>>(s1);
   YG_LAUNCHED();
-  k_hop_multi<3, 2><<<nblk(n, 128), 128, 0, L.stream>>>(s2);
+  k_hop_multi<3, 2><<<blocks, S * nb, smem, L.stream>>>(s2);
   YG_LAUNCHED();
   L.mvm += 2;
 }
