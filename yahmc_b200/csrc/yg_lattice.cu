@@ -44,6 +44,10 @@ Lattice::~Lattice() {
   if (host_result) cudaFreeHost(host_result);
   if (sl_hist) cudaFreeHost(sl_hist);
   for (cudaEvent_t e : sl_ev) if (e) cudaEventDestroy(e);
+  if (stream) {
+    cudaStreamSynchronize(stream);
+    cudaStreamDestroy(stream);
+  }
   for (DevBuf *b : {&fund, &links, &clover, &ldl, &cl_force, &mom, &tables, &red_partial, &red_result, &links_f,
                     &clover_f, &cinv_f, &sl_links, &sl_clover, &cpk64, &sl_part, &sl_scal, &fund_backup})
     b->release();
@@ -275,6 +279,9 @@ Lattice *lattice_create(const yg_params &p) {
   YG_CUDA(cudaGetDeviceCount(&dev_count));
   Lattice *L = new Lattice();
   try {
+    // the lattice's own stream; a blocking stream, so work on the legacy default stream
+    // (and events recorded there) still orders with it
+    YG_CUDA(cudaStreamCreateWithFlags(&L->stream, cudaStreamDefault));
     L->p = p;
     L->d = d;
     L->nc = p.nc;

@@ -15,6 +15,10 @@
 // Arithmetic is FP32 throughout; FP16 is a storage format only.
 #include <cuda_fp16.h>
 #include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <thread>
 #include "yg_lattice.h"
 #include "yg_kernels.h"
 
@@ -303,30 +307,50 @@ __device__ __forceinline__ void shop_dir(float2 (&acc)[12], const SHopArgs &a, i
   }
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream serialisation
+// may start while its predecessor drains; it computes what needs no predecessor data
+// (coordinates, neighbour indices), then waits for the predecessor grid to complete and its
+// memory to be visible.  Each kernel signals its successor once its block has stored its
+// results.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
+// the neighbours of a site: f[mu] = x+mu, b[mu] = x-mu
+struct SiteNbr {
+  int c[4];
+  int f[4], b[4];
+};
+
+__device__ __forceinline__ void site_nbr(SiteNbr &n, const Geom &g, int id) {
+  coords_of(g, id, n.c);
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++) {
+    n.f[mu] = neighbour(g, n.c, mu, +1);
+    n.b[mu] = neighbour(g, n.c, mu, -1);
+  }
+}
+
 // STEP 1 (odd output):  dst = M_o^-1 (coeff * hop(src))
 // STEP 2 (even output): dst = gamma5 (M_e src2 + coeff * hop(src))
 // returns |dst|^2 of the site (before FP16 rounding)
 template <int P, int K, int STEP>
-__device__ __forceinline__ float shop_site(const SHopArgs &a, int id) {
+__device__ __forceinline__ float shop_site(const SHopArgs &a, int id, const SiteNbr &n) {
   const Geom &g = a.g;
-  int c[4];
-  coords_of(g, id, c);
-  int T = g.dim[0];
+  const int T = g.dim[0], t0 = n.c[0];
   float2 acc[12];
 #pragma unroll
   for (int k = 0; k < 12; k++) acc[k] = make_float2(0.f, 0.f);
-  int f, b;
-  f = neighbour(g, c, 0, +1); shop_dir<P, K, 0, -1>(acc, a, f, id, c[0]);
-  b = neighbour(g, c, 0, -1); shop_dir<P, K, 0, +1>(acc, a, b, b, c[0] == 0 ? T - 1 : c[0] - 1);
-  f = neighbour(g, c, 1, +1); shop_dir<P, K, 1, -1>(acc, a, f, id, c[0]);
-  b = neighbour(g, c, 1, -1); shop_dir<P, K, 1, +1>(acc, a, b, b, c[0]);
-  f = neighbour(g, c, 2, +1); shop_dir<P, K, 2, -1>(acc, a, f, id, c[0]);
-  b = neighbour(g, c, 2, -1); shop_dir<P, K, 2, +1>(acc, a, b, b, c[0]);
-  f = neighbour(g, c, 3, +1); shop_dir<P, K, 3, -1>(acc, a, f, id, c[0]);
-  b = neighbour(g, c, 3, -1); shop_dir<P, K, 3, +1>(acc, a, b, b, c[0]);
+  shop_dir<P, K, 0, -1>(acc, a, n.f[0], id, t0);
+  shop_dir<P, K, 0, +1>(acc, a, n.b[0], n.b[0], t0 == 0 ? T - 1 : t0 - 1);
+  shop_dir<P, K, 1, -1>(acc, a, n.f[1], id, t0);
+  shop_dir<P, K, 1, +1>(acc, a, n.b[1], n.b[1], t0);
+  shop_dir<P, K, 2, -1>(acc, a, n.f[2], id, t0);
+  shop_dir<P, K, 2, +1>(acc, a, n.b[2], n.b[2], t0);
+  shop_dir<P, K, 3, -1>(acc, a, n.f[3], id, t0);
+  shop_dir<P, K, 3, +1>(acc, a, n.b[3], n.b[3], t0);
   int blk = id >= g.Vh, h = id - blk * g.Vh;
   float2 out[12];
-  bool bnd = spinor_zeroed(g, c[0]);
+  bool bnd = spinor_zeroed(g, t0);
   float cl[72];
   cload<P>(cl, a.C, blk, h, g.Vh);
   if (STEP == 1) {
@@ -360,13 +384,23 @@ template <int P, int K, int STEP, int NRM>
 __global__ void __launch_bounds__(128) k_shop(SHopArgs a) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (!NRM) {
-    if (t < a.n) shop_site<P, K, STEP>(a, a.lo + t);
+    SiteNbr n;
+    if (t < a.n) site_nbr(n, a.g, a.lo + t);
+    griddep_wait();
+    if (t < a.n) shop_site<P, K, STEP>(a, a.lo + t, n);
+    griddep_launch();
     return;
   }
+  griddep_wait();
   double n2 = 0.0;
-  for (; t < a.n; t += gridDim.x * blockDim.x) n2 += (double)shop_site<P, K, STEP>(a, a.lo + t);
+  for (; t < a.n; t += gridDim.x * blockDim.x) {
+    SiteNbr n;
+    site_nbr(n, a.g, a.lo + t);
+    n2 += (double)shop_site<P, K, STEP>(a, a.lo + t, n);
+  }
   n2 = block_total(n2);
   if (threadIdx.x == 0) a.part[blockIdx.x] = n2;
+  griddep_launch();
 }
 
 // ------------------------------------------------------------------ builds (once per gauge field / mass)
@@ -505,6 +539,7 @@ __global__ void __launch_bounds__(256) k_s_cg_update(float2 *x, float2 *r, const
                                                      const void *q, const float *qn, double *scal,
                                                      const double *part_pq, int n_pq, double *part_r, int par,
                                                      int Vh) {
+  griddep_wait();
   const double pq = sum_partials(part_pq, n_pq);
   const double alpha = scal[S_RR0 + par] / pq;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -534,19 +569,24 @@ __global__ void __launch_bounds__(256) k_s_cg_update(float2 *x, float2 *r, const
   }
   acc = block_total(acc);
   if (threadIdx.x == 0) part_r[blockIdx.x] = acc;
+  griddep_launch();
 }
 
 // |r|^2 from the update's partials, beta = |r|^2 / |r_old|^2, p = r + beta p; block 0
-// stores |r|^2 for the next iteration and into *hist (mapped host memory the host reads
-// one iteration later)
+// stores |r|^2 for the next iteration and into *hist, then the iteration number into *seq
+// (both mapped host memory, which the host polls one iteration later)
 template <int P>
 __global__ void __launch_bounds__(256) k_s_xpay(void *p, float *pn, double *scal, const double *part_r, int n_r,
-                                                int par, double *hist, const float2 *r, int Vh) {
+                                                int par, double *hist, unsigned long long *seq,
+                                                unsigned long long iter, const float2 *r, int Vh) {
+  griddep_wait();
   const double rr = sum_partials(part_r, n_r);
   const float b = (float)(rr / scal[S_RR0 + par]);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     scal[S_RR0 + (par ^ 1)] = rr;
-    *hist = rr;
+    *reinterpret_cast<volatile double *>(hist) = rr;
+    __threadfence_system();
+    *reinterpret_cast<volatile unsigned long long *>(seq) = iter;
   }
   for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += gridDim.x * blockDim.x) {
     float2 pp[12];
@@ -558,6 +598,7 @@ __global__ void __launch_bounds__(256) k_s_xpay(void *p, float *pn, double *scal
     }
     sstore<P>(p, pn, pp, 0, h, Vh);
   }
+  griddep_launch();
 }
 
 __global__ void k_s_set(double *scal, int i, double v) { scal[i] = v; }
@@ -601,8 +642,8 @@ void ensure_sloppy(Lattice &L, double mass, int prec, int reals) {
     throw Error(YG_ERR_ARG, "12-real links need SU(3) fundamental links");
   if (!L.p.eo) throw Error(YG_ERR_ARG, "the mixed-precision solver needs even-odd preconditioning");
   if (!L.sl_hist) {
-    YG_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&L.sl_hist), 4 * sizeof(double), cudaHostAllocMapped));
-    for (cudaEvent_t &e : L.sl_ev) YG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    // mapped host words: [0], [1] the |r|^2 of the last two iterations, [4] their counter
+    YG_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&L.sl_hist), 8 * sizeof(double), cudaHostAllocMapped));
     L.sl_scal.alloc(S_WORDS * sizeof(double));
     YG_CUDA(cudaMemsetAsync(L.sl_scal.p, 0, S_WORDS * sizeof(double), L.stream));
   }
@@ -642,7 +683,25 @@ void ensure_sloppy(Lattice &L, double mass, int prec, int reals) {
   L.sl_valid = true;
 }
 
+// launch with programmatic stream serialisation (the kernel waits for its predecessor
+// itself, griddep_wait)
+template <typename... KArgs, typename... Args>
+static void launch_pdl(void (*kern)(KArgs...), int grid, int block, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  YG_CUDA(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
+}
+
 static double *dscal(Lattice &L) { return L.sl_scal.as<double>(); }
+static unsigned long long *hist_seq(Lattice &L) { return reinterpret_cast<unsigned long long *>(L.sl_hist + 4); }
 static double *part_pq(Lattice &L) { return L.sl_part.as<double>(); }
 static double *part_r(Lattice &L) { return L.sl_part.as<double>() + L.sl_grid_nrm; }
 
@@ -665,10 +724,10 @@ static void sloppy_hphi(Lattice &L, SField dst, SField src, SField tmp, bool nrm
   b.lo = 0;
   b.part = part_pq(L);
   YG_SLOPPY_DISPATCH(L.sl_prec, L.sl_reals, {
-    k_shop<SP, SK, 1, 0><<<nblk(a.n, 128), 128, 0, L.stream>>>(a);
+    launch_pdl(k_shop<SP, SK, 1, 0>, nblk(a.n, 128), 128, L.stream, a);
     YG_LAUNCHED();
-    if (nrm) k_shop<SP, SK, 2, 1><<<L.sl_grid_nrm, 128, 0, L.stream>>>(b);
-    else k_shop<SP, SK, 2, 0><<<nblk(b.n, 128), 128, 0, L.stream>>>(b);
+    if (nrm) launch_pdl(k_shop<SP, SK, 2, 1>, L.sl_grid_nrm, 128, L.stream, b);
+    else launch_pdl(k_shop<SP, SK, 2, 0>, nblk(b.n, 128), 128, L.stream, b);
     YG_LAUNCHED();
   });
   L.mvm += 2;
@@ -677,19 +736,35 @@ static void sloppy_hphi(Lattice &L, SField dst, SField src, SField tmp, bool nrm
 // par = iteration parity (selects the |r|^2 slot)
 static void sloppy_cg_update(Lattice &L, float *x, float *r, SField p, SField q, int par) {
   YG_SLOPPY_DISPATCH(L.sl_prec, 18, {
-    k_s_cg_update<SP><<<L.sl_grid_vec, 256, 0, L.stream>>>((float2 *)x, (float2 *)r, p.data, p.norm, q.data, q.norm,
-                                                           dscal(L), part_pq(L), L.sl_grid_nrm, part_r(L), par,
-                                                           (int)L.Vh);
+    launch_pdl(k_s_cg_update<SP>, L.sl_grid_vec, 256, L.stream, (float2 *)x, (float2 *)r, p.data, p.norm, q.data,
+               q.norm, dscal(L), part_pq(L), L.sl_grid_nrm, part_r(L), par, (int)L.Vh);
     YG_LAUNCHED();
   });
 }
 
-static void sloppy_xpay(Lattice &L, SField p, const float *r, int par, double *hist) {
+static void sloppy_xpay(Lattice &L, SField p, const float *r, int par, double *hist, unsigned long long iter) {
   YG_SLOPPY_DISPATCH(L.sl_prec, 18, {
-    k_s_xpay<SP><<<L.sl_grid_vec, 256, 0, L.stream>>>(p.data, p.norm, dscal(L), part_r(L), L.sl_grid_vec, par, hist,
-                                                      (const float2 *)r, (int)L.Vh);
+    launch_pdl(k_s_xpay<SP>, L.sl_grid_vec, 256, L.stream, p.data, p.norm, dscal(L), part_r(L), L.sl_grid_vec, par,
+               hist, hist_seq(L), iter, (const float2 *)r, (int)L.Vh);
     YG_LAUNCHED();
   });
+}
+
+// wait until the GPU has finished inner iteration `iter` (its xpay wrote the counter);
+// a GPU error or a counter that stops advancing for 30 s ends the wait with an error
+static void wait_iteration(Lattice &L, unsigned long long iter) {
+  volatile unsigned long long *seq = hist_seq(L);
+  if (*seq >= iter) return;
+  auto t0 = std::chrono::steady_clock::now();
+  while (*seq < iter) {
+    const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (dt > 1e-3) std::this_thread::yield();
+    if (dt > 30.0) {
+      YG_CUDA(cudaStreamSynchronize(L.stream));
+      if (*seq < iter) throw Error(YG_TIMEOUT, "cg_mixed: the inner iteration counter stopped advancing");
+      return;
+    }
+  }
 }
 
 static void sloppy_from_d(Lattice &L, SField dst, const double *src) {
@@ -717,10 +792,6 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, doub
 
 }  // namespace yg
 
-#include <chrono>
-#include <cmath>
-#include <cstdio>
-
 namespace yg {
 
 int cg(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
@@ -739,6 +810,7 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, doub
   float *fx = reinterpret_cast<float *>(L.scratch_field(42));
   SField p = sfield(L, 41), q = sfield(L, 43), t = sfield(L, 44), o = sfield(L, 45);
   volatile double *hist = L.sl_hist;
+  *hist_seq(L) = 0;                 // no GPU work of this lattice is in flight here
 
   auto residual = [&]() {           // r = b - A x in FP64, returns |r|^2
     blas_copy(L, xd, x);
@@ -779,12 +851,11 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, doub
       sloppy_hphi(L, t, p, o, true);
       sloppy_hphi(L, q, t, o, false);
       sloppy_cg_update(L, fx, fr, p, q, slot);
-      sloppy_xpay(L, p, fr, slot, const_cast<double *>(hist) + slot);
-      YG_CUDA(cudaEventRecord(L.sl_ev[slot], L.stream));
+      sloppy_xpay(L, p, fr, slot, const_cast<double *>(hist) + slot, (unsigned long long)it + 1);
       it++;
       if (!pending) { pending = true; continue; }
       // the previous iteration's |r|^2, read while this one runs
-      YG_CUDA(cudaEventSynchronize(L.sl_ev[slot ^ 1]));
+      wait_iteration(L, (unsigned long long)it - 1);
       double rr_prev = hist[slot ^ 1];
       if (!std::isfinite(rr_prev)) throw Error(YG_NONFINITE, "non-finite value in cg_mixed");
       if (rr_prev < 0.25 * min_cycle) { min_cycle = rr_prev; since_min = 0; }
