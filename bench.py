@@ -72,19 +72,25 @@ def parse():
 
 # inner operator of the mixed-precision solver: None = generic FP32 (every representation),
 # (spinor bits, link reals) = the compressed d = 3 operator
-INNER = {"generic-f32": (0, 18), "f32-l18": (32, 18), "f32-l12": (32, 12), "f16-l18": (16, 18), "f16-l12": (16, 12)}
+INNER = {"generic-f32": (0, 18, 0, 0), "f32-l18": (32, 18, 0, 0), "f32-l12": (32, 12, 0, 0),
+         "f16-l18": (16, 18, 0, 0), "f16-l12": (16, 12, 0, 0),
+         "f32-i16links-l12": (32, 12, 15, 32), "f32-i16-l12": (32, 12, 15, 15), "f16-i16-l12": (16, 12, 15, 15)}
 
 
 DTYPE = {"generic-f32": "f32 inner / f64 reliable updates and residual",
          "f32-l18": "f32 inner / f64 reliable updates and residual",
          "f32-l12": "f32 inner (12-real links) / f64 reliable updates and residual",
          "f16-l18": "f32 inner arithmetic on f16 storage / f64 reliable updates and residual",
-         "f16-l12": "f32 inner arithmetic on f16 storage (12-real links) / f64 reliable updates and residual"}
+         "f16-l12": "f32 inner arithmetic on f16 storage (12-real links) / f64 reliable updates and residual",
+         "f32-i16links-l12": "f32 inner (int16 12-real links) / f64 reliable updates and residual",
+         "f32-i16-l12": "f32 inner (int16 12-real links and clover) / f64 reliable updates and residual",
+         "f16-i16-l12": "f32 inner arithmetic on f16 spinors, int16 links and clover / f64 reliable updates and residual"}
 
 
 def solve_mixed(lat, x, b, inner, delta):
     spec = INNER[inner]
-    return lat.cg_mixed("Hphi_sq", MASS, PREC, x, b, inner_precision=spec[0], link_reals=spec[1], delta=delta)
+    return lat.cg_mixed("Hphi_sq", MASS, PREC, x, b, inner_precision=spec[0], link_reals=spec[1], delta=delta,
+                        link_storage=spec[2], clover_storage=spec[3])
 
 
 def hbm_peak():

@@ -195,12 +195,17 @@ int yg_cg_inverter_multi(yg_lattice *lat, const yg_inv_par *par, int nrhs, doubl
  *                    arithmetic; 0 selects the generic FP32 operator of yg_cg_mixed (any d)
  *   link_reals       18, or 12 (two rows, third rebuilt; SU(3) fundamental only)
  *   delta            reliable update when |r| falls below delta * |r| at the last update
+ *   link_storage,    storage of the inner operator's links and clover blocks; the combinations
+ *   clover_storage   built are all-FP32, FP32 spinors with int16 links (FP32 or int16 clover),
+ *                    and FP16 spinors with FP16 or int16 matrices
  * The compressed inner operator exists for d = 3 representations with even-odd
  * preconditioning; the stopping test is the true FP64 residual, as for yg_cg_mixed. */
 typedef struct {
   int inner_precision;
   int link_reals;
   double delta;
+  int link_storage;     /* 0: as inner_precision; 32 FP32, 16 FP16, 15 int16 fixed point (entries / 32767) */
+  int clover_storage;   /* 0: as inner_precision; 32, 16, or 15 (int16 with a per-site scale) */
 } yg_mixed_opts;
 int yg_cg_mixed_opts(yg_lattice *lat, const yg_inv_par *par, const yg_mixed_opts *opts, double *x, double *b,
                      yg_solve_stats *stats);

@@ -23,14 +23,19 @@ def _true_residual(lat, op, mass, x, b):
     return lat.spinor_sqnorm(v) / lat.spinor_sqnorm(b)
 
 
-CASES = [("su3_fund_ap", 32, 12), ("su3_fund_ap", 32, 18), ("su3_fund_ap", 16, 12), ("su3_fund_ap", 16, 18),
-         ("su3_fund_open", 16, 12), ("su3_fund_sf", 32, 12), ("su3_fund_per", 16, 12),
-         ("su3_fund_ap_nocl", 16, 12), ("su2_adj_ap", 32, 18), ("su2_adj_ap", 16, 18),
-         ("su3_fund_ap", 0, 18), ("su2_adj_ap", 0, 18)]          # 0: the generic FP32 inner operator
+CASES = [("su3_fund_ap", 32, 12, 0, 0), ("su3_fund_ap", 32, 18, 0, 0), ("su3_fund_ap", 16, 12, 0, 0),
+         ("su3_fund_ap", 16, 18, 0, 0), ("su3_fund_open", 16, 12, 0, 0), ("su3_fund_sf", 32, 12, 0, 0),
+         ("su3_fund_per", 16, 12, 0, 0), ("su3_fund_ap_nocl", 16, 12, 0, 0), ("su2_adj_ap", 32, 18, 0, 0),
+         ("su2_adj_ap", 16, 18, 0, 0),
+         ("su3_fund_ap", 0, 18, 0, 0), ("su2_adj_ap", 0, 18, 0, 0),          # 0: the generic FP32 inner operator
+         # int16 fixed-point links / clover blocks (storage 15)
+         ("su3_fund_ap", 32, 12, 15, 32), ("su3_fund_ap", 32, 12, 15, 15), ("su3_fund_open", 32, 12, 15, 15),
+         ("su3_fund_sf", 32, 18, 15, 15), ("su3_fund_ap_nocl", 32, 12, 15, 15), ("su2_adj_ap", 32, 18, 15, 15),
+         ("su3_fund_ap", 16, 12, 15, 15)]
 
 
-@pytest.mark.parametrize("name,inner,reals", CASES)
-def test_compressed_inner_cg(name, inner, reals):
+@pytest.mark.parametrize("name,inner,reals,lfmt,cfmt", CASES)
+def test_compressed_inner_cg(name, inner, reals, lfmt, cfmt):
     dims = (8, 8, 8, 8) if name.startswith("su3") else (4, 6, 4, 8)
     lat, O, rng = make_pair(name, dims, seed=31)
     b0 = source(O, rng)
@@ -39,13 +44,24 @@ def test_compressed_inner_cg(name, inner, reals):
     it64 = lat.cg_inverter("Hphi_sq", mass, 1e-24, x64, b)
     for prec in (1e-24, 1e-28):
         x = lat.field()
-        st = lat.cg_mixed("Hphi_sq", mass, prec, x, b, inner_precision=inner, link_reals=reals, delta=0.1)
+        st = lat.cg_mixed("Hphi_sq", mass, prec, x, b, inner_precision=inner, link_reals=reals, delta=0.1,
+                          link_storage=lfmt, clover_storage=cfmt)
         assert st["status"] == 0, st
         assert st["fallback"] == 0, st
         assert st["true_residual"] < prec
         assert _true_residual(lat, "Hphi_sq", mass, x, b) < prec
         if prec == 1e-24:
             assert st["iterations"] <= 1.5 * it64 + 10, (st, it64)
+
+
+def test_storage_format_errors():
+    from yahmc_b200 import YGError
+    lat, O, rng = make_pair("su3_fund_ap", (4, 4, 4, 4), seed=37)
+    b, x = lat.field(source(O, rng)), lat.field()
+    for lfmt, cfmt in [(16, 32), (32, 16), (15, 16), (7, 7)]:          # combinations not built
+        with pytest.raises(YGError):
+            lat.cg_mixed("Hphi_sq", -0.4, 1e-20, x, b, inner_precision=32, link_reals=12, link_storage=lfmt,
+                         clover_storage=cfmt)
 
 
 @pytest.mark.parametrize("delta", [0.01, 0.3, 1e-4])

@@ -49,7 +49,7 @@ Lattice::~Lattice() {
     cudaStreamDestroy(stream);
   }
   for (DevBuf *b : {&fund, &links, &clover, &ldl, &cl_force, &mom, &tables, &red_partial, &red_result, &links_f,
-                    &clover_f, &cinv_f, &sl_links, &sl_clover, &cpk64, &sl_part, &sl_scal, &fund_backup})
+                    &clover_f, &cinv_f, &sl_links, &sl_clover, &cpk64, &sl_part, &sl_scal, &fund_backup, &sl_cnorm})
     b->release();
 }
 

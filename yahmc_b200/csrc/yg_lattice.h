@@ -87,7 +87,8 @@ struct Lattice {
   // compressed inner operator of the mixed solver for d = 3 (yg_sloppy.cu)
   DevBuf sl_links;  // 12 or 18 reals per link, FP32 or FP16
   DevBuf sl_clover; // packed Hermitian blocks: M_e on even sites, M_o^-1 on odd sites
-  int sl_prec = 0, sl_reals = 0;
+  int sl_prec = 0, sl_reals = 0, sl_lfmt = 0, sl_cfmt = 0;
+  DevBuf sl_cnorm;     // per-site scales of int16 clover records
   double sl_mass = 0;
   bool sl_valid = false;
   DevBuf sl_part;      // per-block partial sums of the device-scalar reductions
@@ -175,8 +176,8 @@ int auto_inverter(Lattice &L, const yg_inv_par &par, double *x, double *b, int *
 int rational_calc(Lattice &L, const yg_inv_par &par, double a0, int order, const double *poles,
                   const double *residues, double *x, double *b, int *iters);
 int cg_mixed(Lattice &L, const yg_inv_par &par, double *x, double *b, yg_solve_stats *st);
-int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, double delta, double *x, double *b,
-                    yg_solve_stats *st);
+int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int lfmt, int cfmt, double delta,
+                    double *x, double *b, yg_solve_stats *st);
 
 // ---- yg_forces.cu
 void clover_fermion_force(Lattice &L, double residue, double *lhs, double *rhs);

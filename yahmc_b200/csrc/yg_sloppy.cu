@@ -112,19 +112,36 @@ __device__ __forceinline__ void sstore(void *base, float *norm, const float2 (&s
   }
 }
 
-// Links: complex word k of link (site blk,h ; mu): FP32 float2 / FP16 half2 at
-//   U[((blk*4 + mu)*K + k)*Vh + h], K = 9 (18 reals, row-major) or 6 (rows 0,1)
-template <int P>
-__device__ __forceinline__ float2 lload(const void *base, long i) {
-  if (P == 32) return __ldg(reinterpret_cast<const float2 *>(base) + i);
-  unsigned v = __ldg(reinterpret_cast<const unsigned *>(base) + i);
-  return h2f(v);
+// Storage formats of the inner operator's matrices (links and clover blocks):
+//   ST_F32  FP32;  ST_F16  FP16;  ST_I16  16-bit fixed point (value = int16 / 32767 times a
+//   scale: 1 for links, whose entries lie in [-1, 1], and a per-site max |entry| for the
+//   clover blocks), 15 significant bits against FP16's 11.
+constexpr int ST_F32 = 32, ST_F16 = 16, ST_I16 = 15;
+constexpr float kI16 = 32767.f;
+
+__device__ __forceinline__ float2 s2f(unsigned v) {          // two int16 -> two float (unscaled)
+  return make_float2((float)(short)(v & 0xffffu), (float)(short)(v >> 16));
+}
+__device__ __forceinline__ unsigned f2s(float a, float b) {   // two floats in [-1,1] -> two int16
+  int ia = __float2int_rn(fminf(fmaxf(a, -1.f), 1.f) * kI16);
+  int ib = __float2int_rn(fminf(fmaxf(b, -1.f), 1.f) * kI16);
+  return ((unsigned)ia & 0xffffu) | ((unsigned)ib << 16);
 }
 
-template <int P, int K>
+// Links: complex word k of link (site blk,h ; mu): FP32 float2, FP16 half2 or int16 pair at
+//   U[((blk*4 + mu)*K + k)*Vh + h], K = 9 (18 reals, row-major) or 6 (rows 0,1)
+template <int LP>
+__device__ __forceinline__ float2 lload(const void *base, long i) {
+  if (LP == ST_F32) return __ldg(reinterpret_cast<const float2 *>(base) + i);
+  unsigned v = __ldg(reinterpret_cast<const unsigned *>(base) + i);
+  if (LP == ST_F16) return h2f(v);
+  return cscale(s2f(v), 1.f / kI16);
+}
+
+template <int LP, int K>
 __device__ __forceinline__ void link_load(float2 (&u)[9], const void *U, int blk, int h, int Vh, int mu, float sgn) {
 #pragma unroll
-  for (int k = 0; k < K; k++) u[k] = lload<P>(U, ((long)(blk * 4 + mu) * K + k) * Vh + h);
+  for (int k = 0; k < K; k++) u[k] = lload<LP>(U, ((long)(blk * 4 + mu) * K + k) * Vh + h);
   if (K == 6) {
     // row 2 = conj(row0 x row1); the stored rows carry the antiperiodic sign s, and
     // (s r0) x (s r1) = r0 x r1, so the reconstructed row is multiplied by s again
@@ -136,11 +153,11 @@ __device__ __forceinline__ void link_load(float2 (&u)[9], const void *U, int blk
 }
 
 // Packed Hermitian blocks: 72 reals per site (block b: 6 diagonal reals, then the 15
-// complex lower-triangle entries (1,0),(2,0),(2,1),...,(5,4)), FP32 as 18 float4 / FP16 as
-// 9 uint4 at C[(blk*W + w)*Vh + h].
-template <int P>
-__device__ __forceinline__ void cload(float (&c)[72], const void *base, int blk, int h, int Vh) {
-  if (P == 32) {
+// complex lower-triangle entries (1,0),(2,0),(2,1),...,(5,4)), FP32 as 18 float4, FP16 or
+// int16 as 9 uint4 at C[(blk*W + w)*Vh + h]; int16 records scale by cn[blk*Vh + h] / 32767.
+template <int CP>
+__device__ __forceinline__ void cload(float (&c)[72], const void *base, const float *cn, int blk, int h, int Vh) {
+  if (CP == ST_F32) {
     const float4 *f = reinterpret_cast<const float4 *>(base);
 #pragma unroll
     for (int w = 0; w < 18; w++) {
@@ -149,10 +166,13 @@ __device__ __forceinline__ void cload(float (&c)[72], const void *base, int blk,
     }
   } else {
     const uint4 *f = reinterpret_cast<const uint4 *>(base);
+    const float sc = CP == ST_I16 ? __ldg(cn + (long)blk * Vh + h) * (1.f / kI16) : 1.f;
 #pragma unroll
     for (int w = 0; w < 9; w++) {
       uint4 v = __ldg(f + (long)(blk * 9 + w) * Vh + h);
-      float2 a = h2f(v.x), b = h2f(v.y), cc = h2f(v.z), d = h2f(v.w);
+      float2 a, b, cc, d;
+      if (CP == ST_F16) { a = h2f(v.x); b = h2f(v.y); cc = h2f(v.z); d = h2f(v.w); }
+      else { a = cscale(s2f(v.x), sc); b = cscale(s2f(v.y), sc); cc = cscale(s2f(v.z), sc); d = cscale(s2f(v.w), sc); }
       c[8 * w + 0] = a.x; c[8 * w + 1] = a.y; c[8 * w + 2] = b.x; c[8 * w + 3] = b.y;
       c[8 * w + 4] = cc.x; c[8 * w + 5] = cc.y; c[8 * w + 6] = d.x; c[8 * w + 7] = d.y;
     }
@@ -204,6 +224,7 @@ struct SHopArgs {
   float *dst_norm;
   const void *U;            // sloppy links
   const void *C;            // packed clover blocks
+  const float *Cn;          // their per-site scales (int16 storage)
   float coeff;              // +1/2 (step 1) or -1/2 (step 2)
   int lo, n;                // output sites [lo, lo+n): the odd block (step 1) or even (step 2)
   double *part;             // NRM: one partial sum of |dst|^2 per block
@@ -246,7 +267,7 @@ __device__ __forceinline__ double sum_partials(const double *part, int n) {
 
 // one direction: SIG = -1 forward (1 - gamma_mu), +1 backward (1 + gamma_mu); as hop_dir
 // in yg_dirac_impl.cuh (dirac.cpp:258-697)
-template <int P, int K, int MU, int SIG>
+template <int P, int LP, int K, int MU, int SIG>
 __device__ __forceinline__ void shop_dir(float2 (&acc)[12], const SHopArgs &a, int nid, int lid, int lt) {
   const Geom &g = a.g;
   float2 p[12];
@@ -274,7 +295,7 @@ __device__ __forceinline__ void shop_dir(float2 (&acc)[12], const SHopArgs &a, i
   int lb = lid >= g.Vh, lh = lid - lb * g.Vh;
   float sgn = (g.bc == YG_BC_ANTIPERIODIC && MU == 0 && lt == 0) ? -1.f : 1.f;
   float2 u[9];
-  link_load<P, K>(u, a.U, lb, lh, g.Vh, MU, sgn);
+  link_load<LP, K>(u, a.U, lb, lh, g.Vh, MU, sgn);
   float2 chi[2][3];
 #pragma unroll
   for (int i = 0; i < 3; i++) {
@@ -333,26 +354,26 @@ __device__ __forceinline__ void site_nbr(SiteNbr &n, const Geom &g, int id) {
 // STEP 1 (odd output):  dst = M_o^-1 (coeff * hop(src))
 // STEP 2 (even output): dst = gamma5 (M_e src2 + coeff * hop(src))
 // returns |dst|^2 of the site (before FP16 rounding)
-template <int P, int K, int STEP>
+template <int P, int LP, int CP, int K, int STEP>
 __device__ __forceinline__ float shop_site(const SHopArgs &a, int id, const SiteNbr &n) {
   const Geom &g = a.g;
   const int T = g.dim[0], t0 = n.c[0];
   float2 acc[12];
 #pragma unroll
   for (int k = 0; k < 12; k++) acc[k] = make_float2(0.f, 0.f);
-  shop_dir<P, K, 0, -1>(acc, a, n.f[0], id, t0);
-  shop_dir<P, K, 0, +1>(acc, a, n.b[0], n.b[0], t0 == 0 ? T - 1 : t0 - 1);
-  shop_dir<P, K, 1, -1>(acc, a, n.f[1], id, t0);
-  shop_dir<P, K, 1, +1>(acc, a, n.b[1], n.b[1], t0);
-  shop_dir<P, K, 2, -1>(acc, a, n.f[2], id, t0);
-  shop_dir<P, K, 2, +1>(acc, a, n.b[2], n.b[2], t0);
-  shop_dir<P, K, 3, -1>(acc, a, n.f[3], id, t0);
-  shop_dir<P, K, 3, +1>(acc, a, n.b[3], n.b[3], t0);
+  shop_dir<P, LP, K, 0, -1>(acc, a, n.f[0], id, t0);
+  shop_dir<P, LP, K, 0, +1>(acc, a, n.b[0], n.b[0], t0 == 0 ? T - 1 : t0 - 1);
+  shop_dir<P, LP, K, 1, -1>(acc, a, n.f[1], id, t0);
+  shop_dir<P, LP, K, 1, +1>(acc, a, n.b[1], n.b[1], t0);
+  shop_dir<P, LP, K, 2, -1>(acc, a, n.f[2], id, t0);
+  shop_dir<P, LP, K, 2, +1>(acc, a, n.b[2], n.b[2], t0);
+  shop_dir<P, LP, K, 3, -1>(acc, a, n.f[3], id, t0);
+  shop_dir<P, LP, K, 3, +1>(acc, a, n.b[3], n.b[3], t0);
   int blk = id >= g.Vh, h = id - blk * g.Vh;
   float2 out[12];
   bool bnd = spinor_zeroed(g, t0);
   float cl[72];
-  cload<P>(cl, a.C, blk, h, g.Vh);
+  cload<CP>(cl, a.C, a.Cn, blk, h, g.Vh);
   if (STEP == 1) {
 #pragma unroll
     for (int k = 0; k < 12; k++) acc[k] = cscale(acc[k], a.coeff);
@@ -380,14 +401,14 @@ __device__ __forceinline__ float shop_site(const SHopArgs &a, int id, const Site
 // NRM = 1 (first Hphi of a CG iteration, t = Hphi p): also the per-block partials of
 // <p, A p> = |t|^2 (Hphi is Hermitian and A = Hphi^2); a grid-stride loop over a grid of
 // resident blocks keeps the number of partials small
-template <int P, int K, int STEP, int NRM>
+template <int P, int LP, int CP, int K, int STEP, int NRM>
 __global__ void __launch_bounds__(128) k_shop(SHopArgs a) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (!NRM) {
     SiteNbr n;
     if (t < a.n) site_nbr(n, a.g, a.lo + t);
     griddep_wait();
-    if (t < a.n) shop_site<P, K, STEP>(a, a.lo + t, n);
+    if (t < a.n) shop_site<P, LP, CP, K, STEP>(a, a.lo + t, n);
     griddep_launch();
     return;
   }
@@ -396,7 +417,7 @@ __global__ void __launch_bounds__(128) k_shop(SHopArgs a) {
   for (; t < a.n; t += gridDim.x * blockDim.x) {
     SiteNbr n;
     site_nbr(n, a.g, a.lo + t);
-    n2 += (double)shop_site<P, K, STEP>(a, a.lo + t, n);
+    n2 += (double)shop_site<P, LP, CP, K, STEP>(a, a.lo + t, n);
   }
   n2 = block_total(n2);
   if (threadIdx.x == 0) a.part[blockIdx.x] = n2;
@@ -404,30 +425,31 @@ __global__ void __launch_bounds__(128) k_shop(SHopArgs a) {
 }
 
 // ------------------------------------------------------------------ builds (once per gauge field / mass)
-template <int P>
+template <int LP>
 __device__ __forceinline__ void lstore(void *base, long i, double2 v) {
-  if (P == 32) reinterpret_cast<float2 *>(base)[i] = make_float2((float)v.x, (float)v.y);
-  else reinterpret_cast<unsigned *>(base)[i] = f2h(make_float2((float)v.x, (float)v.y));
+  if (LP == ST_F32) reinterpret_cast<float2 *>(base)[i] = make_float2((float)v.x, (float)v.y);
+  else if (LP == ST_F16) reinterpret_cast<unsigned *>(base)[i] = f2h(make_float2((float)v.x, (float)v.y));
+  else reinterpret_cast<unsigned *>(base)[i] = f2s((float)v.x, (float)v.y);
 }
 
 // links: the first K complex entries (row-major) of each FP64 represented link
-template <int P, int K>
+template <int LP, int K>
 __global__ void k_pack_links(void *dst, const double2 *links, Geom g) {
   long r = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (r >= 4L * g.V) return;
   int id = (int)(r >> 2), mu = (int)(r & 3);
   int blk = id >= g.Vh, h = id - blk * g.Vh;
   for (int k = 0; k < K; k++)
-    lstore<P>(dst, ((long)(blk * 4 + mu) * K + k) * g.Vh + h, links[fidx(g, id, mu * 9 + k, 36)]);
+    lstore<LP>(dst, ((long)(blk * 4 + mu) * K + k) * g.Vh + h, links[fidx(g, id, mu * 9 + k, 36)]);
 }
 
-template <int P>
-__device__ __forceinline__ void cstore(void *base, const float (&c)[72], int blk, int h, int Vh) {
-  if (P == 32) {
+template <int CP>
+__device__ __forceinline__ void cstore(void *base, float *cn, const float (&c)[72], int blk, int h, int Vh) {
+  if (CP == ST_F32) {
     float4 *f = reinterpret_cast<float4 *>(base);
     for (int w = 0; w < 18; w++)
       f[(long)(blk * 18 + w) * Vh + h] = make_float4(c[4 * w], c[4 * w + 1], c[4 * w + 2], c[4 * w + 3]);
-  } else {
+  } else if (CP == ST_F16) {
     uint4 *f = reinterpret_cast<uint4 *>(base);
     for (int w = 0; w < 9; w++) {
       uint4 v;
@@ -437,6 +459,20 @@ __device__ __forceinline__ void cstore(void *base, const float (&c)[72], int blk
       v.w = f2h(make_float2(c[8 * w + 6], c[8 * w + 7]));
       f[(long)(blk * 9 + w) * Vh + h] = v;
     }
+  } else {
+    float m = 0.f;
+    for (int k = 0; k < 72; k++) m = fmaxf(m, fabsf(c[k]));
+    const float inv = m > 0.f ? 1.f / m : 0.f;
+    uint4 *f = reinterpret_cast<uint4 *>(base);
+    for (int w = 0; w < 9; w++) {
+      uint4 v;
+      v.x = f2s(c[8 * w] * inv, c[8 * w + 1] * inv);
+      v.y = f2s(c[8 * w + 2] * inv, c[8 * w + 3] * inv);
+      v.z = f2s(c[8 * w + 4] * inv, c[8 * w + 5] * inv);
+      v.w = f2s(c[8 * w + 6] * inv, c[8 * w + 7] * inv);
+      f[(long)(blk * 9 + w) * Vh + h] = v;
+    }
+    cn[(long)blk * Vh + h] = m;
   }
 }
 
@@ -453,8 +489,9 @@ __device__ __forceinline__ void pack_block(float *c, const double2 (&M)[36]) {
 
 // even sites: M_e = diag + [[A0,A1],[A1^dag,-A0]] (+) [[A2,A3],[A3^dag,-A2]] (clover_kernel,
 // dirac.cpp:25-107) with diag = 4+m+cf(t); without a clover term, diag = (4+m)^2 alone
-template <int P>
-__global__ void k_pack_clover_even(void *dst, const double2 *cl, Geom g, double diag, double cfm1, int clover) {
+template <int CP>
+__global__ void k_pack_clover_even(void *dst, float *cn, const double2 *cl, Geom g, double diag, double cfm1,
+                                   int clover) {
   int h = blockIdx.x * blockDim.x + threadIdx.x;
   if (h >= g.Vh) return;
   int id = h;
@@ -480,12 +517,12 @@ __global__ void k_pack_clover_even(void *dst, const double2 *cl, Geom g, double 
     }
     pack_block(c + 36 * b, M);
   }
-  cstore<P>(dst, c, 0, h, g.Vh);
+  cstore<CP>(dst, cn, c, 0, h, g.Vh);
 }
 
 // odd sites: the explicit inverse M_o^-1 from the FP64 LDL factors (identity without clover)
-template <int P>
-__global__ void k_pack_clover_odd(void *dst, const double2 *ldl, Geom g, int clover) {
+template <int CP>
+__global__ void k_pack_clover_odd(void *dst, float *cn, const double2 *ldl, Geom g, int clover) {
   int h = blockIdx.x * blockDim.x + threadIdx.x;
   if (h >= g.Vh) return;
   constexpr int N = 6, Pk = 21;
@@ -511,7 +548,7 @@ __global__ void k_pack_clover_odd(void *dst, const double2 *ldl, Geom g, int clo
     }
     pack_block(c + 36 * b, M);
   }
-  cstore<P>(dst, c, 1, h, g.Vh);
+  cstore<CP>(dst, cn, c, 1, h, g.Vh);
 }
 
 // ------------------------------------------------------------------ sloppy vector kernels
@@ -625,18 +662,46 @@ static int sgrid(long n) {
   return (int)(g < cap ? g : cap);
 }
 
-#define YG_SLOPPY_DISPATCH(P_, K_, ...)                                                      \
+// run-time storage formats -> template arguments: SP spinor, SL links, SC clover, SK complex
+// words stored per link.  The combinations built: FP32 throughout; FP32 spinors with int16
+// links (and FP32 or int16 clover); FP16 spinors with FP16 or int16 matrices.
+#define YG_SLOPPY_ONE(P_, L_, C_, ...)                                                        \
+  if (prec_ == P_ && lf_ == L_ && cf_ == C_) {                                               \
+    constexpr int SP = P_, SL = L_, SC = C_;                                                 \
+    if (reals_ == 12) { constexpr int SK = 6; __VA_ARGS__; }                                 \
+    else { constexpr int SK = 9; __VA_ARGS__; }                                              \
+    done_ = true;                                                                            \
+  }
+#define YG_SLOPPY_DISPATCH(PREC, LF, CF, REALS, ...)                                           \
   do {                                                                                       \
-    if (P_ == 32 && K_ == 12) { constexpr int SP = 32, SK = 6; __VA_ARGS__; }                \
-    else if (P_ == 32 && K_ == 18) { constexpr int SP = 32, SK = 9; __VA_ARGS__; }           \
-    else if (P_ == 16 && K_ == 12) { constexpr int SP = 16, SK = 6; __VA_ARGS__; }           \
-    else if (P_ == 16 && K_ == 18) { constexpr int SP = 16, SK = 9; __VA_ARGS__; }           \
-    else throw Error(YG_ERR_ARG, "inner precision must be 32 or 16 and link reals 18 or 12"); \
+    const int prec_ = (PREC), lf_ = (LF), cf_ = (CF), reals_ = (REALS);                      \
+    bool done_ = false;                                                                      \
+    YG_SLOPPY_ONE(32, 32, 32, __VA_ARGS__)                                                   \
+    else YG_SLOPPY_ONE(32, 15, 32, __VA_ARGS__)                                              \
+    else YG_SLOPPY_ONE(32, 15, 15, __VA_ARGS__)                                              \
+    else YG_SLOPPY_ONE(16, 16, 16, __VA_ARGS__)                                              \
+    else YG_SLOPPY_ONE(16, 15, 15, __VA_ARGS__)                                              \
+    if (!done_) throw Error(YG_ERR_ARG, "unsupported combination of inner storage formats");  \
   } while (0)
 
-void ensure_sloppy(Lattice &L, double mass, int prec, int reals) {
+// spinor format only (the inner CG's vector kernels)
+#define YG_SPINOR_DISPATCH(PREC, ...)                                                         \
+  do {                                                                                       \
+    if ((PREC) == 32) { constexpr int SP = 32; __VA_ARGS__; }                                \
+    else if ((PREC) == 16) { constexpr int SP = 16; __VA_ARGS__; }                           \
+    else throw Error(YG_ERR_ARG, "inner precision must be 32 or 16");                         \
+  } while (0)
+
+// 0 (automatic) -> the spinor format; 15 is the int16 fixed-point format
+static int matrix_format(int requested, int prec) { return requested == 0 ? prec : requested; }
+
+void ensure_sloppy(Lattice &L, double mass, int prec, int reals, int lfmt, int cfmt) {
+  lfmt = matrix_format(lfmt, prec);
+  cfmt = matrix_format(cfmt, prec);
   if ((prec != 32 && prec != 16) || (reals != 18 && reals != 12))
     throw Error(YG_ERR_ARG, "inner precision must be 32 or 16 and link reals 18 or 12");
+  for (int f : {lfmt, cfmt})
+    if (f != ST_F32 && f != ST_F16 && f != ST_I16) throw Error(YG_ERR_ARG, "matrix storage must be 32, 16 or 15");
   if (L.d != 3) throw Error(YG_ERR_ARG, "the compressed inner operator exists for d = 3 representations");
   if (reals == 12 && !(L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL))
     throw Error(YG_ERR_ARG, "12-real links need SU(3) fundamental links");
@@ -647,38 +712,44 @@ void ensure_sloppy(Lattice &L, double mass, int prec, int reals) {
     L.sl_scal.alloc(S_WORDS * sizeof(double));
     YG_CUDA(cudaMemsetAsync(L.sl_scal.p, 0, S_WORDS * sizeof(double), L.stream));
   }
-  if (L.sl_valid && L.sl_prec == prec && L.sl_reals == reals && L.sl_mass == mass) return;
+  if (L.sl_valid && L.sl_prec == prec && L.sl_reals == reals && L.sl_lfmt == lfmt && L.sl_cfmt == cfmt &&
+      L.sl_mass == mass)
+    return;
   {
     // resident-grid sizes of the reduction kernels, and room for their partials
     int dev = 0, sms = 0, per_nrm = 0, per_vec = 0;
     YG_CUDA(cudaGetDevice(&dev));
     YG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    YG_SLOPPY_DISPATCH(prec, reals, {
-      YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_nrm, k_shop<SP, SK, 2, 1>, 128, 0));
+    YG_SLOPPY_DISPATCH(prec, lfmt, cfmt, reals, {
+      YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_nrm, k_shop<SP, SL, SC, SK, 2, 1>, 128, 0));
       YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_vec, k_s_cg_update<SP>, 256, 0));
     });
     L.sl_grid_nrm = (int)std::min<long>((long)sms * std::max(per_nrm, 1), nblk(L.Vh, 128));
     L.sl_grid_vec = (int)std::min<long>((long)sms * std::max(per_vec, 1), nblk(L.Vh, 256));
     L.sl_part.alloc(sizeof(double) * (size_t)(L.sl_grid_nrm + L.sl_grid_vec));
   }
-  size_t esz = prec == 32 ? 4 : 2;
-  int K = reals / 2;
-  L.sl_links.alloc(esz * 2 * K * 4 * (size_t)L.V);
-  L.sl_clover.alloc(esz * 72 * (size_t)L.V);
+  const int K = reals / 2;
+  L.sl_links.alloc((lfmt == ST_F32 ? 8 : 4) * (size_t)K * 4 * L.V);
+  L.sl_clover.alloc((cfmt == ST_F32 ? 4 : 2) * 72 * (size_t)L.V);
+  L.sl_cnorm.alloc(sizeof(float) * (size_t)L.V);
   if (L.p.clover) ensure_ldl(L, 4.0 + mass);
   int clover = L.p.clover ? 1 : 0;
   double diag = clover ? 4.0 + mass : (4.0 + mass) * (4.0 + mass);
-  YG_SLOPPY_DISPATCH(prec, reals, {
-    k_pack_links<SP, SK><<<nblk(4 * L.V, 128), 128, 0, L.stream>>>(L.sl_links.p, L.links.as<double2>(), L.g);
+  YG_SLOPPY_DISPATCH(prec, lfmt, cfmt, reals, {
+    k_pack_links<SL, SK><<<nblk(4 * L.V, 128), 128, 0, L.stream>>>(L.sl_links.p, L.links.as<double2>(), L.g);
     YG_LAUNCHED();
-    k_pack_clover_even<SP><<<nblk(L.Vh, 64), 64, 0, L.stream>>>(L.sl_clover.p, L.clover.as<double2>(), L.g, diag,
-                                                                 L.p.cf - 1.0, clover);
+    k_pack_clover_even<SC><<<nblk(L.Vh, 64), 64, 0, L.stream>>>(L.sl_clover.p, L.sl_cnorm.as<float>(),
+                                                                 L.clover.as<double2>(), L.g, diag, L.p.cf - 1.0,
+                                                                 clover);
     YG_LAUNCHED();
-    k_pack_clover_odd<SP><<<nblk(L.Vh, 64), 64, 0, L.stream>>>(L.sl_clover.p, L.ldl.as<double2>(), L.g, clover);
+    k_pack_clover_odd<SC><<<nblk(L.Vh, 64), 64, 0, L.stream>>>(L.sl_clover.p, L.sl_cnorm.as<float>(),
+                                                                L.ldl.as<double2>(), L.g, clover);
     YG_LAUNCHED();
   });
   L.sl_prec = prec;
   L.sl_reals = reals;
+  L.sl_lfmt = lfmt;
+  L.sl_cfmt = cfmt;
   L.sl_mass = mass;
   L.sl_valid = true;
 }
@@ -712,6 +783,7 @@ static void sloppy_hphi(Lattice &L, SField dst, SField src, SField tmp, bool nrm
   a.g = L.g;
   a.U = L.sl_links.p;
   a.C = L.sl_clover.p;
+  a.Cn = L.sl_cnorm.as<float>();
   a.src = src.data; a.src_norm = src.norm;
   a.dst = tmp.data; a.dst_norm = tmp.norm;
   a.coeff = 0.5f;
@@ -723,11 +795,11 @@ static void sloppy_hphi(Lattice &L, SField dst, SField src, SField tmp, bool nrm
   b.coeff = -0.5f;
   b.lo = 0;
   b.part = part_pq(L);
-  YG_SLOPPY_DISPATCH(L.sl_prec, L.sl_reals, {
-    launch_pdl(k_shop<SP, SK, 1, 0>, nblk(a.n, 128), 128, L.stream, a);
+  YG_SLOPPY_DISPATCH(L.sl_prec, L.sl_lfmt, L.sl_cfmt, L.sl_reals, {
+    launch_pdl(k_shop<SP, SL, SC, SK, 1, 0>, nblk(a.n, 128), 128, L.stream, a);
     YG_LAUNCHED();
-    if (nrm) launch_pdl(k_shop<SP, SK, 2, 1>, L.sl_grid_nrm, 128, L.stream, b);
-    else launch_pdl(k_shop<SP, SK, 2, 0>, nblk(b.n, 128), 128, L.stream, b);
+    if (nrm) launch_pdl(k_shop<SP, SL, SC, SK, 2, 1>, L.sl_grid_nrm, 128, L.stream, b);
+    else launch_pdl(k_shop<SP, SL, SC, SK, 2, 0>, nblk(b.n, 128), 128, L.stream, b);
     YG_LAUNCHED();
   });
   L.mvm += 2;
@@ -735,7 +807,7 @@ static void sloppy_hphi(Lattice &L, SField dst, SField src, SField tmp, bool nrm
 
 // par = iteration parity (selects the |r|^2 slot)
 static void sloppy_cg_update(Lattice &L, float *x, float *r, SField p, SField q, int par) {
-  YG_SLOPPY_DISPATCH(L.sl_prec, 18, {
+  YG_SPINOR_DISPATCH(L.sl_prec, {
     launch_pdl(k_s_cg_update<SP>, L.sl_grid_vec, 256, L.stream, (float2 *)x, (float2 *)r, p.data, p.norm, q.data,
                q.norm, dscal(L), part_pq(L), L.sl_grid_nrm, part_r(L), par, (int)L.Vh);
     YG_LAUNCHED();
@@ -743,7 +815,7 @@ static void sloppy_cg_update(Lattice &L, float *x, float *r, SField p, SField q,
 }
 
 static void sloppy_xpay(Lattice &L, SField p, const float *r, int par, double *hist, unsigned long long iter) {
-  YG_SLOPPY_DISPATCH(L.sl_prec, 18, {
+  YG_SPINOR_DISPATCH(L.sl_prec, {
     launch_pdl(k_s_xpay<SP>, L.sl_grid_vec, 256, L.stream, p.data, p.norm, dscal(L), part_r(L), L.sl_grid_vec, par,
                hist, hist_seq(L), iter, (const float2 *)r, (int)L.Vh);
     YG_LAUNCHED();
@@ -768,7 +840,7 @@ static void wait_iteration(Lattice &L, unsigned long long iter) {
 }
 
 static void sloppy_from_d(Lattice &L, SField dst, const double *src) {
-  YG_SLOPPY_DISPATCH(L.sl_prec, 18, {
+  YG_SPINOR_DISPATCH(L.sl_prec, {
     k_s_from_d<SP><<<sgrid(L.Vh), 256, 0, L.stream>>>(dst.data, dst.norm, (const double2 *)src, (int)L.Vh);
     YG_LAUNCHED();
   });
@@ -787,8 +859,8 @@ static void set_scalar(Lattice &L, int i, double v) {
 // iterated |r| fell below delta times its value at the last update, r is replaced by it
 // and the search direction is kept.  The solve stops only on the true FP64 squared
 // residual |b - A x|^2 < prec |b|^2; a stall falls back to the FP64 CG.
-int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, double delta, double *x, double *b,
-                    yg_solve_stats *st);
+int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int lfmt, int cfmt, double delta,
+                    double *x, double *b, yg_solve_stats *st);
 
 }  // namespace yg
 
@@ -796,12 +868,12 @@ namespace yg {
 
 int cg(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
 
-int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, double delta, double *x, double *b,
-                    yg_solve_stats *st) {
+int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int lfmt, int cfmt, double delta,
+                    double *x, double *b, yg_solve_stats *st) {
   auto t0 = std::chrono::steady_clock::now();
   if (par.op != YG_OP_HPHI_SQ) throw Error(YG_ERR_ARG, "cg_mixed solves Hphi_sq systems");
   if (!(delta > 0.0 && delta < 1.0)) throw Error(YG_ERR_ARG, "reliable-update delta must lie in (0,1)");
-  ensure_sloppy(L, par.mass, prec, reals);
+  ensure_sloppy(L, par.mass, prec, reals, lfmt, cfmt);
   long lo, n;
   L.view_range(YG_VIEW_DEFAULT, lo, n);
   const long cnt = n * 4L * L.d;
