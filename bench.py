@@ -4,8 +4,8 @@ Workload (defaults): 32^4 SU(3) fundamental, even-odd preconditioned Wilson-clov
 m = -0.75, csw = 1.0, periodic space / antiperiodic time.  One step = one solve of
 Hphi_sq x = b (the D^dag D system of cg_inverter, cg.cpp:132-202) to a TRUE FP64
 relative residual of 1e-12 (prec = 1e-24 in the reference's squared convention), with
-the mixed-precision solver (compressed FP32 inner operator with 12-real links, FP64
-reliable updates and stopping test).
+the mixed-precision solver (FP32 arithmetic on FP16 spinors with per-site norms, FP32
+12-real links and clover blocks; FP64 reliable updates and stopping test).
 
 Reported beside it: the same solve with the plain FP64 CG (the reference's algorithm on
 the GPU), the FP64 Dslash (Dphi_oe) bandwidth against the measured HBM peak, the same
@@ -55,10 +55,10 @@ def parse():
     ap.add_argument("--seed", type=int, default=20241203)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dslash-iters", type=int, default=50)
-    ap.add_argument("--inner", default="f32-l12", choices=list(INNER),
+    ap.add_argument("--inner", default="f16spinor-l12", choices=list(INNER),
                     help="inner operator of the mixed solver: generic FP32, or the compressed d = 3 "
                          "operator with FP32/FP16 spinors and 18/12-real links")
-    ap.add_argument("--delta", type=float, default=0.003, help="reliable-update threshold")
+    ap.add_argument("--delta", type=float, default=0.1, help="reliable-update threshold")
     ap.add_argument("--variants", action="store_true", help="also time every inner operator once")
     ap.add_argument("--therm-trajectories", type=int, default=THERM["trajectories"],
                     help="HMC trajectories of the field generation (fewer only to profile a few launches)")
@@ -74,7 +74,8 @@ def parse():
 # (spinor bits, link reals) = the compressed d = 3 operator
 INNER = {"generic-f32": (0, 18, 0, 0), "f32-l18": (32, 18, 0, 0), "f32-l12": (32, 12, 0, 0),
          "f16-l18": (16, 18, 0, 0), "f16-l12": (16, 12, 0, 0),
-         "f32-i16links-l12": (32, 12, 15, 32), "f32-i16-l12": (32, 12, 15, 15), "f16-i16-l12": (16, 12, 15, 15)}
+         "f32-i16links-l12": (32, 12, 15, 32), "f32-i16-l12": (32, 12, 15, 15), "f16-i16-l12": (16, 12, 15, 15),
+         "f16spinor-l12": (16, 12, 32, 32)}
 
 
 DTYPE = {"generic-f32": "f32 inner / f64 reliable updates and residual",
@@ -84,7 +85,8 @@ DTYPE = {"generic-f32": "f32 inner / f64 reliable updates and residual",
          "f16-l12": "f32 inner arithmetic on f16 storage (12-real links) / f64 reliable updates and residual",
          "f32-i16links-l12": "f32 inner (int16 12-real links) / f64 reliable updates and residual",
          "f32-i16-l12": "f32 inner (int16 12-real links and clover) / f64 reliable updates and residual",
-         "f16-i16-l12": "f32 inner arithmetic on f16 spinors, int16 links and clover / f64 reliable updates and residual"}
+         "f16-i16-l12": "f32 inner arithmetic on f16 spinors, int16 links and clover / f64 reliable updates and residual",
+         "f16spinor-l12": "f32 inner arithmetic on f16 spinors, f32 12-real links and clover / f64 reliable updates and residual"}
 
 
 def solve_mixed(lat, x, b, inner, delta):

@@ -177,8 +177,9 @@ int yg_rational_calc(yg_lattice *lat, const yg_inv_par *par, double a0, int orde
                      const double *residues, double *x, double *b, int *iters);
 /* No reference counterpart: CG on the same operator with FP32 inner iterations and FP64
  * reliable updates; stops on the TRUE FP64 squared residual |b-Ax|^2 < prec*|b|^2.  Uses
- * the compressed FP32 inner operator (12-real links for SU(3) fundamental) for d = 3 and
- * the generic FP32 operator otherwise. */
+ * the compressed inner operator for d = 3 (FP16 spinors with per-site norms, FP32 links --
+ * 12-real for SU(3) fundamental -- and clover blocks, delta 0.1) and the generic FP32
+ * operator otherwise. */
 int yg_cg_mixed(yg_lattice *lat, const yg_inv_par *par, double *x, double *b, yg_solve_stats *stats);
 
 /* No reference counterpart: nrhs cg_inverter solves (cg.cpp:132-202) of the same operator
@@ -197,7 +198,7 @@ int yg_cg_inverter_multi(yg_lattice *lat, const yg_inv_par *par, int nrhs, doubl
  *   delta            reliable update when |r| falls below delta * |r| at the last update
  *   link_storage,    storage of the inner operator's links and clover blocks; the combinations
  *   clover_storage   built are all-FP32, FP32 spinors with int16 links (FP32 or int16 clover),
- *                    and FP16 spinors with FP16 or int16 matrices
+ *                    and FP16 spinors with FP32, FP16 or int16 matrices
  * The compressed inner operator exists for d = 3 representations with even-odd
  * preconditioning; the stopping test is the true FP64 residual, as for yg_cg_mixed. */
 typedef struct {

@@ -31,7 +31,7 @@ CASES = [("su3_fund_ap", 32, 12, 0, 0), ("su3_fund_ap", 32, 18, 0, 0), ("su3_fun
          # int16 fixed-point links / clover blocks (storage 15)
          ("su3_fund_ap", 32, 12, 15, 32), ("su3_fund_ap", 32, 12, 15, 15), ("su3_fund_open", 32, 12, 15, 15),
          ("su3_fund_sf", 32, 18, 15, 15), ("su3_fund_ap_nocl", 32, 12, 15, 15), ("su2_adj_ap", 32, 18, 15, 15),
-         ("su3_fund_ap", 16, 12, 15, 15)]
+         ("su3_fund_ap", 16, 12, 15, 15), ("su3_fund_ap", 16, 12, 32, 32)]
 
 
 @pytest.mark.parametrize("name,inner,reals,lfmt,cfmt", CASES)

@@ -268,10 +268,13 @@ int yg_cg_mixed(yg_lattice *l, const yg_inv_par *p, double *x, double *b, yg_sol
   return guard_status([&] {
     check_par(p); need(x, "x"); need(b, "b");
     yg::Lattice &L = lat(l);
-    // the compressed FP32 inner operator where it exists (d = 3, even-odd), else the generic one
+    // the compressed inner operator where it exists (d = 3, even-odd): FP16 spinors with
+    // per-site norms, FP32 links (12-real for SU(3) fundamental) and clover blocks, delta
+    // 0.1 -- 16-bit spinors only add noise to each inner step, while 16-bit matrices would
+    // change the operator itself; else the generic FP32 operator
     if (L.d == 3 && L.p.eo) {
       int reals = (L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL) ? 12 : 18;
-      return yg::cg_mixed_sloppy(L, *p, 32, reals, 0, 0, 0.003, x, b, st);
+      return yg::cg_mixed_sloppy(L, *p, 16, reals, 32, 32, 0.1, x, b, st);
     }
     return yg::cg_mixed(L, *p, x, b, st);
   });

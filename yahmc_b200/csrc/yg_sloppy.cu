@@ -664,7 +664,7 @@ static int sgrid(long n) {
 
 // run-time storage formats -> template arguments: SP spinor, SL links, SC clover, SK complex
 // words stored per link.  The combinations built: FP32 throughout; FP32 spinors with int16
-// links (and FP32 or int16 clover); FP16 spinors with FP16 or int16 matrices.
+// links (and FP32 or int16 clover); FP16 spinors with FP32, FP16 or int16 matrices.
 #define YG_SLOPPY_ONE(P_, L_, C_, ...)                                                        \
   if (prec_ == P_ && lf_ == L_ && cf_ == C_) {                                               \
     constexpr int SP = P_, SL = L_, SC = C_;                                                 \
@@ -680,6 +680,7 @@ static int sgrid(long n) {
     else YG_SLOPPY_ONE(32, 15, 32, __VA_ARGS__)                                              \
     else YG_SLOPPY_ONE(32, 15, 15, __VA_ARGS__)                                              \
     else YG_SLOPPY_ONE(16, 16, 16, __VA_ARGS__)                                              \
+    else YG_SLOPPY_ONE(16, 32, 32, __VA_ARGS__)                                              \
     else YG_SLOPPY_ONE(16, 15, 15, __VA_ARGS__)                                              \
     if (!done_) throw Error(YG_ERR_ARG, "unsupported combination of inner storage formats");  \
   } while (0)
