@@ -191,6 +191,14 @@ int yg_cg_mixed(yg_lattice *lat, const yg_inv_par *par, double *x, double *b, yg
 int yg_cg_inverter_multi(yg_lattice *lat, const yg_inv_par *par, int nrhs, double *const *xs, double *const *bs,
                          int *iters);
 
+/* No reference counterpart: nrhs solves of Hphi_sq with FP32 inner iterations (the compressed
+ * operator with FP32 links and clover blocks) and FP64 reliable updates, advanced together;
+ * every system stops on its own TRUE FP64 residual |b_i - A x_i|^2 < prec |b_i|^2 (a
+ * system that stalls continues with the batched FP64 CG).  stats[i] per system.
+ * 1 <= nrhs <= 16, d = 3, even-odd; xs[i] on entry is the initial guess. */
+int yg_cg_mixed_multi(yg_lattice *lat, const yg_inv_par *par, int nrhs, double *const *xs, double *const *bs,
+                      double delta, yg_solve_stats *stats);
+
 /* No reference counterpart: options of the mixed-precision solver.
  *   inner_precision  32 (FP32 storage) or 16 (FP16 storage with per-site norms), FP32
  *                    arithmetic; 0 selects the generic FP32 operator of yg_cg_mixed (any d)

@@ -81,3 +81,29 @@ def test_multi_argument_errors():
     b2 = lat2.field(source(O2, rng2))
     with pytest.raises(YGError):
         lat2.cg_inverter_multi("Hphi_sq", -0.4, 1e-20, [lat2.field()], [b2])
+
+
+@pytest.mark.parametrize("name", ["su3_fund_ap", "su3_fund_open", "su3_fund_ap_nocl", "su2_adj_ap"])
+def test_mixed_multi_true_residuals(name):
+    """The batched mixed CG: every system meets its true FP64 residual, without fallback,
+    in about the single-system FP64 iteration count."""
+    dims = (8, 8, 8, 8) if name.startswith("su3") else (4, 6, 4, 8)
+    lat, O, rng = make_pair(name, dims, seed=55)
+    nb, mass = 6, -0.4
+    srcs = [source(O, rng) for _ in range(nb)]
+    bs = [lat.field(s) for s in srcs]
+    xs = [lat.field() for _ in range(nb)]
+    lat.upload(xs[1], 0.01 * source(O, rng))
+    x64 = lat.field()
+    it64 = lat.cg_inverter("Hphi_sq", mass, 1e-24, x64, bs[0])
+    for prec in (1e-24, 1e-28):
+        for x in xs:
+            lat.spinor_zero(x)
+        sts = lat.cg_mixed_multi("Hphi_sq", mass, prec, xs, bs, delta=0.1)
+        assert lat.last_status == 0
+        for i in range(nb):
+            assert sts[i]["fallback"] == 0, sts[i]
+            assert sts[i]["true_residual"] < prec
+            assert _true_residual(lat, "Hphi_sq", mass, xs[i], bs[i]) < prec
+        if prec == 1e-24:
+            assert sts[0]["iterations"] <= 1.5 * it64 + 10, (sts[0], it64)

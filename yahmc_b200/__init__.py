@@ -103,6 +103,7 @@ _SIGNATURES = {
     "yg_cg_mixed": [_P, ctypes.POINTER(InvPar), _P, _P, ctypes.POINTER(SolveStats)],
     "yg_cg_mixed_opts": [_P, ctypes.POINTER(InvPar), ctypes.POINTER(MixedOpts), _P, _P, ctypes.POINTER(SolveStats)],
     "yg_cg_inverter_multi": [_P, _P, _I, _P, _P, _P],
+    "yg_cg_mixed_multi": [_P, _P, _I, _P, _P, _D, _P],
     "yg_momenta_upload": [_P, _P], "yg_momenta_download": [_P, _P], "yg_momenta_zero": [_P],
     "yg_clover_force_download": [_P, _P], "yg_begin_fermion_force": [_P], "yg_end_fermion_force": [_P, _D],
     "yg_wilson_fermion_force": [_P, _D, _D, _D, _P, _P], "yg_wilson_fermion_force_q": [_P, _D, _D, _D, _P],
@@ -380,6 +381,22 @@ class Lattice:
         if rc not in (0, 4):
             self._check(rc)
         return list(its)
+
+    def cg_mixed_multi(self, op, mass, prec, xs, bs, delta=0.1, log=0, maxiter=0):
+        """len(xs) mixed-precision solves advanced together; one stats dict per system"""
+        n = len(xs)
+        if n != len(bs):
+            raise ValueError("xs and bs differ in length")
+        par = self._par(op, mass, prec, log, maxiter)
+        px = (ctypes.c_void_p * n)(*[x.ptr for x in xs])
+        pb = (ctypes.c_void_p * n)(*[b.ptr for b in bs])
+        sts = (SolveStats * n)()
+        rc = self.lib.yg_cg_mixed_multi(self.h, ctypes.byref(par), n, px, pb, float(delta), sts)
+        self.last_status = rc
+        if rc not in (0, 4, 5):
+            self._check(rc)
+        return [{"status": rc, "iterations": st.iterations, "reliable_updates": st.reliable_updates,
+                 "fallback": st.fallback, "true_residual": st.true_residual, "seconds": st.seconds} for st in sts]
 
     def cg_mixed(self, op, mass, prec, x, b, log=0, maxiter=0, inner_precision=None, link_reals=18, delta=0.1,
                  link_storage=0, clover_storage=0):

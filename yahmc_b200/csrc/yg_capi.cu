@@ -264,6 +264,14 @@ int yg_cg_inverter_multi(yg_lattice *l, const yg_inv_par *p, int nrhs, double *c
     return yg::cg_multi(lat(l), *p, nrhs, xs, bs, iters);
   });
 }
+int yg_cg_mixed_multi(yg_lattice *l, const yg_inv_par *p, int nrhs, double *const *xs, double *const *bs,
+                      double delta, yg_solve_stats *stats) {
+  return guard_status([&] {
+    check_par(p); need(xs, "xs"); need(bs, "bs"); need(stats, "stats");
+    for (int i = 0; i < nrhs; i++) { need(xs[i], "xs[i]"); need(bs[i], "bs[i]"); }
+    return yg::cg_mixed_multi(lat(l), *p, nrhs, xs, bs, delta, stats);
+  });
+}
 int yg_cg_mixed(yg_lattice *l, const yg_inv_par *p, double *x, double *b, yg_solve_stats *st) {
   return guard_status([&] {
     check_par(p); need(x, "x"); need(b, "b");

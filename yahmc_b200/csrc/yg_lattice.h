@@ -203,5 +203,10 @@ void gauge_restore(Lattice &L);
 
 // several cg_inverter solves sharing every operator application (yg_multi.cu)
 int cg_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, double *const *bs, int *iters);
+// the same systems with FP32 inner iterations and FP64 reliable updates (yg_multi.cu)
+int cg_mixed_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, double *const *bs, double delta,
+                   yg_solve_stats *stats);
+// the compressed inner operator's matrices (yg_sloppy.cu); formats 32 / 16 / 15, 0 = as prec
+void ensure_sloppy(Lattice &L, double mass, int prec, int reals, int lfmt, int cfmt);
 
 }  // namespace yg

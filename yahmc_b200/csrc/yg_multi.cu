@@ -10,6 +10,8 @@
 // threads).  Every system keeps the reference's CG recurrence, stopping rule and iteration
 // count; a converged system stops being updated.
 #include <algorithm>
+#include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <vector>
 #include "yg_dirac_impl.cuh"
@@ -572,6 +574,494 @@ int cg_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, dou
     throw;
   }
   for (double2 *b : bufs) cudaFree(b);
+  return status;
+}
+
+// ==================================================================== mixed precision
+// The batched CG with FP32 inner iterations: FP32 batched fields (float2 words in the
+// batched layout), the compressed operator's FP32 matrices (12- or 18-real links, packed
+// Hermitian clover blocks M_e / M_o^-1, built by ensure_sloppy) staged per block of sites
+// in shared memory, FP64 reliable updates through the batched FP64 operator.
+
+struct MultiFHopArgs {
+  Geom g;
+  const float2 *src;      // batched FP32 hop input
+  const float2 *src2;     // STEP 2: batched psi_e
+  float2 *dst;
+  const float2 *U;        // FP32 links, K complex words per link
+  const float4 *C;        // FP32 packed clover blocks, 18 float4 per site
+  float coeff;
+  int lo, n, nb, sites;
+};
+
+// y = M x for one packed Hermitian 6x6 block (6 diagonal reals, then the lower triangle)
+__device__ __forceinline__ void herm6(float2 (&y)[6], const float *c, const float2 (&x)[6]) {
+#pragma unroll
+  for (int r = 0; r < 6; r++) y[r] = cscale(x[r], c[r]);
+  int k = 6;
+#pragma unroll
+  for (int r = 1; r < 6; r++)
+#pragma unroll
+    for (int q = 0; q < r; q++, k += 2) {
+      const float2 m = make_float2(c[k], c[k + 1]);
+      cfma(y[r], m, x[q]);
+      cfmac(y[q], m, x[r]);
+    }
+}
+
+template <int MU, int SIG>
+__device__ __forceinline__ void fhop_dir(float2 (&acc)[12], const float2 *src, const float2 *Ls, const Geom &g,
+                                         int nid, int S, int j, int nb, int i) {
+  float2 h[2][3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const float2 p0 = __ldg(src + bidx(g, nid, 0 * 3 + c, 12, nb, i));
+    const float2 p1 = __ldg(src + bidx(g, nid, 1 * 3 + c, 12, nb, i));
+    const float2 p2 = __ldg(src + bidx(g, nid, 2 * 3 + c, 12, nb, i));
+    const float2 p3 = __ldg(src + bidx(g, nid, 3 * 3 + c, 12, nb, i));
+    if (MU == 0) {
+      h[0][c] = SIG < 0 ? cadd(p0, p2) : csub(p0, p2);
+      h[1][c] = SIG < 0 ? cadd(p1, p3) : csub(p1, p3);
+    } else if (MU == 1) {
+      h[0][c] = SIG < 0 ? cadd(p0, ctimesi(p3)) : csub(p0, ctimesi(p3));
+      h[1][c] = SIG < 0 ? cadd(p1, ctimesi(p2)) : csub(p1, ctimesi(p2));
+    } else if (MU == 2) {
+      h[0][c] = SIG < 0 ? cadd(p0, p3) : csub(p0, p3);
+      h[1][c] = SIG < 0 ? csub(p1, p2) : cadd(p1, p2);
+    } else {
+      h[0][c] = SIG < 0 ? cadd(p0, ctimesi(p2)) : csub(p0, ctimesi(p2));
+      h[1][c] = SIG < 0 ? csub(p1, ctimesi(p3)) : cadd(p1, ctimesi(p3));
+    }
+  }
+  const float2 *Lp = Ls + (SIG < 0 ? MU : 4 + MU) * 9 * S + j;
+  float2 chi[2][3];
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    float2 s0 = make_float2(0.f, 0.f), s1 = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      if (SIG > 0) {
+        const float2 u = Lp[(q * 3 + r) * S];
+        cfmac(s0, u, h[0][q]);
+        cfmac(s1, u, h[1][q]);
+      } else {
+        const float2 u = Lp[(r * 3 + q) * S];
+        cfma(s0, u, h[0][q]);
+        cfma(s1, u, h[1][q]);
+      }
+    }
+    chi[0][r] = s0;
+    chi[1][r] = s1;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    acc[c] = cadd(acc[c], chi[0][c]);
+    acc[3 + c] = cadd(acc[3 + c], chi[1][c]);
+    if (MU == 0) {
+      acc[6 + c] = SIG < 0 ? cadd(acc[6 + c], chi[0][c]) : csub(acc[6 + c], chi[0][c]);
+      acc[9 + c] = SIG < 0 ? cadd(acc[9 + c], chi[1][c]) : csub(acc[9 + c], chi[1][c]);
+    } else if (MU == 1) {
+      acc[6 + c] = SIG < 0 ? cadd(acc[6 + c], ctimesmi(chi[1][c])) : cadd(acc[6 + c], ctimesi(chi[1][c]));
+      acc[9 + c] = SIG < 0 ? cadd(acc[9 + c], ctimesmi(chi[0][c])) : cadd(acc[9 + c], ctimesi(chi[0][c]));
+    } else if (MU == 2) {
+      acc[6 + c] = SIG < 0 ? csub(acc[6 + c], chi[1][c]) : cadd(acc[6 + c], chi[1][c]);
+      acc[9 + c] = SIG < 0 ? cadd(acc[9 + c], chi[0][c]) : csub(acc[9 + c], chi[0][c]);
+    } else {
+      acc[6 + c] = SIG < 0 ? cadd(acc[6 + c], ctimesmi(chi[0][c])) : cadd(acc[6 + c], ctimesi(chi[0][c]));
+      acc[9 + c] = SIG < 0 ? cadd(acc[9 + c], ctimesi(chi[1][c])) : cadd(acc[9 + c], ctimesmi(chi[1][c]));
+    }
+  }
+}
+
+// bytes of shared memory per site: 8 links x 9 float2, 18 float4 clover words, 8 neighbour
+// indices and the site's time coordinate
+constexpr int kFSiteBytes = 8 * 9 * 8 + 18 * 16 + 9 * 4;
+
+// STEP 1 (odd sites): dst = M_o^-1 (coeff hop src); STEP 2 (even sites): dst = gamma5 (M_e
+// src2 + coeff hop src); zero on the spinor boundary slices -- the compressed operator of
+// the single-system mixed CG, for nb systems at once
+template <int K, int STEP>
+__global__ void __launch_bounds__(192) k_fhop_multi(MultiFHopArgs a) {
+  extern __shared__ __align__(16) unsigned char fsm[];
+  const int S = a.sites, nb = a.nb;
+  float2 *Ls = reinterpret_cast<float2 *>(fsm);                       // [8*9][S]
+  float4 *Cs = reinterpret_cast<float4 *>(fsm + 8 * 9 * 8 * S);       // [18][S]
+  int *Ns = reinterpret_cast<int *>(fsm + (8 * 9 * 8 + 18 * 16) * S);  // [8][S]
+  int *Ts = Ns + 8 * S;                                               // [S]
+  const Geom &g = a.g;
+  const int j = threadIdx.x / nb, i = threadIdx.x % nb;
+  const int s0 = blockIdx.x * S;
+  const bool active = s0 + j < a.n;
+  const int id = a.lo + s0 + j;
+  int c[4] = {0, 0, 0, 0};
+  if (active) {
+    coords_of(g, id, c);
+    for (int slot = i; slot < 8; slot += nb) Ns[slot * S + j] = neighbour(g, c, slot & 3, slot < 4 ? +1 : -1);
+    if (i == 0) Ts[j] = c[0];
+  }
+  __syncthreads();
+  const int nsites = min(S, a.n - s0);
+  const int T = g.dim[0];
+  // links: one (site, slot) per thread step; 12-real links get row 2 rebuilt here, with the
+  // antiperiodic sign the stored rows carry applied again
+  for (int q = threadIdx.x; q < 8 * S; q += blockDim.x) {
+    const int slot = q / S, jj = q - slot * S;
+    if (jj >= nsites) continue;
+    const int sid = a.lo + s0 + jj;
+    const int mu = slot & 3;
+    const int lid = slot < 4 ? sid : Ns[slot * S + jj];
+    const int lb = lid >= g.Vh, lh = lid - lb * g.Vh;
+    float2 u[9];
+#pragma unroll
+    for (int k = 0; k < K; k++) u[k] = __ldg(a.U + ((long)(lb * 4 + mu) * K + k) * g.Vh + lh);
+    if (K == 6) {
+      const int tl = slot < 4 ? Ts[jj] : (mu == 0 ? (Ts[jj] == 0 ? T - 1 : Ts[jj] - 1) : Ts[jj]);
+      const float sgn = (g.bc == YG_BC_ANTIPERIODIC && mu == 0 && tl == 0) ? -1.f : 1.f;
+      const float2 a0 = u[0], a1 = u[1], a2 = u[2], b0 = u[3], b1 = u[4], b2 = u[5];
+      u[6] = cscale(cconj(csub(cmul(a1, b2), cmul(a2, b1))), sgn);
+      u[7] = cscale(cconj(csub(cmul(a2, b0), cmul(a0, b2))), sgn);
+      u[8] = cscale(cconj(csub(cmul(a0, b1), cmul(a1, b0))), sgn);
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++) Ls[(slot * 9 + k) * S + jj] = u[k];
+  }
+  for (int q = threadIdx.x; q < 18 * S; q += blockDim.x) {
+    const int w = q / S, jj = q - w * S;
+    if (jj >= nsites) continue;
+    const int sid = a.lo + s0 + jj;
+    const int blk = sid >= g.Vh, h = sid - blk * g.Vh;
+    Cs[w * S + jj] = __ldg(a.C + (long)(blk * 18 + w) * g.Vh + h);
+  }
+  __syncthreads();
+  if (!active) return;
+  float2 acc[12];
+#pragma unroll
+  for (int k = 0; k < 12; k++) acc[k] = make_float2(0.f, 0.f);
+  fhop_dir<0, -1>(acc, a.src, Ls, g, Ns[0 * S + j], S, j, nb, i);
+  fhop_dir<0, +1>(acc, a.src, Ls, g, Ns[4 * S + j], S, j, nb, i);
+  fhop_dir<1, -1>(acc, a.src, Ls, g, Ns[1 * S + j], S, j, nb, i);
+  fhop_dir<1, +1>(acc, a.src, Ls, g, Ns[5 * S + j], S, j, nb, i);
+  fhop_dir<2, -1>(acc, a.src, Ls, g, Ns[2 * S + j], S, j, nb, i);
+  fhop_dir<2, +1>(acc, a.src, Ls, g, Ns[6 * S + j], S, j, nb, i);
+  fhop_dir<3, -1>(acc, a.src, Ls, g, Ns[3 * S + j], S, j, nb, i);
+  fhop_dir<3, +1>(acc, a.src, Ls, g, Ns[7 * S + j], S, j, nb, i);
+  float cl[72];
+#pragma unroll
+  for (int w = 0; w < 18; w++) {
+    const float4 v = Cs[w * S + j];
+    cl[4 * w] = v.x; cl[4 * w + 1] = v.y; cl[4 * w + 2] = v.z; cl[4 * w + 3] = v.w;
+  }
+  float2 in[12];
+  if (STEP == 1) {
+#pragma unroll
+    for (int k = 0; k < 12; k++) in[k] = cscale(acc[k], a.coeff);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 12; k++) in[k] = __ldg(a.src2 + bidx(g, id, k, 12, nb, i));
+  }
+  float2 out[12];
+#pragma unroll
+  for (int b = 0; b < 2; b++) {
+    float2 x[6], y[6];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      x[r] = in[(2 * b) * 3 + r];
+      x[r + 3] = in[(2 * b + 1) * 3 + r];
+    }
+    herm6(y, cl + 36 * b, x);
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      out[(2 * b) * 3 + r] = y[r];
+      out[(2 * b + 1) * 3 + r] = y[r + 3];
+    }
+  }
+  if (STEP == 2) {
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+      out[k] = cadd(out[k], cscale(acc[k], a.coeff));
+      if (k >= 6) out[k] = cscale(out[k], -1.f);              // gamma5
+    }
+  }
+  const bool bnd = spinor_zeroed(g, c[0]);
+#pragma unroll
+  for (int k = 0; k < 12; k++) a.dst[bidx(g, id, k, 12, nb, i)] = bnd ? make_float2(0.f, 0.f) : out[k];
+}
+
+// ---- batched FP32 vectors (float2 words, batched layout, the default view from word 0)
+template <int KIND>    // 0: Re <a_i, b_i> ; 1: |a_i|^2
+__global__ void k_fm_reduce(double *part, const float2 *a, const float2 *b, long cnt, int nb) {
+  const long n = cnt * nb;
+  double acc = 0;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const float2 x = a[e];
+    if (KIND == 0) {
+      const float2 y = b[e];
+      acc += (double)fmaf(x.x, y.x, x.y * y.y);
+    } else {
+      acc += (double)fmaf(x.x, x.x, x.y * x.y);
+    }
+  }
+  block_partials(acc, part, nb);
+}
+
+// x_i += alpha_i p_i ; r_i -= alpha_i q_i ; partials of |r_i|^2
+__global__ void k_fm_update(double *part, float2 *x, float2 *r, const float2 *p, const float2 *q, MultiScalars al,
+                            long cnt, int nb) {
+  const long n = cnt * nb;
+  const float a = (float)al.a[threadIdx.x % nb];
+  double acc = 0;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    float2 xv = x[e], rv = r[e];
+    const float2 pv = p[e], qv = q[e];
+    xv.x = fmaf(a, pv.x, xv.x);
+    xv.y = fmaf(a, pv.y, xv.y);
+    rv.x = fmaf(-a, qv.x, rv.x);
+    rv.y = fmaf(-a, qv.y, rv.y);
+    x[e] = xv;
+    r[e] = rv;
+    acc += (double)fmaf(rv.x, rv.x, rv.y * rv.y);
+  }
+  block_partials(acc, part, nb);
+}
+
+// p_i = r_i + beta_i p_i for the systems flagged in `on`
+__global__ void k_fm_xpay(float2 *p, const float2 *r, MultiScalars be, MultiScalars on, long cnt, int nb) {
+  const long n = cnt * nb;
+  const int i = threadIdx.x % nb;
+  if (on.a[i] == 0.0) return;
+  const float b = (float)be.a[i];
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const float2 pv = p[e], rv = r[e];
+    p[e] = make_float2(fmaf(b, pv.x, rv.x), fmaf(b, pv.y, rv.y));
+  }
+}
+
+__global__ void k_fm_from_d(float2 *f, const double2 *d, long n) {
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const double2 v = d[e];
+    f[e] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
+__global__ void k_fm_add_to_d(double2 *d, const float2 *f, long n) {
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const float2 v = f[e];
+    double2 w = d[e];
+    w.x += (double)v.x;
+    w.y += (double)v.y;
+    d[e] = w;
+  }
+}
+
+// dst = Hphi src with the compressed FP32 operator on batched FP32 fields (tmp: odd sites)
+static void fhphi_multi(Lattice &L, int nb, float2 *dst, const float2 *src, float2 *tmp) {
+  MultiFHopArgs a{};
+  a.g = L.g;
+  a.U = L.sl_links.as<float2>();
+  a.C = L.sl_clover.as<float4>();
+  a.nb = nb;
+  const int S = std::min(24, std::max(1, 192 / nb));
+  a.sites = S;
+  MultiFHopArgs s1 = a;
+  s1.src = src; s1.dst = tmp; s1.coeff = 0.5f; s1.lo = (int)L.Vh; s1.n = (int)L.Vh;
+  MultiFHopArgs s2 = a;
+  s2.src = tmp; s2.src2 = src; s2.dst = dst; s2.coeff = -0.5f; s2.lo = 0; s2.n = (int)L.Vh;
+  const size_t smem = (size_t)kFSiteBytes * S;
+  const int blocks = nblk(L.Vh, S);
+  if (L.sl_reals == 12) {
+    k_fhop_multi<6, 1><<<blocks, S * nb, smem, L.stream>>>(s1);
+    YG_LAUNCHED();
+    k_fhop_multi<6, 2><<<blocks, S * nb, smem, L.stream>>>(s2);
+  } else {
+    k_fhop_multi<9, 1><<<blocks, S * nb, smem, L.stream>>>(s1);
+    YG_LAUNCHED();
+    k_fhop_multi<9, 2><<<blocks, S * nb, smem, L.stream>>>(s2);
+  }
+  YG_LAUNCHED();
+  L.mvm += 2;
+}
+
+// nrhs solves of Hphi_sq with FP32 inner iterations and FP64 reliable updates; each system
+// stops on its TRUE FP64 residual |b_i - A x_i|^2 < prec |b_i|^2
+int cg_mixed_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, double *const *bs, double delta,
+                   yg_solve_stats *stats) {
+  auto t0 = std::chrono::steady_clock::now();
+  if (par.op != YG_OP_HPHI_SQ) throw Error(YG_ERR_ARG, "the batched mixed CG solves Hphi_sq systems");
+  if (nrhs < 1 || nrhs > kMaxRhs) throw Error(YG_ERR_ARG, "1..16 right-hand sides");
+  if (!L.p.eo) throw Error(YG_ERR_ARG, "the batched CG needs even-odd preconditioning");
+  if (L.d != 3) throw Error(YG_ERR_ARG, "the batched operator is built for d = 3");
+  if (!(delta > 0.0 && delta < 1.0)) throw Error(YG_ERR_ARG, "reliable-update delta must lie in (0,1)");
+  const int nb = nrhs;
+  const int reals = (L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL) ? 12 : 18;
+  // FP32 matrices of the compressed operator (shared with the single-system solver)
+  ensure_sloppy(L, par.mass, 16, reals, 32, 32);
+  Multi m(L, nb);
+  const long wall = (long)L.V * 4 * L.d;
+  const long nview = m.cnt * nb;                 // batched elements of the default view
+  std::vector<void *> bufs;
+  auto f64 = [&]() { double2 *p = m.field(); bufs.push_back(p); return p; };
+  auto f32 = [&]() {
+    float2 *p = nullptr;
+    YG_CUDA(cudaMalloc(&p, sizeof(float2) * (size_t)wall * nb));
+    bufs.push_back(p);
+    YG_CUDA(cudaMemsetAsync(p, 0, sizeof(float2) * (size_t)wall * nb, L.stream));
+    return p;
+  };
+  int status = YG_OK;
+  try {
+    double2 *X = f64(), *B = f64(), *R = f64(), *P64 = f64(), *Q = f64(), *T = f64(), *M = f64();
+    float2 *FX = f32(), *FR = f32(), *FP = f32(), *FQ = f32(), *FT = f32(), *FO = f32();
+    FieldPtrs fx{}, fb{};
+    for (int i = 0; i < nb; i++) {
+      fx.f[i] = (double2 *)xs[i];
+      fb.f[i] = (double2 *)bs[i];
+    }
+    k_multi_pack<<<nblk(wall * nb, 256), 256, 0, L.stream>>>(X, fx, 0, wall, nb, 0);
+    YG_LAUNCHED();
+    k_multi_pack<<<nblk(wall * nb, 256), 256, 0, L.stream>>>(B, fb, 0, wall, nb, 0);
+    YG_LAUNCHED();
+    const int sg = (int)std::min<long>(nblk(nview, 256), 148L * 16);
+    auto residual = [&]() {               // R = B - A X (FP64), per-system |R|^2
+      YG_CUDA(cudaMemcpyAsync(P64, X, sizeof(double2) * (size_t)wall * nb, cudaMemcpyDeviceToDevice, L.stream));
+      op_multi(L, YG_OP_HPHI_SQ, nb, par.mass, Q, P64, T, M);
+      k_multi_sub<<<m.grid, m.threads, 0, L.stream>>>(R, B, Q, m.w0, m.cnt, nb);
+      YG_LAUNCHED();
+      return m.sqnorm(R);
+    };
+    auto f_reduce = [&](int kind, const float2 *a, const float2 *b) {
+      if (kind == 0) k_fm_reduce<0><<<m.grid, m.threads, 0, L.stream>>>(m.part.as<double>(), a, b, m.cnt, nb);
+      else k_fm_reduce<1><<<m.grid, m.threads, 0, L.stream>>>(m.part.as<double>(), a, b, m.cnt, nb);
+      YG_LAUNCHED();
+      return m.sums();
+    };
+    const std::vector<double> norm = m.sqnorm(B);
+    std::vector<double> rr = residual(), rr_s(nb), maxrr(nb), best(nb), min_cycle(nb);
+    std::vector<int> active(nb), it(nb, 0), stall(nb, 0), since(nb, 0);
+    int nactive = 0, updates = 0;
+    for (int i = 0; i < nb; i++) {
+      active[i] = !(rr[i] < norm[i] * par.prec);
+      nactive += active[i];
+      rr_s[i] = maxrr[i] = best[i] = min_cycle[i] = rr[i];
+    }
+    k_fm_from_d<<<sg, 256, 0, L.stream>>>(FR, R, nview);
+    YG_LAUNCHED();
+    YG_CUDA(cudaMemcpyAsync(FP, FR, sizeof(float2) * (size_t)nview, cudaMemcpyDeviceToDevice, L.stream));
+    const double d2 = delta * delta;
+    constexpr int kStagnate = 100;
+    bool fallback = false;
+    int k = 0;
+    while (nactive > 0) {
+      k++;
+      if (par.maxiter > 0 && k > par.maxiter) { status = YG_MAXITER; break; }
+      fhphi_multi(L, nb, FT, FP, FO);
+      fhphi_multi(L, nb, FQ, FT, FO);
+      const std::vector<double> pq = f_reduce(0, FP, FQ);
+      MultiScalars al{}, be{}, on{};
+      for (int i = 0; i < nb; i++) {
+        if (!active[i]) continue;
+        if (!std::isfinite(pq[i])) throw Error(YG_NONFINITE, "non-finite value in cg_mixed_multi");
+        al.a[i] = rr_s[i] / pq[i];
+      }
+      k_fm_update<<<m.grid, m.threads, 0, L.stream>>>(m.part.as<double>(), FX, FR, FP, FQ, al, m.cnt, nb);
+      YG_LAUNCHED();
+      const std::vector<double> rn = m.sums();
+      bool trigger = false;
+      for (int i = 0; i < nb; i++) {
+        if (!active[i]) continue;
+        it[i] = k;
+        be.a[i] = rn[i] / rr_s[i];
+        on.a[i] = 1.0;
+        rr_s[i] = rn[i];
+        if (rn[i] < 0.25 * min_cycle[i]) { min_cycle[i] = rn[i]; since[i] = 0; }
+        else since[i]++;
+        if (rn[i] < d2 * maxrr[i] || rn[i] < norm[i] * par.prec || since[i] >= kStagnate) trigger = true;
+      }
+      k_fm_xpay<<<m.grid, m.threads, 0, L.stream>>>(FP, FR, be, on, m.cnt, nb);
+      YG_LAUNCHED();
+      if (!trigger) continue;
+      // reliable update of every system: fold the FP32 increments into X, recompute R
+      k_fm_add_to_d<<<sg, 256, 0, L.stream>>>(X, FX, nview);
+      YG_LAUNCHED();
+      YG_CUDA(cudaMemsetAsync(FX, 0, sizeof(float2) * (size_t)nview, L.stream));
+      const std::vector<double> rt = residual();
+      updates++;
+      for (int i = 0; i < nb; i++) {
+        if (!active[i]) continue;
+        rr[i] = rt[i];
+        if (rt[i] < norm[i] * par.prec) {
+          active[i] = 0;
+          nactive--;
+          continue;
+        }
+        if (rt[i] > 100.0 * best[i]) fallback = true;             // the inner solve diverged
+        if (rt[i] < 0.5 * best[i]) stall[i] = 0;
+        else if (++stall[i] >= 8) fallback = true;
+        best[i] = std::min(best[i], rt[i]);
+        rr_s[i] = maxrr[i] = min_cycle[i] = rt[i];
+        since[i] = 0;
+      }
+      if (fallback) break;
+      k_fm_from_d<<<sg, 256, 0, L.stream>>>(FR, R, nview);
+      YG_LAUNCHED();
+    }
+    if (status == YG_MAXITER) {
+      k_fm_add_to_d<<<sg, 256, 0, L.stream>>>(X, FX, nview);
+      YG_LAUNCHED();
+    }
+    k_multi_pack<<<nblk(nview, 256), 256, 0, L.stream>>>(X, fx, m.w0, m.cnt, nb, 1);
+    YG_LAUNCHED();
+    YG_CUDA(cudaStreamSynchronize(L.stream));
+    std::vector<int> fb_flag(nb, 0);
+    if (fallback) {
+      // the systems still open continue with the batched FP64 CG from their iterates
+      std::vector<double *> ox, ob;
+      std::vector<int> idx;
+      for (int i = 0; i < nb; i++)
+        if (active[i]) { ox.push_back(xs[i]); ob.push_back(bs[i]); idx.push_back(i); }
+      for (void *b : bufs) cudaFree(b);
+      bufs.clear();
+      std::vector<int> its(idx.size());
+      yg_inv_par p64 = par;
+      p64.log = 0;
+      status = cg_multi(L, p64, (int)idx.size(), ox.data(), ob.data(), its.data());
+      for (size_t q = 0; q < idx.size(); q++) {
+        it[idx[q]] += its[q];
+        fb_flag[idx[q]] = 1;
+      }
+      // true residuals of the fallback systems
+      Multi m2(L, nb);
+      double2 *X2 = m2.field(), *B2 = m2.field(), *R2 = m2.field(), *Q2 = m2.field(), *T2 = m2.field(),
+              *M2 = m2.field();
+      bufs = {X2, B2, R2, Q2, T2, M2};
+      k_multi_pack<<<nblk(wall * nb, 256), 256, 0, L.stream>>>(X2, fx, 0, wall, nb, 0);
+      YG_LAUNCHED();
+      k_multi_pack<<<nblk(wall * nb, 256), 256, 0, L.stream>>>(B2, fb, 0, wall, nb, 0);
+      YG_LAUNCHED();
+      op_multi(L, YG_OP_HPHI_SQ, nb, par.mass, Q2, X2, T2, M2);
+      k_multi_sub<<<m2.grid, m2.threads, 0, L.stream>>>(R2, B2, Q2, m2.w0, m2.cnt, nb);
+      YG_LAUNCHED();
+      rr = m2.sqnorm(R2);
+    }
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    for (int i = 0; i < nb; i++) {
+      if (status == YG_OK && rr[i] >= norm[i] * par.prec) status = YG_STALL;
+      if (stats) {
+        stats[i].iterations = it[i];
+        stats[i].reliable_updates = updates;
+        stats[i].fallback = fb_flag[i];
+        stats[i].true_residual = rr[i] / norm[i];
+        stats[i].seconds = secs;
+      }
+    }
+    if (par.log)
+      for (int i = 0; i < nb; i++)
+        fprintf(stderr, "[INVERTER][30]cg_mixed_multi[%d]: iterations = %d, precision = %1.4e\n", i, it[i],
+                rr[i] / norm[i]);
+  } catch (...) {
+    for (void *b : bufs) cudaFree(b);
+    throw;
+  }
+  for (void *b : bufs) cudaFree(b);
   return status;
 }
 
