@@ -199,6 +199,11 @@ int yg_cg_inverter_multi(yg_lattice *lat, const yg_inv_par *par, int nrhs, doubl
 int yg_cg_mixed_multi(yg_lattice *lat, const yg_inv_par *par, int nrhs, double *const *xs, double *const *bs,
                       double delta, yg_solve_stats *stats);
 
+/* No reference counterpart (measurement support): mean time per launch of `reps` launches of
+ * step 1 of yg_cg_mixed's inner operator (its dominant kernel), timed with CUDA events on the
+ * lattice's stream, and the compulsory bytes one launch moves. */
+int yg_inner_hop_profile(yg_lattice *lat, double mass, int reps, double *ms_per_launch, double *bytes_per_launch);
+
 /* No reference counterpart: options of the mixed-precision solver.
  *   inner_precision  32 (FP32 storage) or 16 (FP16 storage with per-site norms), FP32
  *                    arithmetic; 0 selects the generic FP32 operator of yg_cg_mixed (any d)

@@ -104,6 +104,7 @@ _SIGNATURES = {
     "yg_cg_mixed_opts": [_P, ctypes.POINTER(InvPar), ctypes.POINTER(MixedOpts), _P, _P, ctypes.POINTER(SolveStats)],
     "yg_cg_inverter_multi": [_P, _P, _I, _P, _P, _P],
     "yg_cg_mixed_multi": [_P, _P, _I, _P, _P, _D, _P],
+    "yg_inner_hop_profile": [_P, _D, _I, _P, _P],
     "yg_momenta_upload": [_P, _P], "yg_momenta_download": [_P, _P], "yg_momenta_zero": [_P],
     "yg_clover_force_download": [_P, _P], "yg_begin_fermion_force": [_P], "yg_end_fermion_force": [_P, _D],
     "yg_wilson_fermion_force": [_P, _D, _D, _D, _P, _P], "yg_wilson_fermion_force_q": [_P, _D, _D, _D, _P],
@@ -381,6 +382,12 @@ class Lattice:
         if rc not in (0, 4):
             self._check(rc)
         return list(its)
+
+    def inner_hop_profile(self, mass, reps=50):
+        """(ms per launch, compulsory bytes per launch) of the mixed solver's dominant kernel"""
+        ms, by = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.yg_inner_hop_profile(self.h, mass, int(reps), ctypes.byref(ms), ctypes.byref(by)))
+        return ms.value, by.value
 
     def cg_mixed_multi(self, op, mass, prec, xs, bs, delta=0.1, log=0, maxiter=0):
         """len(xs) mixed-precision solves advanced together; one stats dict per system"""

@@ -272,6 +272,9 @@ int yg_cg_mixed_multi(yg_lattice *l, const yg_inv_par *p, int nrhs, double *cons
     return yg::cg_mixed_multi(lat(l), *p, nrhs, xs, bs, delta, stats);
   });
 }
+int yg_inner_hop_profile(yg_lattice *l, double mass, int reps, double *ms, double *bytes) {
+  return guard([&] { need(ms, "ms"); need(bytes, "bytes"); yg::inner_hop_profile(lat(l), mass, reps, ms, bytes); });
+}
 int yg_cg_mixed(yg_lattice *l, const yg_inv_par *p, double *x, double *b, yg_solve_stats *st) {
   return guard_status([&] {
     check_par(p); need(x, "x"); need(b, "b");

@@ -208,5 +208,6 @@ int cg_mixed_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *x
                    yg_solve_stats *stats);
 // the compressed inner operator's matrices (yg_sloppy.cu); formats 32 / 16 / 15, 0 = as prec
 void ensure_sloppy(Lattice &L, double mass, int prec, int reals, int lfmt, int cfmt);
+void inner_hop_profile(Lattice &L, double mass, int reps, double *ms, double *bytes);
 
 }  // namespace yg

@@ -986,4 +986,45 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int 
   return status;
 }
 
+// Measurement support: mean time of `reps` launches of step 1 of the compressed inner
+// operator (the kernel that dominates cg_mixed) with the solver's default storage, timed
+// with CUDA events on the lattice's stream, and the compulsory bytes one launch moves
+// (neighbour spinors read once, links, clover blocks, output spinor).
+void inner_hop_profile(Lattice &L, double mass, int reps, double *ms, double *bytes) {
+  if (reps < 1) throw Error(YG_ERR_ARG, "reps must be >= 1");
+  const int reals = (L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL) ? 12 : 18;
+  ensure_sloppy(L, mass, 16, reals, 32, 32);
+  SField src = sfield(L, 41), dst = sfield(L, 44);
+  sloppy_from_d(L, src, L.scratch_field(3));
+  SHopArgs a{};
+  a.g = L.g;
+  a.U = L.sl_links.p;
+  a.C = L.sl_clover.p;
+  a.Cn = L.sl_cnorm.as<float>();
+  a.src = src.data; a.src_norm = src.norm;
+  a.dst = dst.data; a.dst_norm = dst.norm;
+  a.coeff = 0.5f;
+  a.lo = (int)L.Vh; a.n = (int)L.Vh;
+  cudaEvent_t e0, e1;
+  YG_CUDA(cudaEventCreate(&e0));
+  YG_CUDA(cudaEventCreate(&e1));
+  YG_SLOPPY_DISPATCH(L.sl_prec, L.sl_lfmt, L.sl_cfmt, L.sl_reals, {
+    for (int w = 0; w < 3; w++) launch_pdl(k_shop<SP, SL, SC, SK, 1, 0>, nblk(a.n, 128), 128, L.stream, a);
+    YG_CUDA(cudaEventRecord(e0, L.stream));
+    for (int r = 0; r < reps; r++) launch_pdl(k_shop<SP, SL, SC, SK, 1, 0>, nblk(a.n, 128), 128, L.stream, a);
+    YG_CUDA(cudaEventRecord(e1, L.stream));
+    for (int r = 0; r < reps + 3; r++) YG_LAUNCHED();
+  });
+  YG_CUDA(cudaEventSynchronize(e1));
+  float t = 0.f;
+  YG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = t / reps;
+  const double spinor = L.sl_prec == 16 ? 52.0 : 96.0;
+  const double link = (reals / 2) * (L.sl_lfmt == ST_F32 ? 8.0 : 4.0);
+  const double clov = 72.0 * (L.sl_cfmt == ST_F32 ? 4.0 : 2.0) + (L.sl_cfmt == ST_I16 ? 4.0 : 0.0);
+  *bytes = (double)L.Vh * (spinor + 8.0 * link + clov + spinor);
+}
+
 }  // namespace yg
