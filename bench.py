@@ -60,6 +60,9 @@ def parse():
                          "operator with FP32/FP16 spinors and 18/12-real links")
     ap.add_argument("--delta", type=float, default=0.1, help="reliable-update threshold")
     ap.add_argument("--variants", action="store_true", help="also time every inner operator once")
+    ap.add_argument("--field-cache", default=None,
+                    help="npz file holding the generated field: loaded when present, written otherwise "
+                         "(lets a profiled run skip the field generation)")
     ap.add_argument("--therm-trajectories", type=int, default=THERM["trajectories"],
                     help="HMC trajectories of the field generation (fewer only to profile a few launches)")
     ap.add_argument("--nrhs", type=int, default=12, help="systems of the batched-CG measurement (<= 1: skip)")
@@ -127,9 +130,15 @@ def thermalised_links(dims, seed, trajectories=None):
     return U, plaq, acc
 
 
-def make_inputs(dims, seed, rank=0, trajectories=None):
+def make_inputs(dims, seed, rank=0, trajectories=None, cache=None):
     from yahmc_b200 import fields
-    U, plaq, acc = thermalised_links(dims, seed, trajectories)
+    if cache and os.path.exists(cache):
+        z = np.load(cache)
+        U, plaq, acc = z["U"], float(z["plaquette"]), float(z["acceptance"])
+    else:
+        U, plaq, acc = thermalised_links(dims, seed, trajectories)
+        if cache:
+            np.savez(cache, U=U, plaquette=plaq, acceptance=acc)
     T, X, Y, Z = dims
     V = T * X * Y * Z
     rng = np.random.default_rng(seed + 7919 * rank)
@@ -223,7 +232,7 @@ def run_reference(a, rank, world):
     threads = os.cpu_count() or 1
     import yahmc_b200 as yg
     yg.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    U, b, info = make_inputs(a.dims, a.seed, 0, a.therm_trajectories)   # input preparation (GPU HMC)
+    U, b, info = make_inputs(a.dims, a.seed, 0, a.therm_trajectories, a.field_cache)   # input preparation
     # one full solve is the bounded sample: about a minute on 16 host cores at 32^4; the
     # reference code has no warm-up effect worth a second minute
     steps, warm = 1, 0
@@ -249,7 +258,7 @@ def run_ours(a, rank, world, dist):
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
     dev = torch.cuda.current_device()
     yg.set_device(dev)
-    U, b, info = make_inputs(a.dims, a.seed, rank, a.therm_trajectories)
+    U, b, info = make_inputs(a.dims, a.seed, rank, a.therm_trajectories, a.field_cache)
     lat = yg.Lattice(a.dims, nc=3, repr="fundamental", bc="antiperiodic", clover=True, eo=True, csw=CSW)
     lat.set_links(U)
     V, d = lat.V, lat.d
