@@ -178,8 +178,10 @@ int yg_rational_calc(yg_lattice *lat, const yg_inv_par *par, double a0, int orde
 /* No reference counterpart: CG on the same operator with FP32 inner iterations and FP64
  * reliable updates; stops on the TRUE FP64 squared residual |b-Ax|^2 < prec*|b|^2.  Uses
  * the compressed inner operator for d = 3 (FP16 spinors with per-site norms, FP32 links --
- * 12-real for SU(3) fundamental -- and clover blocks, delta 0.1) and the generic FP32
- * operator otherwise. */
+ * 12-real for SU(3) fundamental -- and clover blocks, delta 0.1; if that stalls, the inner
+ * solve restarts with FP32 spinors from its best iterate) and the generic FP32 operator
+ * otherwise.  stats->fallback: bit 0 the FP64 CG finished the solve, bit 1 the inner
+ * storage was raised to FP32. */
 int yg_cg_mixed(yg_lattice *lat, const yg_inv_par *par, double *x, double *b, yg_solve_stats *stats);
 
 /* No reference counterpart: nrhs cg_inverter solves (cg.cpp:132-202) of the same operator
@@ -220,6 +222,7 @@ typedef struct {
   double delta;
   int link_storage;     /* 0: as inner_precision; 32 FP32, 16 FP16, 15 int16 fixed point (entries / 32767) */
   int clover_storage;   /* 0: as inner_precision; 32, 16, or 15 (int16 with a per-site scale) */
+  int escalate;         /* 1: a stalled FP16 inner solve restarts with FP32 storage (as yg_cg_mixed) */
 } yg_mixed_opts;
 int yg_cg_mixed_opts(yg_lattice *lat, const yg_inv_par *par, const yg_mixed_opts *opts, double *x, double *b,
                      yg_solve_stats *stats);

@@ -118,3 +118,21 @@ def test_compressed_inner_argument_errors():
     b4, x4 = lat4.field(source(O4, rng4)), lat4.field()
     with pytest.raises(YGError):
         lat4.cg_mixed("Hphi_sq", -0.4, 1e-20, x4, b4, inner_precision=32, link_reals=18)   # d = 2
+
+
+def test_precision_ladder():
+    """A delta far below FP16's resolution stalls the FP16 inner solve; with escalation the
+    solve restarts the inner CG with FP32 storage from its best iterate (fallback bit 1)
+    and still meets the true residual."""
+    lat, O, rng = make_pair("su3_fund_ap", (8, 8, 8, 8), seed=38)
+    b = lat.field(source(O, rng))
+    x = lat.field()
+    st = lat.cg_mixed("Hphi_sq", -0.4, 1e-26, x, b, inner_precision=16, link_reals=12, delta=1e-5, escalate=True)
+    assert st["status"] == 0, st
+    assert st["fallback"] & 2, st
+    assert _true_residual(lat, "Hphi_sq", -0.4, x, b) < 1e-26
+    # the library default (FP16 spinors, FP32 matrices, escalation on)
+    x = lat.field()
+    st = lat.cg_mixed("Hphi_sq", -0.4, 1e-26, x, b)
+    assert st["status"] == 0 and st["fallback"] == 0, st
+    assert _true_residual(lat, "Hphi_sq", -0.4, x, b) < 1e-26

@@ -61,7 +61,7 @@ class InvPar(ctypes.Structure):
 
 class MixedOpts(ctypes.Structure):
     _fields_ = [("inner_precision", ctypes.c_int), ("link_reals", ctypes.c_int), ("delta", ctypes.c_double),
-                ("link_storage", ctypes.c_int), ("clover_storage", ctypes.c_int)]
+                ("link_storage", ctypes.c_int), ("clover_storage", ctypes.c_int), ("escalate", ctypes.c_int)]
 
 
 class SolveStats(ctypes.Structure):
@@ -406,7 +406,7 @@ class Lattice:
                  "fallback": st.fallback, "true_residual": st.true_residual, "seconds": st.seconds} for st in sts]
 
     def cg_mixed(self, op, mass, prec, x, b, log=0, maxiter=0, inner_precision=None, link_reals=18, delta=0.1,
-                 link_storage=0, clover_storage=0):
+                 link_storage=0, clover_storage=0, escalate=False):
         """Mixed-precision CG (true FP64 stopping criterion).  inner_precision None: the
         library's choice (yg_cg_mixed); 0: the generic FP32 inner operator; 32 or 16: the
         compressed d = 3 inner operator with link_reals 18 or 12 and reliable-update
@@ -417,7 +417,8 @@ class Lattice:
         if inner_precision is None:
             rc = self.lib.yg_cg_mixed(self.h, ctypes.byref(par), x.ptr, b.ptr, ctypes.byref(st))
         else:
-            o = MixedOpts(int(inner_precision), int(link_reals), float(delta), int(link_storage), int(clover_storage))
+            o = MixedOpts(int(inner_precision), int(link_reals), float(delta), int(link_storage), int(clover_storage),
+                          int(bool(escalate)))
             rc = self.lib.yg_cg_mixed_opts(self.h, ctypes.byref(par), ctypes.byref(o), x.ptr, b.ptr, ctypes.byref(st))
         if rc not in (0, 4, 5):
             self._check(rc)

@@ -253,7 +253,7 @@ int yg_cg_mixed_opts(yg_lattice *l, const yg_inv_par *p, const yg_mixed_opts *o,
     check_par(p); need(o, "opts"); need(x, "x"); need(b, "b");
     if (o->inner_precision == 0) return yg::cg_mixed(lat(l), *p, x, b, st);
     return yg::cg_mixed_sloppy(lat(l), *p, o->inner_precision, o->link_reals, o->link_storage, o->clover_storage,
-                               o->delta, x, b, st);
+                               o->delta, x, b, st, o->escalate != 0);
   });
 }
 int yg_cg_inverter_multi(yg_lattice *l, const yg_inv_par *p, int nrhs, double *const *xs, double *const *bs,
@@ -285,7 +285,7 @@ int yg_cg_mixed(yg_lattice *l, const yg_inv_par *p, double *x, double *b, yg_sol
     // change the operator itself; else the generic FP32 operator
     if (L.d == 3 && L.p.eo) {
       int reals = (L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL) ? 12 : 18;
-      return yg::cg_mixed_sloppy(L, *p, 16, reals, 32, 32, 0.1, x, b, st);
+      return yg::cg_mixed_sloppy(L, *p, 16, reals, 32, 32, 0.1, x, b, st, /*escalate=*/true);
     }
     return yg::cg_mixed(L, *p, x, b, st);
   });

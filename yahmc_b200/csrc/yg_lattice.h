@@ -177,7 +177,7 @@ int rational_calc(Lattice &L, const yg_inv_par &par, double a0, int order, const
                   const double *residues, double *x, double *b, int *iters);
 int cg_mixed(Lattice &L, const yg_inv_par &par, double *x, double *b, yg_solve_stats *st);
 int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int lfmt, int cfmt, double delta,
-                    double *x, double *b, yg_solve_stats *st);
+                    double *x, double *b, yg_solve_stats *st, bool escalate = false);
 
 // ---- yg_forces.cu
 void clover_fermion_force(Lattice &L, double residue, double *lhs, double *rhs);

@@ -861,7 +861,7 @@ static void set_scalar(Lattice &L, int i, double v) {
 // and the search direction is kept.  The solve stops only on the true FP64 squared
 // residual |b - A x|^2 < prec |b|^2; a stall falls back to the FP64 CG.
 int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int lfmt, int cfmt, double delta,
-                    double *x, double *b, yg_solve_stats *st);
+                    double *x, double *b, yg_solve_stats *st, bool escalate);
 
 }  // namespace yg
 
@@ -870,7 +870,7 @@ namespace yg {
 int cg(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
 
 int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int lfmt, int cfmt, double delta,
-                    double *x, double *b, yg_solve_stats *st) {
+                    double *x, double *b, yg_solve_stats *st, bool escalate) {
   auto t0 = std::chrono::steady_clock::now();
   if (par.op != YG_OP_HPHI_SQ) throw Error(YG_ERR_ARG, "cg_mixed solves Hphi_sq systems");
   if (!(delta > 0.0 && delta < 1.0)) throw Error(YG_ERR_ARG, "reliable-update delta must lie in (0,1)");
@@ -900,11 +900,14 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int 
   double best = rr;
   double *xbest = L.scratch_field(46);      // the iterate with the smallest true residual
   blas_copy(L, xbest, x);
-  if (rr >= target) {
+
+  // the inner CG from the current x until the true residual meets prec (YG_OK), maxiter,
+  // or a stall / divergence of the true residual (YG_STALL)
+  auto run_inner = [&]() -> int {
     f_from_d(L, fr, r, cnt);
     sloppy_from_d(L, p, r);
     YG_CUDA(cudaMemsetAsync(fx, 0, sizeof(float2) * cnt, L.stream));
-    set_scalar(L, S_RR0, rr);                 // iteration 0 reads slot 0
+    set_scalar(L, S_RR0 + (it & 1), rr);      // the slot the first iteration reads
     double maxrr = rr;
     const double d2 = delta * delta;
     bool pending = false;           // an enqueued iteration whose |r|^2 is still to be read
@@ -914,11 +917,11 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int 
     constexpr int kStagnate = 100;
     double min_cycle = rr;
     int since_min = 0;
+    stall = 0;
     while (true) {
       if (par.maxiter > 0 && it >= par.maxiter) {
-        status = YG_MAXITER;
         d_add_f(L, x, fx, cnt);     // keep the progress of the inner iterations
-        break;
+        return YG_MAXITER;
       }
       int slot = it & 1;
       sloppy_hphi(L, t, p, o, true);
@@ -940,11 +943,11 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int 
         double rr_true = residual();
         updates++;
         rr = rr_true;
-        if (rr_true < target) break;
+        if (rr_true < target) return YG_OK;
         if (rr_true < best) blas_copy(L, xbest, x);
-        if (rr_true > 100.0 * best) { status = YG_STALL; break; }       // the inner solve diverged
+        if (rr_true > 100.0 * best) return YG_STALL;               // the inner solve diverged
         if (rr_true < 0.5 * best) stall = 0;
-        else if (++stall >= 8) { status = YG_STALL; break; }
+        else if (++stall >= 8) return YG_STALL;
         best = std::min(best, rr_true);
         f_from_d(L, fr, r, cnt);
         set_scalar(L, S_RR0 + (it & 1), rr_true); // the slot the next iteration reads
@@ -954,15 +957,29 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int 
         pending = false;            // the enqueued |r|^2 predates the update
       }
     }
+  };
+
+  int raised = 0;
+  if (rr >= target) {
+    status = run_inner();
+    if (status == YG_STALL && escalate && prec == 16) {
+      // FP16 spinors (or matrices) too coarse for this system: restart the inner CG with
+      // FP32 storage from the best iterate before handing over to the FP64 CG
+      raised = 1;
+      ensure_sloppy(L, par.mass, 32, reals, 32, 32);
+      blas_copy(L, x, xbest);
+      rr = residual();
+      status = rr < target ? YG_OK : run_inner();
+    }
   }
-  int fallback = 0;
+  int fallback = raised ? 2 : 0;
   if (status != YG_OK) {
     // plain FP64 CG (the reference's solver) from the best iterate; its recursive residual
     // can stop above the true one, so it restarts until the true residual meets prec
     blas_copy(L, x, xbest);
     yg_inv_par p64 = par;
     p64.log = 0;
-    fallback = 1;
+    fallback |= 1;
     for (int attempt = 0; attempt < 3; attempt++) {
       int it64 = 0;
       status = cg(L, p64, x, b, &it64);
