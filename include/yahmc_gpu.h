@@ -227,6 +227,16 @@ typedef struct {
 int yg_cg_mixed_opts(yg_lattice *lat, const yg_inv_par *par, const yg_mixed_opts *opts, double *x, double *b,
                      yg_solve_stats *stats);
 
+/* ---- chronological initial guess (mre.h) -------------------------------- */
+/* The past solutions live on the device.  op is YG_OP_DPHI / HPHI / HPHI_SQ (mre_par.mvm),
+ * max <= 15 (MRE_MAX); max = 0 disables the extrapolation (yg_mre_guess leaves dst alone). */
+typedef struct yg_mre yg_mre;
+int yg_mre_init(yg_lattice *lat, int max, int op, double mass, yg_mre **out);   /* mre.cpp:85-111 */
+int yg_mre_store(yg_mre *m, const double *solution);                          /* mre.cpp:35-51 */
+int yg_mre_guess(yg_mre *m, double *dst, const double *src);                  /* mre.cpp:53-83 */
+int yg_mre_reset(yg_mre *m);                                                   /* mre.cpp:113-116 */
+int yg_mre_free(yg_mre *m);
+
 /* ---- forces (forces.h:6-15) -------------------------------------------- */
 int yg_momenta_upload(yg_lattice *lat, const double *host);     /* afield_momenta, 4*V suNa */
 int yg_momenta_download(yg_lattice *lat, double *host);

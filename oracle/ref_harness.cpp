@@ -44,6 +44,7 @@
 #include <checks.h>
 #include <timing.h>
 #include <update.h>
+#include <mre.h>
 
 /* defined in library/update.cpp without a header declaration */
 double hamiltonian();
@@ -397,6 +398,13 @@ void yref_update_links(double eps) { update_links(eps); }
 void yref_reunitarize(void) { reunitarize(); }
 void yref_represent_gauge_field(void) { represent_gauge_field(); }
 double yref_hamiltonian(void) { return hamiltonian(); }     /* no monomials: the momentum part */
+
+/* ---- chronological initial guess (mre.h) ---- */
+static mre_par mre_state;
+void yref_mre_init(int max, int op, double mass) { mre_init(mre_state, max, op_from_id(op), mass); }
+void yref_mre_store(double *f) { SpinorField s; wrap(s, f); mre_store(mre_state, s); }
+void yref_mre_guess(double *dst, double *src) { SpinorField d, s; wrap(d, dst); wrap(s, src); mre_guess(mre_state, d, s); }
+void yref_mre_reset(void) { mre_reset(mre_state); }
 
 /* ---- the reference's own self-checks (checks/check.cpp:4-26) ---- */
 int yref_check_group(void) { return check_group(); }

@@ -718,6 +718,51 @@ class Oracle:
             p[V] += r[V]
         return it
 
+    # ---- mre.cpp:15-117 (chronological initial guess) with lu of solver.cpp:4-95
+    def mre_init(self, max_, op, mass):
+        self.mre = {"max": min(max_, 15), "op": op, "mass": mass, "num": 0,
+                    "s": [self.new_field() for _ in range(min(max_, 15))]}
+
+    def mre_store(self, sol):
+        m = self.mre
+        if m["max"] == 0:
+            return
+        tmp = m["s"].pop()
+        m["s"].insert(0, tmp)
+        tmp[:] = sol                       # spinor_copy: the whole field
+        m["num"] += 1
+
+    def mre_guess(self, dst, src):
+        """dst = sum_k x_k s_k; the stored solutions are orthonormalised in place with the
+        reference's coefficient <s_i, s_j> = sum s_i conj(s_j) (mre.cpp:14-33)."""
+        m = self.mre
+        if m["max"] == 0:
+            return
+        lo, hi = self.default_range()
+        V = slice(lo, hi)
+        k = min(m["num"], m["max"])
+        dst[:] = 0
+        s = m["s"]
+        for i in range(k):
+            s[i][V] *= 1.0 / np.sqrt(np.sum(np.abs(s[i][V]) ** 2))
+            for j in range(i + 1, k):
+                rij = np.sum(s[i][V] * np.conj(s[j][V]))
+                s[j][V] -= rij * s[i][V]
+        A = np.zeros((k, k), dtype=complex)
+        b = np.zeros(k, dtype=complex)
+        A_op = self.op(m["op"])
+        out = self.new_field()
+        for i in range(k):
+            A_op(m["mass"], out, s[i])
+            for j in range(k):
+                A[j, i] = np.sum(out[V] * np.conj(s[j][V]))
+            b[i] = np.sum(src[V] * np.conj(s[i][V]))
+        if k == 0:
+            return
+        x = np.linalg.solve(A, b)
+        for i in range(k):
+            dst[V] += x[i] * s[i][V]
+
     def cg_mshift(self, op, mass, prec, shifts, b, maxiter=100000):
         """cg_mshift, cg.cpp:11-130.  Returns (iterations, [x_n])."""
         A = self.op(op)

@@ -186,3 +186,23 @@ def test_md_support(name):
     R.call("reunitarize")
     O.reunitarize_links()
     assert _rel(yo.mat_from_raw(R.get_links(), nc).reshape(V, 4, nc, nc), O.fund) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["su3_fund_ap", "su3_fund_open", "su2_adj_ap", "su3_fund_ap_nocl"])
+def test_mre_guess(name):
+    """mre_store / mre_guess (mre.cpp:15-117) with lu (solver.cpp:4-95): 6 stored solutions in
+    a 4-deep history, then the extrapolated guess for a new source."""
+    R, O, rng, src = _setup(name, 8)
+    R.call("mre_init", 4, 2, -0.3)
+    O.mre_init(4, "Hphi_sq", -0.3)
+    for _ in range(6):
+        s = fields.gaussian_spinor(O.V, O.d, rng)
+        O.bcs_on_spinor(s)
+        R.call("mre_store", yo.spinor_to_raw(s))
+        O.mre_store(s)
+    d_r = np.zeros(O.V * 8 * O.d)
+    R.call("mre_guess", d_r, yo.spinor_to_raw(src))
+    d_o = O.new_field()
+    O.mre_guess(d_o, src.copy())
+    lo, hi = O.default_range()
+    assert _rel(yo.spinor_from_raw(d_r, O.d)[lo:hi], d_o[lo:hi]) < 1e-12

@@ -105,6 +105,8 @@ _SIGNATURES = {
     "yg_cg_inverter_multi": [_P, _P, _I, _P, _P, _P],
     "yg_cg_mixed_multi": [_P, _P, _I, _P, _P, _D, _P],
     "yg_inner_hop_profile": [_P, _D, _I, _P, _P],
+    "yg_mre_init": [_P, _I, _I, _D, _P], "yg_mre_store": [_P, _P], "yg_mre_guess": [_P, _P, _P],
+    "yg_mre_reset": [_P], "yg_mre_free": [_P],
     "yg_momenta_upload": [_P, _P], "yg_momenta_download": [_P, _P], "yg_momenta_zero": [_P],
     "yg_clover_force_download": [_P, _P], "yg_begin_fermion_force": [_P], "yg_end_fermion_force": [_P, _D],
     "yg_wilson_fermion_force": [_P, _D, _D, _D, _P, _P], "yg_wilson_fermion_force_q": [_P, _D, _D, _D, _P],
@@ -136,6 +138,28 @@ def load_library(path: Path | str | None = None):
         fn.restype = None if name in ("yg_lattice_destroy", "yg_mvm_reset") else ctypes.c_int
     _lib = lib
     return lib
+
+
+class Mre:
+    """Chronological initial guess (mre.h): store past solutions, extrapolate a guess."""
+
+    def __init__(self, lat, max_, op, mass):
+        self.lat, self.lib = lat, lat.lib
+        h = ctypes.c_void_p()
+        lat._check(self.lib.yg_mre_init(lat.h, int(max_), _OPS[op] if isinstance(op, str) else int(op), mass,
+                                        ctypes.byref(h)))
+        self.h = h
+
+    def store(self, f): self.lat._check(self.lib.yg_mre_store(self.h, f.ptr))
+
+    def guess(self, dst, src): self.lat._check(self.lib.yg_mre_guess(self.h, dst.ptr, src.ptr))
+
+    def reset(self): self.lat._check(self.lib.yg_mre_reset(self.h))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.yg_mre_free(self.h)
+            self.h = None
 
 
 def set_device(device: int) -> None:
@@ -382,6 +406,10 @@ class Lattice:
         if rc not in (0, 4):
             self._check(rc)
         return list(its)
+
+    def mre(self, max_, op, mass):
+        """mre_init (mre.cpp:85-111): a history of up to max_ past solutions of `op`"""
+        return Mre(self, max_, op, mass)
 
     def inner_hop_profile(self, mass, reps=50):
         """(ms per launch, compulsory bytes per launch) of the mixed solver's dominant kernel"""

@@ -291,6 +291,33 @@ int yg_cg_mixed(yg_lattice *l, const yg_inv_par *p, double *x, double *b, yg_sol
   });
 }
 
+// ---- chronological initial guess
+struct yg_mre {
+  yg::Mre *m;
+};
+int yg_mre_init(yg_lattice *l, int max, int op, double mass, yg_mre **out) {
+  return guard([&] {
+    need(out, "out");
+    *out = nullptr;
+    yg_mre *h = new yg_mre{yg::mre_create(lat(l), max, op, mass)};
+    *out = h;
+  });
+}
+int yg_mre_store(yg_mre *h, const double *sol) {
+  return guard([&] { need(h, "mre"); need(sol, "solution"); yg::mre_store(*h->m, sol); });
+}
+int yg_mre_guess(yg_mre *h, double *dst, const double *src) {
+  return guard([&] { need(h, "mre"); need(dst, "dst"); need(src, "src"); yg::mre_guess(*h->m, dst, src); });
+}
+int yg_mre_reset(yg_mre *h) { return guard([&] { need(h, "mre"); yg::mre_reset(*h->m); }); }
+int yg_mre_free(yg_mre *h) {
+  return guard([&] {
+    if (!h) return;
+    yg::mre_destroy(h->m);
+    delete h;
+  });
+}
+
 // ---- forces
 int yg_momenta_upload(yg_lattice *l, const double *h) { return guard([&] { need(h, "host"); yg::momenta_upload(lat(l), h); }); }
 int yg_momenta_download(yg_lattice *l, double *h) { return guard([&] { need(h, "host"); yg::momenta_download(lat(l), h); }); }

@@ -210,4 +210,12 @@ int cg_mixed_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *x
 void ensure_sloppy(Lattice &L, double mass, int prec, int reals, int lfmt, int cfmt);
 void inner_hop_profile(Lattice &L, double mass, int reps, double *ms, double *bytes);
 
+// chronological initial guess (yg_mre.cu)
+struct Mre;
+Mre *mre_create(Lattice &L, int max, int op, double mass);
+void mre_destroy(Mre *m);
+void mre_reset(Mre &m);
+void mre_store(Mre &m, const double *sol);
+void mre_guess(Mre &m, double *dst, const double *src);
+
 }  // namespace yg
