@@ -227,6 +227,17 @@ typedef struct {
 int yg_cg_mixed_opts(yg_lattice *lat, const yg_inv_par *par, const yg_mixed_opts *opts, double *x, double *b,
                      yg_solve_stats *stats);
 
+/* ---- gauge configuration files (gaugefield.cpp:44-179, hirep.cpp:56-212) ---- */
+/* CFG: 256-byte header (ident, version, dims, nc, repr, num_cnfg, num_accept, plaquette),
+ * HiRep: big-endian (N, T, X, Y, Z, plaquette); both then every site's four links in
+ * t, x, y, z order.  Loading checks the header against the lattice (an error where the
+ * reference stops), applies the gauge boundary conditions, represents the field, and
+ * returns |stored plaquette - plaquette of the loaded field|. */
+int yg_gauge_save_cfg(yg_lattice *lat, const char *path, int num_cnfg, int num_accept);
+int yg_gauge_load_cfg(yg_lattice *lat, const char *path, int *num_cnfg, int *num_accept, double *plaquette_diff);
+int yg_gauge_save_hirep(yg_lattice *lat, const char *path);
+int yg_gauge_load_hirep(yg_lattice *lat, const char *path, int *num_cnfg, double *plaquette_diff);
+
 /* ---- chronological initial guess (mre.h) -------------------------------- */
 /* The past solutions live on the device.  op is YG_OP_DPHI / HPHI / HPHI_SQ (mre_par.mvm),
  * max <= 15 (MRE_MAX); max = 0 disables the extrapolation (yg_mre_guess leaves dst alone). */

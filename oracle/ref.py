@@ -108,6 +108,8 @@ class RefLattice:
             "yref_avr_wilson": [_I, _I],
             "yref_update_links": [_D], "yref_reunitarize": [], "yref_represent_gauge_field": [],
             "yref_hamiltonian": [],
+            "yref_gauge_save": [ctypes.c_char_p], "yref_gauge_load": [ctypes.c_char_p],
+            "yref_gauge_save_hirep": [ctypes.c_char_p], "yref_gauge_load_hirep": [ctypes.c_char_p],
             "yref_mre_init": [_I, _I, _D], "yref_mre_store": [_P], "yref_mre_guess": [_P, _P], "yref_mre_reset": [],
             "yref_represent": [_P, _P, _I],
         }.items():

@@ -45,6 +45,7 @@
 #include <timing.h>
 #include <update.h>
 #include <mre.h>
+#include <hirep.h>
 
 /* defined in library/update.cpp without a header declaration */
 double hamiltonian();
@@ -398,6 +399,12 @@ void yref_update_links(double eps) { update_links(eps); }
 void yref_reunitarize(void) { reunitarize(); }
 void yref_represent_gauge_field(void) { represent_gauge_field(); }
 double yref_hamiltonian(void) { return hamiltonian(); }     /* no monomials: the momentum part */
+
+/* ---- gauge configuration files (gaugefield.cpp:44-179, hirep.cpp:56-212) ---- */
+void yref_gauge_save(const char *path) { gauge_field_save(path); }
+void yref_gauge_load(const char *path) { gauge_field_load(path); }
+void yref_gauge_save_hirep(const char *path) { gauge_field_save_hirep(path); }
+void yref_gauge_load_hirep(const char *path) { gauge_field_load_hirep(path); }
 
 /* ---- chronological initial guess (mre.h) ---- */
 static mre_par mre_state;

@@ -1267,3 +1267,83 @@ class Oracle:
         momentum boundary conditions."""
         self.bcs_on_momenta()
         return TF / 2.0 * float(np.sum(self.mom ** 2))
+
+
+# ---------------------------------------------------------------- gauge configuration files
+# gaugefield.cpp:44-179 (CFG, native byte order) and hirep.cpp:56-212 (HiRep, big-endian).
+# U is (V, 4, N, N) complex in the even-odd site order; files run over t, x, y, z.
+CFG_IDENT, CFG_VERSION = 0x47464359, 0x20          # include/gaugefield.h:20-21
+_CFG_HEADER = np.dtype([("ident", "<i4"), ("version", "<i4"), ("dim_t", "<i4"), ("dim_x", "<i4"),
+                        ("dim_y", "<i4"), ("dim_z", "<i4"), ("nc", "<i4"), ("repr", "<i4"),
+                        ("num_cnfg", "<i4"), ("num_accept", "<i4"), ("plaquette", "<f8"),
+                        ("reserved", "V208")])      # header_t, packed, 256 bytes
+
+
+def _file_order(dims, eo=True):
+    """site ids of the lexicographic t, x, y, z loop (ipt, geometry.cpp:756-878): the
+    even-odd order with even-odd preconditioning, the loop index itself without"""
+    T, X, Y, Z = dims
+    V = T * X * Y * Z
+    lex = np.arange(V)
+    if not eo:
+        return lex
+    t, r = np.divmod(lex, X * Y * Z)
+    x, r = np.divmod(r, Y * Z)
+    y, z = np.divmod(r, Z)
+    return (((t + x + y + z) & 1) * V + lex) // 2
+
+
+def _links_to_file(U, dims, dtype, eo=True):
+    """(V,4,N,N) complex -> the per-site (re, im) interleaved doubles of suNg::write"""
+    nc = U.shape[-1]
+    u = U[_file_order(dims, eo)].reshape(-1, 4, nc * nc)
+    out = np.empty(u.shape + (2,), dtype=dtype)
+    out[..., 0] = u.real
+    out[..., 1] = u.imag
+    return out.reshape(-1)
+
+
+def _links_from_file(raw, dims, nc, eo=True):
+    V = int(np.prod(dims))
+    r = np.asarray(raw, dtype=np.float64).reshape(V, 4, nc * nc, 2)
+    u = (r[..., 0] + 1j * r[..., 1]).reshape(V, 4, nc, nc)
+    U = np.empty_like(u)
+    U[_file_order(dims, eo)] = u
+    return U
+
+
+def cfg_write(path, U, dims, nc, repr_id, plaquette, num_cnfg=0, num_accept=0, eo=True):
+    h = np.zeros(1, dtype=_CFG_HEADER)
+    h["ident"], h["version"] = CFG_IDENT, CFG_VERSION
+    h["dim_t"], h["dim_x"], h["dim_y"], h["dim_z"] = dims
+    h["nc"], h["repr"], h["num_cnfg"], h["num_accept"], h["plaquette"] = nc, repr_id, num_cnfg, num_accept, plaquette
+    with open(path, "wb") as f:
+        f.write(h.tobytes())
+        f.write(_links_to_file(U, dims, "<f8", eo).tobytes())
+
+
+def cfg_read(path, eo=True):
+    with open(path, "rb") as f:
+        h = np.frombuffer(f.read(_CFG_HEADER.itemsize), dtype=_CFG_HEADER)[0]
+        dims = (int(h["dim_t"]), int(h["dim_x"]), int(h["dim_y"]), int(h["dim_z"]))
+        nc = int(h["nc"])
+        raw = np.frombuffer(f.read(), dtype="<f8")
+    return {"ident": int(h["ident"]), "version": int(h["version"]), "dims": dims, "nc": nc, "repr": int(h["repr"]),
+            "num_cnfg": int(h["num_cnfg"]), "num_accept": int(h["num_accept"]), "plaquette": float(h["plaquette"]),
+            "U": _links_from_file(raw, dims, nc, eo)}
+
+
+def hirep_write(path, U, dims, nc, plaquette, eo=True):
+    with open(path, "wb") as f:
+        f.write(np.array([nc, *dims], dtype=">i4").tobytes())
+        f.write(np.array([plaquette], dtype=">f8").tobytes())
+        f.write(_links_to_file(U, dims, ">f8", eo).tobytes())
+
+
+def hirep_read(path, eo=True):
+    with open(path, "rb") as f:
+        info = np.frombuffer(f.read(20), dtype=">i4")
+        plaq = float(np.frombuffer(f.read(8), dtype=">f8")[0])
+        raw = np.frombuffer(f.read(), dtype=">f8").astype(np.float64)
+    nc, dims = int(info[0]), tuple(int(v) for v in info[1:5])
+    return {"nc": nc, "dims": dims, "plaquette": plaq, "U": _links_from_file(raw, dims, nc, eo)}

@@ -206,3 +206,36 @@ def test_mre_guess(name):
     O.mre_guess(d_o, src.copy())
     lo, hi = O.default_range()
     assert _rel(yo.spinor_from_raw(d_r, O.d)[lo:hi], d_o[lo:hi]) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["su3_fund_ap", "su2_adj_ap", "su3_fund_open"])
+def test_gauge_files(name, tmp_path):
+    """gauge_field_save/load (gaugefield.cpp:44-161) and the HiRep pair (hirep.cpp:56-212):
+    the oracle reads the reference's files bit-exactly, and the reference loads the
+    oracle's files into the same links (boundary conditions applied)."""
+    R, O, rng, src = _setup(name, 9)
+    nc = O.nc
+    U = yo.mat_from_raw(R.get_links(), nc).reshape(O.V, 4, nc, nc)
+    p = tmp_path / "a.cfg"
+    R.call("gauge_save", str(p).encode())
+    c = yo.cfg_read(p)
+    assert c["ident"] == yo.CFG_IDENT and c["version"] == yo.CFG_VERSION
+    assert c["dims"] == DIMS and c["nc"] == nc and c["repr"] == yo.REPR_NAMES.index(O.p.rep)
+    assert np.array_equal(c["U"], U)
+    assert abs(c["plaquette"] - R.call("avr_wilson", 1, 1)) < 1e-15
+    h = tmp_path / "a.hirep"
+    R.call("gauge_save_hirep", str(h).encode())
+    hr = yo.hirep_read(h)
+    assert hr["dims"] == DIMS and hr["nc"] == nc and np.array_equal(hr["U"], U)
+    W = fields.haar_su(nc, O.V * 4, rng).reshape(O.V, 4, nc, nc)
+    O.fund = W.copy()
+    O.bcs_on_gauge()
+    q = tmp_path / "b.cfg"
+    yo.cfg_write(q, W, DIMS, nc, yo.REPR_NAMES.index(O.p.rep), 0.5, 7, 3)
+    R.call("gauge_load", str(q).encode())
+    assert np.array_equal(yo.mat_from_raw(R.get_links(), nc).reshape(O.V, 4, nc, nc), O.fund)
+    R.set_links(fields.complex_to_raw(U))
+    q = tmp_path / "run1_n42"
+    yo.hirep_write(q, W, DIMS, nc, 0.25)
+    R.call("gauge_load_hirep", str(q).encode())
+    assert np.array_equal(yo.mat_from_raw(R.get_links(), nc).reshape(O.V, 4, nc, nc), O.fund)

@@ -107,6 +107,8 @@ _SIGNATURES = {
     "yg_inner_hop_profile": [_P, _D, _I, _P, _P],
     "yg_mre_init": [_P, _I, _I, _D, _P], "yg_mre_store": [_P, _P], "yg_mre_guess": [_P, _P, _P],
     "yg_mre_reset": [_P], "yg_mre_free": [_P],
+    "yg_gauge_save_cfg": [_P, ctypes.c_char_p, _I, _I], "yg_gauge_load_cfg": [_P, ctypes.c_char_p, _P, _P, _P],
+    "yg_gauge_save_hirep": [_P, ctypes.c_char_p], "yg_gauge_load_hirep": [_P, ctypes.c_char_p, _P, _P],
     "yg_momenta_upload": [_P, _P], "yg_momenta_download": [_P, _P], "yg_momenta_zero": [_P],
     "yg_clover_force_download": [_P, _P], "yg_begin_fermion_force": [_P], "yg_end_fermion_force": [_P, _D],
     "yg_wilson_fermion_force": [_P, _D, _D, _D, _P, _P], "yg_wilson_fermion_force_q": [_P, _D, _D, _D, _P],
@@ -406,6 +408,26 @@ class Lattice:
         if rc not in (0, 4):
             self._check(rc)
         return list(its)
+
+    # ---- gauge configuration files (gaugefield.cpp:44-179, hirep.cpp:56-212)
+    def gauge_field_save(self, path, num_cnfg=0, num_accept=0):
+        self._check(self.lib.yg_gauge_save_cfg(self.h, str(path).encode(), int(num_cnfg), int(num_accept)))
+
+    def gauge_field_load(self, path):
+        """returns (num_cnfg, num_accept, |stored - loaded plaquette|)"""
+        nc_, na, pd = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self._check(self.lib.yg_gauge_load_cfg(self.h, str(path).encode(), ctypes.byref(nc_), ctypes.byref(na),
+                                               ctypes.byref(pd)))
+        return nc_.value, na.value, pd.value
+
+    def gauge_field_save_hirep(self, path):
+        self._check(self.lib.yg_gauge_save_hirep(self.h, str(path).encode()))
+
+    def gauge_field_load_hirep(self, path):
+        """returns (num_cnfg, |stored - loaded plaquette|)"""
+        nc_, pd = ctypes.c_int(), ctypes.c_double()
+        self._check(self.lib.yg_gauge_load_hirep(self.h, str(path).encode(), ctypes.byref(nc_), ctypes.byref(pd)))
+        return nc_.value, pd.value
 
     def mre(self, max_, op, mass):
         """mre_init (mre.cpp:85-111): a history of up to max_ past solutions of `op`"""

@@ -291,6 +291,20 @@ int yg_cg_mixed(yg_lattice *l, const yg_inv_par *p, double *x, double *b, yg_sol
   });
 }
 
+// ---- gauge configuration files
+int yg_gauge_save_cfg(yg_lattice *l, const char *path, int num_cnfg, int num_accept) {
+  return guard([&] { need(path, "path"); yg::gauge_save_cfg(lat(l), path, num_cnfg, num_accept); });
+}
+int yg_gauge_load_cfg(yg_lattice *l, const char *path, int *num_cnfg, int *num_accept, double *plaq_diff) {
+  return guard([&] { need(path, "path"); yg::gauge_load_cfg(lat(l), path, num_cnfg, num_accept, plaq_diff); });
+}
+int yg_gauge_save_hirep(yg_lattice *l, const char *path) {
+  return guard([&] { need(path, "path"); yg::gauge_save_hirep(lat(l), path); });
+}
+int yg_gauge_load_hirep(yg_lattice *l, const char *path, int *num_cnfg, double *plaq_diff) {
+  return guard([&] { need(path, "path"); yg::gauge_load_hirep(lat(l), path, num_cnfg, plaq_diff); });
+}
+
 // ---- chronological initial guess
 struct yg_mre {
   yg::Mre *m;

@@ -457,6 +457,21 @@ __global__ void __launch_bounds__(64) k_update_links(double2 *U, const double *m
   for (int k = 0; k < N * N; k++) U[fidx(g, id, mu * N * N + k, 4 * N * N)] = u[k];
 }
 
+// apply_bcs_on_gauge_field alone (bcs.cpp:201-262): the boundary links take their fixed values
+template <int N>
+__global__ void __launch_bounds__(64) k_gauge_bcs(double2 *U, Geom g, SFLinks sf) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= 4L * g.V) return;
+  const int id = (int)(t >> 2), mu = (int)(t & 3);
+  int c[4];
+  coords_of(g, id, c);
+  double2 u[N * N];
+  if (gauge_bc<N>(u, g, c[0], mu, sf)) {
+#pragma unroll
+    for (int k = 0; k < N * N; k++) U[fidx(g, id, mu * N * N + k, 4 * N * N)] = u[k];
+  }
+}
+
 template <int N>
 __global__ void __launch_bounds__(64) k_reunitarize(double2 *U, Geom g) {
   long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -626,6 +641,14 @@ void update_links(Lattice &L, double eps) {
   const SFLinks sf = sf_links(L);
   YG_GAUGE_N(L.nc, k_update_links<GN><<<nblk(4L * L.V, 64), 64, 0, L.stream>>>(L.fund.as<double2>(),
                                                                                L.mom.as<double>(), L.g, eps, sf));
+  YG_LAUNCHED();
+}
+
+// apply_bcs_on_gauge_field, bcs.cpp:201-262 (nothing to do for periodic / antiperiodic)
+void apply_gauge_bcs(Lattice &L) {
+  if (L.p.bc != YG_BC_OPEN && L.p.bc != YG_BC_SF) return;
+  const SFLinks sf = sf_links(L);
+  YG_GAUGE_N(L.nc, k_gauge_bcs<GN><<<nblk(4L * L.V, 64), 64, 0, L.stream>>>(L.fund.as<double2>(), L.g, sf));
   YG_LAUNCHED();
 }
 

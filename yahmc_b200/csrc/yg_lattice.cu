@@ -391,6 +391,15 @@ void gauge_upload(Lattice &L, const double *host) {
   YG_CUDA(cudaStreamSynchronize(L.stream));
 }
 
+// as gauge_field_load does after reading (gaugefield.cpp:146-152): the links, then the
+// boundary conditions on them, then the represented field
+void gauge_upload_with_bcs(Lattice &L, const double *host) {
+  upload_records(L, L.fund, host, L.nc * L.nc, 4);
+  apply_gauge_bcs(L);
+  represent_and_clover(L);
+  YG_CUDA(cudaStreamSynchronize(L.stream));
+}
+
 void gauge_download(Lattice &L, double *host) { download_records(L, host, L.fund.p, L.nc * L.nc, 4); }
 void repr_download(Lattice &L, double *host) { download_records(L, host, L.links.p, L.d * L.d, 4); }
 

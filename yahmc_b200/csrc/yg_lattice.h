@@ -200,6 +200,13 @@ void momenta_gaussian(Lattice &L, unsigned long long seed);
 double momenta_action(Lattice &L);
 void gauge_backup(Lattice &L);
 void gauge_restore(Lattice &L);
+void apply_gauge_bcs(Lattice &L);
+void gauge_upload_with_bcs(Lattice &L, const double *host);
+// gauge configuration files (yg_gaugeio.cu)
+void gauge_save_cfg(Lattice &L, const char *path, int num_cnfg, int num_accept);
+void gauge_load_cfg(Lattice &L, const char *path, int *num_cnfg, int *num_accept, double *plaq_diff);
+void gauge_save_hirep(Lattice &L, const char *path);
+void gauge_load_hirep(Lattice &L, const char *path, int *num_cnfg, double *plaq_diff);
 
 // several cg_inverter solves sharing every operator application (yg_multi.cu)
 int cg_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, double *const *bs, int *iters);
