@@ -2,7 +2,8 @@
 
 Test infrastructure.  For each physics configuration below, every .cpp file of
 the reference's library/, library/monomials/ and checks/ directories is
-compiled, where it lies in the reference tree, with g++ -O3 -fopenmp and the
+compiled (with observables/propagator.cpp and observables/mesons.cpp), where it
+lies in the reference tree, with g++ -O3 -fopenmp and the
 compile-time switches of the reference's programs/Makefile:1-45 (NC, REPR_*,
 CLOVER_TERM, UPDATE_EO, BC_*; no MPI), then linked with oracle/ref_harness.cpp
 into ``oracle/_ref/libyahmc_ref_<name>.so``.  GSL (the reference's only
@@ -65,6 +66,7 @@ def _sources(src: Path) -> list[Path]:
     files = sorted((src / "library").glob("*.cpp"))
     files += sorted((src / "library" / "monomials").glob("*.cpp"))
     files += sorted((src / "checks").glob("*.cpp"))
+    files += [src / "observables" / "propagator.cpp", src / "observables" / "mesons.cpp"]
     return files
 
 

@@ -109,6 +109,9 @@ class RefLattice:
             "yref_update_links": [_D], "yref_reunitarize": [], "yref_represent_gauge_field": [],
             "yref_hamiltonian": [],
             "yref_gauge_save": [ctypes.c_char_p], "yref_gauge_load": [ctypes.c_char_p],
+            "yref_point_source": [_I, _I, _P], "yref_semwall_source": [_I, _I, _P],
+            "yref_calc_propagator": [_D, _D, _P, _P], "yref_rand_store": [_P], "yref_rand_load": [_P, _I], "yref_rand_uniform": [_I, _P],
+            "yref_mesons": [_D, _D, _I, _I, ctypes.c_char_p],
             "yref_gauge_save_hirep": [ctypes.c_char_p], "yref_gauge_load_hirep": [ctypes.c_char_p],
             "yref_mre_init": [_I, _I, _D], "yref_mre_store": [_P], "yref_mre_guess": [_P, _P], "yref_mre_reset": [],
             "yref_represent": [_P, _P, _I],
@@ -180,6 +183,38 @@ class RefLattice:
     def call(self, fn: str, *args):
         conv = [(_ptr(a) if isinstance(a, np.ndarray) else a) for a in args]
         return getattr(self.lib, "yref_" + fn)(*conv)
+
+
+def _parse_mesons(text):
+    taus, vals = [], {}
+    for line in text.splitlines():
+        if not line.startswith("[MESONS]"):
+            continue
+        body = line.split("]", 2)[2]
+        if "timeslice" in body:
+            taus.append(int(body.split()[-1]))
+        elif ": " in body:
+            lab, rest = body.split(": ", 1)
+            try:
+                vals[lab] = np.array([float(v) for v in rest.split()])
+            except ValueError:
+                pass
+    return taus, vals
+
+
+def mesons(R: "RefLattice", mass, prec, hits, method):
+    """The reference's meson_init + meson_measure (observables/mesons.cpp:150-298) on R's
+    current links.  Returns (source time slices, {label: printed values}) read from its log."""
+    import os
+    import tempfile
+    if getattr(R, "_meson_log", None) is None:
+        fd, R._meson_log = tempfile.mkstemp(prefix="yahmc_ref_mesons_")
+        os.close(fd)
+    off = os.path.getsize(R._meson_log)
+    R.call("mesons", mass, prec, hits, method, R._meson_log.encode())
+    with open(R._meson_log) as f:
+        f.seek(off)
+        return _parse_mesons(f.read())
 
 
 def get(name: str, dims=(8, 8, 8, 8), **kw) -> RefLattice:

@@ -38,6 +38,8 @@
 #include <bcs.h>
 #include <repr.h>
 #include <random.h>
+#include <spectrum.h>
+#include <logger.h>
 #include <rational.h>
 #include <staples.h>
 #include <wilsonloop.h>
@@ -401,6 +403,37 @@ void yref_represent_gauge_field(void) { represent_gauge_field(); }
 double yref_hamiltonian(void) { return hamiltonian(); }     /* no monomials: the momentum part */
 
 /* ---- gauge configuration files (gaugefield.cpp:44-179, hirep.cpp:56-212) ---- */
+/* ---- propagators and mesons (observables/propagator.cpp, observables/mesons.cpp) ---- */
+void yref_point_source(int n, int tau, double *out) { SpinorField f; wrap(f, out); create_point_source(n, tau, f); }
+void yref_semwall_source(int n, int tau, double *io) { SpinorField f; wrap(f, io); create_semwall_source(n, tau, f); }
+void yref_calc_propagator(double m, double prec, double *dst, double *src)
+{
+	SpinorField d, s;
+	wrap(d, dst);
+	wrap(s, src);
+	calc_propagator(m, prec, d, s);
+}
+/* the generator's state through the reference's rand_store / rand_load (random.cpp:36-46);
+ * rand_init may run only once per process (it registers an atexit free each time) */
+int yref_rand_store(void *buf) { return rand_store(buf); }
+void yref_rand_load(void *buf, int sz) { rand_load(buf, sz); }
+void yref_rand_uniform(int n, double *out) { for(int i = 0; i < n; i++) out[i] = rand_uniform(); }
+/* meson_init + meson_measure; the log (which carries the correlators) goes to `log`.
+ * logger_init registers an atexit fclose each time, so the first call's file is kept for
+ * the rest of the process and later calls append to it. */
+void yref_mesons(double mass, double prec, int hits, int method, const char *log)
+{
+	static int logger_on = 0;
+	if(!logger_on)
+	{
+		logger_init(log, INFO);
+		logger_on = 1;
+	}
+	meson_init(mass, prec, hits, method);
+	meson_measure();
+	fflush(NULL);
+}
+
 void yref_gauge_save(const char *path) { gauge_field_save(path); }
 void yref_gauge_load(const char *path) { gauge_field_load(path); }
 void yref_gauge_save_hirep(const char *path) { gauge_field_save_hirep(path); }

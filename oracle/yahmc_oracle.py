@@ -922,6 +922,103 @@ class Oracle:
             return it
         return self.bicgstab("Dphi", mass, prec, x, b)
 
+    # ---- observables/propagator.cpp
+    def create_point_source(self, n, tau):
+        """create_point_source, propagator.cpp:58-73: a unit source in spin n // d, colour
+        n % d at (tau, 0, 0, 0)."""
+        f = self.new_field()
+        f[self.index(tau, 0, 0, 0), n % self.d, n // self.d] = 1.0
+        return f
+
+    def timeslice_sites(self, tau):
+        """the site ids of time slice tau in increasing order (the sites_for order in which
+        create_semwall_source draws its noise)"""
+        return np.sort(np.nonzero(self.t == tau)[0])
+
+    def create_semwall_source(self, n, tau, f, z2=None):
+        """create_semwall_source, propagator.cpp:22-56.  n = 0: Z2 noise on spin 0 of slice
+        tau, z2[k, i] = (re, im) of colour i at the k-th slice site (rand_z2() values in the
+        reference's draw order); n > 0: spin n-1 moves to spin n."""
+        if n == 0:
+            f[:] = 0
+            z = np.asarray(z2, dtype=np.float64).reshape(-1, self.d, 2)
+            f[self.timeslice_sites(tau), :, 0] = z[..., 0] + 1j * z[..., 1]
+        else:
+            f[:, :, n] = f[:, :, n - 1]
+            f[:, :, n - 1] = 0
+
+    def calc_propagator(self, mass, prec, dst, src):
+        """calc_propagator, propagator.cpp:75-166: with even-odd preconditioning the even
+        system D x_e = b_e - D_eo D_oo^-1 b_o (clover) or (4+m) b_e - D_eo b_o (Wilson) is
+        solved by auto_inverter (BiCGstab on Dphi, dst as the initial guess) and the odd
+        sites follow from x_o = D_oo^-1 (b_o - D_oe x_e); without it, D x = b directly."""
+        if not self.p.eo:
+            return self.auto_inverter("Dphi", mass, prec, dst, src)
+        lo, hi = self.part_range(EVEN)
+        olo, ohi = self.part_range(ODD)
+        tmp, eo = self.new_field(), self.new_field()
+        if self.p.clover:
+            self.Dphi_oo_inv(mass, tmp, src)
+            self.Dphi_eo(tmp, tmp)
+            eo[lo:hi] = -1.0 * tmp[lo:hi]
+            eo[lo:hi] += src[lo:hi]
+            it = self.auto_inverter("Dphi", mass, prec, dst, eo)
+            self.Dphi_oe(tmp, dst)
+            dst[olo:ohi] = 1.0 * src[olo:ohi]
+            dst[olo:ohi] -= tmp[olo:ohi]
+            self.Dphi_oo_inv(mass, dst, dst)
+        else:
+            m4 = 4.0 + mass
+            self.Dphi_eo(tmp, src)
+            eo[lo:hi] = m4 * src[lo:hi]
+            eo[lo:hi] -= tmp[lo:hi]
+            it = self.auto_inverter("Dphi", mass, prec, dst, eo)
+            self.Dphi_oe(tmp, dst)
+            dst[olo:ohi] = (1.0 / m4) * src[olo:ohi]
+            dst[olo:ohi] -= (1.0 / m4) * tmp[olo:ohi]
+        return it
+
+    # ---- observables/mesons.cpp
+    def meson_measure(self, mass, prec, method, taus, noises=None, props=None):
+        """the hit loop of meson_measure, mesons.cpp:215-259, with the source time slices
+        (random_timeslice) and, for SEMWALL, each hit's z2 noise given.  The propagators
+        persist across hits as the solver's initial guesses, as the reference's static
+        prop[] do.  Returns the raw correlators (MESON_CHANNELS x T)."""
+        ninv = 4 if method == SEMWALL else 4 * self.d
+        if props is None:
+            props = [self.new_field() for _ in range(ninv)]
+        raw = np.zeros((len(MESON_CHANNELS), self.dims[0]))
+        source = self.new_field()
+        for h, tau in enumerate(taus):
+            for n in range(ninv):
+                if method == SEMWALL:
+                    self.create_semwall_source(n, tau, source, noises[h] if n == 0 else None)
+                else:
+                    source = self.create_point_source(n, tau)
+                self.calc_propagator(mass, prec, props[n], source)
+            raw += self.meson_contract(method, tau, props)
+        return raw
+
+    def meson_contract(self, method, tau, props):
+        """contract_all_correlators, mesons.cpp:55-128: raw[ch, (t - tau) mod T] summed over
+        the sites of each slice, channels in MESON_CHANNELS order.  props: 4 (SEMWALL,
+        prop[A] for source spin A) or 4d (POINT, prop[c*d + x] for source spin c, colour x)
+        fields.  Per site, Re sum_{a,c} v1[a] v2[c] sum_{x,y} P[c,x](col1[a], y) conj(P[col2[c],x](a, y))."""
+        ns = 1 if method == SEMWALL else self.d
+        P = np.stack(props).reshape(4, ns, self.V, self.d, 4)
+        T = self.dims[0]
+        trel = (self.t - tau + T) % T
+        out = np.zeros((len(MESON_CHANNELS), T))
+        for k, (g1, g2) in enumerate(MESON_PAIRS):
+            c1, v1 = MESON_GAMMA[g1]
+            c2, v2 = MESON_GAMMA[g2]
+            site = np.zeros(self.V, dtype=complex)
+            for a in range(4):
+                for c in range(4):
+                    site += v1[a] * v2[c] * np.einsum("xvy,xvy->v", P[c, :, :, :, c1[a]], np.conj(P[c2[c], :, :, :, a]))
+            out[k] = np.bincount(trel, weights=site.real, minlength=T)
+        return out
+
     # ---- forces.cpp
     @staticmethod
     def fmat_create(a_lhs, a_rhs, b_lhs, b_rhs):
@@ -1272,6 +1369,46 @@ class Oracle:
 # ---------------------------------------------------------------- gauge configuration files
 # gaugefield.cpp:44-179 (CFG, native byte order) and hirep.cpp:56-212 (HiRep, big-endian).
 # U is (V, 4, N, N) complex in the even-odd site order; files run over t, x, y, z.
+# ---- meson channels, observables/mesons.cpp:12-27 and include/spectrum.h:7-13.  Each
+# g5*Gamma is a signed spin permutation: row a has its one entry val[a] in column col[a].
+SEMWALL, POINT = 0x01, 0x02
+_I1 = 1j
+MESON_GAMMA = {
+    "ID": ((0, 1, 2, 3), (1, 1, -1, -1)),
+    "G1": ((3, 2, 1, 0), (-_I1, -_I1, -_I1, -_I1)),
+    "G2": ((3, 2, 1, 0), (-1, 1, -1, 1)),
+    "G3": ((2, 3, 0, 1), (-_I1, _I1, -_I1, _I1)),
+    "G5": ((0, 1, 2, 3), (1, 1, 1, 1)),
+    "G5G1": ((3, 2, 1, 0), (-_I1, -_I1, _I1, _I1)),
+    "G5G2": ((3, 2, 1, 0), (-1, 1, 1, -1)),
+    "G5G3": ((2, 3, 0, 1), (-_I1, _I1, _I1, -_I1)),
+    "G0G1": ((1, 0, 3, 2), (-_I1, -_I1, -_I1, -_I1)),
+    "G0G2": ((1, 0, 3, 2), (-1, 1, -1, 1)),
+    "G0G3": ((0, 1, 2, 3), (-_I1, _I1, -_I1, _I1)),
+    "G0G5": ((2, 3, 0, 1), (1, 1, 1, 1)),
+    "G0G5G1": ((1, 0, 3, 2), (_I1, _I1, -_I1, -_I1)),
+    "G0G5G2": ((1, 0, 3, 2), (1, -1, -1, 1)),
+    "G0G5G3": ((0, 1, 2, 3), (_I1, -_I1, -_I1, _I1)),
+}
+MESON_CHANNELS = ("id", "g1", "g2", "g3", "g5", "g5g1", "g5g2", "g5g3", "g0g1", "g0g2", "g0g3", "g0g5",
+                  "g0g5g1", "g0g5g2", "g0g5g3", "g5_g0g5")
+MESON_PAIRS = tuple((c.upper(), c.upper()) for c in MESON_CHANNELS[:15]) + (("G0G5", "G5"),)
+# meson_measure's print list, mesons.cpp:280-295: (label, printed channel, sign).  As in the
+# reference, "g0g5g1" prints the g0g5g2 correlator and "g0g5g2" the g0g5g3 one.
+MESON_PRINT = (("id", "id", -1.0), ("g1", "g1", -1.0), ("g2", "g2", -1.0), ("g3", "g3", -1.0), ("g5", "g5", 1.0),
+               ("g5g1", "g5g1", -1.0), ("g5g2", "g5g2", -1.0), ("g5g3", "g5g3", -1.0), ("g0g1", "g0g1", -1.0),
+               ("g0g2", "g0g2", -1.0), ("g0g3", "g0g3", -1.0), ("g0g5", "g0g5", 1.0), ("g0g5g1", "g0g5g2", 1.0),
+               ("g0g5g2", "g0g5g3", 1.0), ("g0g5g3", "g0g5g3", 1.0), ("g5_g0g5", "g5_g0g5", 1.0))
+
+
+def meson_print_values(raw, method, hits, vol3):
+    """{label: values} as meson_measure prints them (print_correlator, mesons.cpp:131-148):
+    sign / (norm * hits) with norm = vol3 for SEMWALL and 1 for POINT."""
+    norm = vol3 if method == SEMWALL else 1
+    idx = {c: k for k, c in enumerate(MESON_CHANNELS)}
+    return {lab: sign / (norm * hits) * np.asarray(raw[idx[ch]]) for lab, ch, sign in MESON_PRINT}
+
+
 CFG_IDENT, CFG_VERSION = 0x47464359, 0x20          # include/gaugefield.h:20-21
 _CFG_HEADER = np.dtype([("ident", "<i4"), ("version", "<i4"), ("dim_t", "<i4"), ("dim_x", "<i4"),
                         ("dim_y", "<i4"), ("dim_z", "<i4"), ("nc", "<i4"), ("repr", "<i4"),

@@ -239,3 +239,73 @@ def test_gauge_files(name, tmp_path):
     yo.hirep_write(q, W, DIMS, nc, 0.25)
     R.call("gauge_load_hirep", str(q).encode())
     assert np.array_equal(yo.mat_from_raw(R.get_links(), nc).reshape(O.V, 4, nc, nc), O.fund)
+
+
+@pytest.mark.parametrize("name,method", [("su3_fund_ap", yo.POINT), ("su3_fund_ap", yo.SEMWALL),
+                                         ("su3_fund_open", yo.POINT), ("su3_fund_ap_nocl", yo.POINT),
+                                         ("su2_adj_ap", yo.SEMWALL), ("su3_fund_ap_full", yo.SEMWALL)])
+def test_mesons(name, method):
+    """meson_init + meson_measure (mesons.cpp:150-298, with create_*_source and
+    calc_propagator of propagator.cpp): the oracle's correlators against the ones the
+    reference prints (%1.6e, so to half a unit in the 7th digit).  The source time slices
+    are read from its log; the semwall noise is the reference's own stream, replayed with
+    rand_store / rand_load."""
+    R, O, rng, src = _setup(name, 10)
+    hits = 1 if method == yo.POINT else 2
+    state = np.zeros(512)
+    sz = R.call("rand_store", state)
+    taus, printed = ref.mesons(R, -0.3, 1e-24, hits, method)
+    assert len(taus) == hits and len(printed) == 16
+    noises = None
+    if method == yo.SEMWALL:
+        R.call("rand_load", state, sz)
+        vol3, noises, replay = O.V // DIMS[0], [], []
+        for _ in range(hits):
+            if O.p.bc in ("open", "sf"):
+                replay.append(1)                     # random_timeslice, propagator.cpp:10-19
+            else:
+                u = np.zeros(1)
+                R.call("rand_uniform", 1, u)
+                replay.append(int(u[0] * DIMS[0]))
+            u = np.zeros(2 * O.d * vol3)
+            R.call("rand_uniform", len(u), u)
+            noises.append(np.where(u < 0.5, 2 ** -0.5, -2 ** -0.5))
+        assert replay == taus
+    raw = O.meson_measure(-0.3, 1e-24, method, taus, noises)
+    mine = yo.meson_print_values(raw, method, hits, O.V // DIMS[0])
+    for lab, v in printed.items():
+        scale = np.abs(v).max()
+        assert np.all(np.abs(mine[lab] - v) <= 5.01e-7 * np.abs(v) + 1e-12 * scale), lab
+
+
+@pytest.mark.parametrize("name", ["su3_fund_ap", "su3_fund_ap_nocl", "su3_fund_ap_full", "su2_adj_ap"])
+def test_sources_and_propagator(name):
+    """create_point_source, create_semwall_source (noise order = the reference's draw order)
+    and calc_propagator at full precision."""
+    R, O, rng, src = _setup(name, 11)
+    d = O.d
+    for n in (0, d + 1, 4 * d - 1):
+        r = np.zeros(O.V * 8 * d)
+        R.call("point_source", n, 3, r)
+        assert np.array_equal(yo.spinor_from_raw(r, d), O.create_point_source(n, 3))
+    state = np.zeros(512)
+    sz = R.call("rand_store", state)
+    f = np.zeros(O.V * 8 * d)
+    R.call("semwall_source", 0, 5, f)
+    R.call("rand_load", state, sz)
+    u = np.zeros(2 * d * (O.V // DIMS[0]))
+    R.call("rand_uniform", len(u), u)
+    fo = O.new_field()
+    O.create_semwall_source(0, 5, fo, np.where(u < 0.5, 2 ** -0.5, -2 ** -0.5))
+    assert np.array_equal(yo.spinor_from_raw(f, d), fo)
+    for n in (1, 2, 3):
+        R.call("semwall_source", n, 5, f)
+        O.create_semwall_source(n, 5, fo)
+        assert np.array_equal(yo.spinor_from_raw(f, d), fo)
+    x0 = 0.01 * fields.gaussian_spinor(O.V, d, rng)
+    dr, sr = yo.spinor_to_raw(x0).copy(), yo.spinor_to_raw(src).copy()
+    R.call("calc_propagator", -0.3, 1e-24, dr, sr)
+    do, so = x0.copy(), src.copy()
+    O.calc_propagator(-0.3, 1e-24, do, so)
+    assert _rel(yo.spinor_from_raw(dr, d), do) < 1e-12
+    assert np.array_equal(yo.spinor_from_raw(sr, d), so)
