@@ -227,6 +227,27 @@ typedef struct {
 int yg_cg_mixed_opts(yg_lattice *lat, const yg_inv_par *par, const yg_mixed_opts *opts, double *x, double *b,
                      yg_solve_stats *stats);
 
+/* ---- propagators and mesons (observables/propagator.cpp, observables/mesons.cpp) ---- */
+enum { YG_MESON_SEMWALL = 0x01, YG_MESON_POINT = 0x02 };   /* include/spectrum.h:7-8 */
+/* create_point_source (propagator.cpp:58-73): src = unit vector of spin n / d, colour n % d
+ * at (tau, 0, 0, 0) */
+int yg_create_point_source(yg_lattice *lat, int n, int tau, double *src);
+/* create_semwall_source (propagator.cpp:22-56).  For n = 0, z2 holds the 2*d*vol3 rand_z2()
+ * values in the reference's draw order: the sites of slice tau by increasing site index, per
+ * site re, im of colour 0..d-1 (a shim that draws them with the reference's generator
+ * reproduces its sources exactly); z2 is ignored for n > 0 (spin n-1 moves to spin n). */
+int yg_create_semwall_source(yg_lattice *lat, int n, int tau, const double *z2, double *src);
+/* calc_propagator (propagator.cpp:75-166): dst holds the initial guess */
+int yg_calc_propagator(yg_lattice *lat, double mass, double prec, double *dst, double *src, int *iters);
+/* No reference counterpart: n <= 16 propagators of one source slice through the batched CG
+ * (mixed = 1: FP32 inner iterations, d = 3), same stopping rule; dst[i] need no initial guess */
+int yg_calc_propagator_multi(yg_lattice *lat, double mass, double prec, int n, double *const *dst,
+                             double *const *src, int mixed, int *iters);
+/* contract_all_correlators (mesons.cpp:105-128): corr[16*T] += the slice sums of the sixteen
+ * channels (order id g1 g2 g3 g5 g5g1 g5g2 g5g3 g0g1 g0g2 g0g3 g0g5 g0g5g1 g0g5g2 g0g5g3
+ * g5_g0g5) at t - tau; props: 4 (SEMWALL) or 4*d (POINT, index spin*d + colour) fields */
+int yg_meson_contract(yg_lattice *lat, int method, int tau, const double *const *props, int nprops, double *corr);
+
 /* ---- gauge configuration files (gaugefield.cpp:44-179, hirep.cpp:56-212) ---- */
 /* CFG: 256-byte header (ident, version, dims, nc, repr, num_cnfg, num_accept, plaquette),
  * HiRep: big-endian (N, T, X, Y, Z, plaquette); both then every site's four links in

@@ -107,6 +107,9 @@ _SIGNATURES = {
     "yg_inner_hop_profile": [_P, _D, _I, _P, _P],
     "yg_mre_init": [_P, _I, _I, _D, _P], "yg_mre_store": [_P, _P], "yg_mre_guess": [_P, _P, _P],
     "yg_mre_reset": [_P], "yg_mre_free": [_P],
+    "yg_create_point_source": [_P, _I, _I, _P], "yg_create_semwall_source": [_P, _I, _I, _P, _P],
+    "yg_calc_propagator": [_P, _D, _D, _P, _P, _P], "yg_calc_propagator_multi": [_P, _D, _D, _I, _P, _P, _I, _P],
+    "yg_meson_contract": [_P, _I, _I, _P, _I, _P],
     "yg_gauge_save_cfg": [_P, ctypes.c_char_p, _I, _I], "yg_gauge_load_cfg": [_P, ctypes.c_char_p, _P, _P, _P],
     "yg_gauge_save_hirep": [_P, ctypes.c_char_p], "yg_gauge_load_hirep": [_P, ctypes.c_char_p, _P, _P],
     "yg_momenta_upload": [_P, _P], "yg_momenta_download": [_P, _P], "yg_momenta_zero": [_P],
@@ -408,6 +411,56 @@ class Lattice:
         if rc not in (0, 4):
             self._check(rc)
         return list(its)
+
+    # ---- sources, propagators, meson contractions (observables/propagator.cpp, mesons.cpp)
+    def create_point_source(self, n, tau, src):
+        self._check(self.lib.yg_create_point_source(self.h, int(n), int(tau), src.ptr))
+
+    def create_semwall_source(self, n, tau, src, z2=None):
+        """z2: for n = 0, the 2*d*vol3 rand_z2 values (slice sites by increasing index, per site
+        re, im of each colour)"""
+        zp = None
+        if n == 0:
+            z2 = np.ascontiguousarray(z2, dtype=np.float64)
+            vol3 = self.V // self.dims[0]
+            if z2.size != 2 * self.d * vol3:
+                raise ValueError(f"z2 needs {2 * self.d * vol3} values")
+            zp = _ptr(z2)
+        self._check(self.lib.yg_create_semwall_source(self.h, int(n), int(tau), zp, src.ptr))
+
+    def calc_propagator(self, mass, prec, dst, src):
+        """calc_propagator; dst holds the initial guess.  Returns the solver's iterations."""
+        it = ctypes.c_int()
+        rc = self.lib.yg_calc_propagator(self.h, mass, prec, dst.ptr, src.ptr, ctypes.byref(it))
+        self.last_status = rc
+        if rc not in (0, 4):
+            self._check(rc)
+        return it.value
+
+    def calc_propagator_multi(self, mass, prec, dsts, srcs, mixed=False):
+        """len(dsts) <= 16 propagators through the batched CG; returns the iteration counts"""
+        n = len(dsts)
+        if n != len(srcs):
+            raise ValueError("dsts and srcs differ in length")
+        pd = (ctypes.c_void_p * n)(*[x.ptr for x in dsts])
+        ps = (ctypes.c_void_p * n)(*[b.ptr for b in srcs])
+        its = (ctypes.c_int * n)()
+        rc = self.lib.yg_calc_propagator_multi(self.h, mass, prec, n, pd, ps, int(bool(mixed)), its)
+        self.last_status = rc
+        if rc not in (0, 4):
+            self._check(rc)
+        return list(its)
+
+    def meson_contract(self, method, tau, props, corr=None):
+        """adds the sixteen slice-summed channels of one source slice to corr (16 x T)"""
+        T = self.dims[0]
+        if corr is None:
+            corr = np.zeros((16, T))
+        if corr.shape != (16, T) or corr.dtype != np.float64 or not corr.flags.c_contiguous:
+            raise ValueError("corr must be a C-contiguous float64 (16, T) array")
+        pp = (ctypes.c_void_p * len(props))(*[f.ptr for f in props])
+        self._check(self.lib.yg_meson_contract(self.h, int(method), int(tau), pp, len(props), _ptr(corr)))
+        return corr
 
     # ---- gauge configuration files (gaugefield.cpp:44-179, hirep.cpp:56-212)
     def gauge_field_save(self, path, num_cnfg=0, num_accept=0):

@@ -2,6 +2,7 @@
 // conversion, and the thin mapping onto the engine functions.
 #include <cstdio>
 #include <string>
+#include <vector>
 #include "yg_lattice.h"
 
 using yg::Error;
@@ -289,6 +290,37 @@ int yg_cg_mixed(yg_lattice *l, const yg_inv_par *p, double *x, double *b, yg_sol
     }
     return yg::cg_mixed(L, *p, x, b, st);
   });
+}
+
+// ---- propagators and mesons
+int yg_create_point_source(yg_lattice *l, int n, int tau, double *src) {
+  return guard([&] { need(src, "src"); yg::create_point_source(lat(l), n, tau, src); });
+}
+int yg_create_semwall_source(yg_lattice *l, int n, int tau, const double *z2, double *src) {
+  return guard([&] { need(src, "src"); yg::create_semwall_source(lat(l), n, tau, z2, src); });
+}
+int yg_calc_propagator(yg_lattice *l, double mass, double prec, double *dst, double *src, int *iters) {
+  return guard_status([&] {
+    need(dst, "dst"); need(src, "src");
+    int it = 0;
+    const int st = yg::calc_propagator(lat(l), mass, prec, dst, src, &it);
+    if (iters) *iters = it;
+    return st;
+  });
+}
+int yg_calc_propagator_multi(yg_lattice *l, double mass, double prec, int n, double *const *dst, double *const *src,
+                             int mixed, int *iters) {
+  return guard_status([&] {
+    need(dst, "dst"); need(src, "src");
+    std::vector<int> it(n > 0 ? n : 1, 0);
+    const int st = yg::calc_propagator_multi(lat(l), mass, prec, n, dst, src, mixed != 0, it.data());
+    if (iters)
+      for (int i = 0; i < n; i++) iters[i] = it[i];
+    return st;
+  });
+}
+int yg_meson_contract(yg_lattice *l, int method, int tau, const double *const *props, int nprops, double *corr) {
+  return guard([&] { need(props, "props"); need(corr, "corr"); yg::meson_contract(lat(l), method, tau, props, nprops, corr); });
 }
 
 // ---- gauge configuration files

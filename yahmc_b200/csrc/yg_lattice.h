@@ -208,6 +208,14 @@ void gauge_load_cfg(Lattice &L, const char *path, int *num_cnfg, int *num_accept
 void gauge_save_hirep(Lattice &L, const char *path);
 void gauge_load_hirep(Lattice &L, const char *path, int *num_cnfg, double *plaq_diff);
 
+// sources, propagators and meson contractions (yg_mesons.cu)
+void create_point_source(Lattice &L, int n, int tau, double *src);
+void create_semwall_source(Lattice &L, int n, int tau, const double *z2, double *src);
+int calc_propagator(Lattice &L, double mass, double prec, double *dst, double *src, int *iters);
+int calc_propagator_multi(Lattice &L, double mass, double prec, int n, double *const *dst, double *const *src,
+                          bool mixed, int *iters);
+void meson_contract(Lattice &L, int method, int tau, const double *const *props, int nprops, double *corr);
+
 // several cg_inverter solves sharing every operator application (yg_multi.cu)
 int cg_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, double *const *bs, int *iters);
 // the same systems with FP32 inner iterations and FP64 reliable updates (yg_multi.cu)
