@@ -248,6 +248,24 @@ int yg_calc_propagator_multi(yg_lattice *lat, double mass, double prec, int n, d
  * g5_g0g5) at t - tau; props: 4 (SEMWALL) or 4*d (POINT, index spin*d + colour) fields */
 int yg_meson_contract(yg_lattice *lat, int method, int tau, const double *const *props, int nprops, double *corr);
 
+/* ---- Wilson and fermion flow (observables/wilsonflow.cpp, observables/fermionflow.cpp) ---- */
+/* wf_init (wilsonflow.cpp:149-157): zero the flow's momentum field (the MD momenta) */
+int yg_wf_init(yg_lattice *lat);
+/* wf_zeta (wilsonflow.cpp:8-23) and wf_update (wilsonflow.cpp:25-41), the two halves of a stage */
+int yg_wf_zeta(yg_lattice *lat, double alpha);
+int yg_wf_update(yg_lattice *lat, double val);
+/* wf_iterate (wilsonflow.cpp:43-53): one third-order Runge-Kutta step of the Wilson flow.
+ * Like the reference it changes the fundamental links only: call yg_represent_gauge_field
+ * before applying a Dirac operator to the flowed field. */
+int yg_wf_iterate(yg_lattice *lat, double eps);
+/* wf_e_plaq, wf_e_sym, wf_charge (wilsonflow.cpp:55-147) from one pass; any pointer may be NULL */
+int yg_wf_observables(yg_lattice *lat, double *e_plaq, double *e_sym, double *charge);
+/* wf_fermion_init (fermionflow.cpp:76-92) for n <= 32 fields, and wf_fermion_iterate
+ * (fermionflow.cpp:28-74): one step of the gauge flow with the n fields phi[i] flowed in place
+ * (pass the same fields, in the same order, at every step) */
+int yg_wf_fermion_init(yg_lattice *lat, int n);
+int yg_wf_fermion_iterate(yg_lattice *lat, double eps, double *const *phi, int n);
+
 /* ---- gauge configuration files (gaugefield.cpp:44-179, hirep.cpp:56-212) ---- */
 /* CFG: 256-byte header (ident, version, dims, nc, repr, num_cnfg, num_accept, plaquette),
  * HiRep: big-endian (N, T, X, Y, Z, plaquette); both then every site's four links in

@@ -2,7 +2,8 @@
 
 Test infrastructure.  For each physics configuration below, every .cpp file of
 the reference's library/, library/monomials/ and checks/ directories is
-compiled (with observables/propagator.cpp and observables/mesons.cpp), where it
+compiled (with observables/propagator.cpp, mesons.cpp, wilsonflow.cpp and
+fermionflow.cpp), where it
 lies in the reference tree, with g++ -O3 -fopenmp and the
 compile-time switches of the reference's programs/Makefile:1-45 (NC, REPR_*,
 CLOVER_TERM, UPDATE_EO, BC_*; no MPI), then linked with oracle/ref_harness.cpp
@@ -66,7 +67,7 @@ def _sources(src: Path) -> list[Path]:
     files = sorted((src / "library").glob("*.cpp"))
     files += sorted((src / "library" / "monomials").glob("*.cpp"))
     files += sorted((src / "checks").glob("*.cpp"))
-    files += [src / "observables" / "propagator.cpp", src / "observables" / "mesons.cpp"]
+    files += [src / "observables" / n for n in ("propagator.cpp", "mesons.cpp", "wilsonflow.cpp", "fermionflow.cpp")]
     return files
 
 

@@ -112,6 +112,8 @@ class RefLattice:
             "yref_point_source": [_I, _I, _P], "yref_semwall_source": [_I, _I, _P],
             "yref_calc_propagator": [_D, _D, _P, _P], "yref_rand_store": [_P], "yref_rand_load": [_P, _I], "yref_rand_uniform": [_I, _P],
             "yref_mesons": [_D, _D, _I, _I, ctypes.c_char_p],
+            "yref_wf_init": [], "yref_wf_zeta": [_D], "yref_wf_update": [_D], "yref_wf_iterate": [_D],
+            "yref_wf_observables": [_P], "yref_wf_fermion_init": [_P, _I], "yref_wf_fermion_iterate": [_D],
             "yref_gauge_save_hirep": [ctypes.c_char_p], "yref_gauge_load_hirep": [ctypes.c_char_p],
             "yref_mre_init": [_I, _I, _D], "yref_mre_store": [_P], "yref_mre_guess": [_P, _P], "yref_mre_reset": [],
             "yref_represent": [_P, _P, _I],

@@ -39,6 +39,7 @@
 #include <repr.h>
 #include <random.h>
 #include <spectrum.h>
+#include <wilsonflow.h>
 #include <logger.h>
 #include <rational.h>
 #include <staples.h>
@@ -433,6 +434,21 @@ void yref_mesons(double mass, double prec, int hits, int method, const char *log
 	meson_measure();
 	fflush(NULL);
 }
+
+/* ---- Wilson and fermion flow (observables/wilsonflow.cpp, observables/fermionflow.cpp) ---- */
+void yref_wf_init(void) { wf_init(); }
+void yref_wf_zeta(double a) { wf_zeta(a); }
+void yref_wf_update(double v) { wf_update(v); }
+void yref_wf_iterate(double eps) { wf_iterate(eps); }
+void yref_wf_observables(double *out) { out[0] = wf_e_plaq(); out[1] = wf_e_sym(); out[2] = wf_charge(); }
+/* the flowed fields wrap the caller's buffers, which must outlive the iterate calls */
+static SpinorField wf_fields[32];
+void yref_wf_fermion_init(double **ptrs, int n)
+{
+	for(int i = 0; i < n; i++) wrap(wf_fields[i], ptrs[i]);
+	wf_fermion_init(wf_fields, n);
+}
+void yref_wf_fermion_iterate(double eps) { wf_fermion_iterate(eps); }
 
 void yref_gauge_save(const char *path) { gauge_field_save(path); }
 void yref_gauge_load(const char *path) { gauge_field_load(path); }

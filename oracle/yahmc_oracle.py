@@ -1344,6 +1344,121 @@ class Oracle:
             self.fund[self.t == T - 2, 1:] = c2
             self.fund[self.t == T - 1] = 0
 
+    # ---- observables/wilsonflow.cpp
+    def wf_init(self):
+        """wilsonflow.cpp:149-157"""
+        self.mom[:] = 0
+
+    def wf_zeta(self, alpha):
+        """wilsonflow.cpp:8-23: P -= algebra_project(U staple, alpha)"""
+        for mu in range(4):
+            f = self.fund[:, mu] @ self.staples_wilson(mu)
+            self.mom[:, mu] -= algebra_project(f, self.itfund, alpha)
+
+    def wf_update(self, val):
+        """wilsonflow.cpp:25-41: U <- exp(P) U, P <- val P, then the link boundary values"""
+        self.fund = exp_algebra(self.nc, self.mom, 1.0) @ self.fund
+        self.mom *= val
+        self.bcs_on_gauge()
+
+    def wf_iterate(self, eps):
+        """wilsonflow.cpp:43-53"""
+        self.wf_zeta(eps / 4.0)
+        self.wf_update(-17.0 / 9.0)
+        self.wf_zeta(8.0 * eps / 9.0)
+        self.wf_update(-1.0)
+        self.wf_zeta(3.0 * eps / 4.0)
+        self.wf_update(0.0)
+
+    def clover_fund(self, mu, nu):
+        """clover_fund(id,mu,nu), wilsonloop.cpp:33-54: the four leaves, unrepresented"""
+        U, x = self.fund, np.arange(self.V)
+        a, b = self.fw[x, mu], self.fw[x, nu]
+        r = U[x, mu] @ U[a, nu] @ dagger(U[x, nu] @ U[b, mu])
+        a = self.bk[x, mu]
+        b = self.fw[a, nu]
+        r = r + U[x, nu] @ dagger(U[a, nu] @ U[b, mu]) @ U[a, mu]
+        a, b = self.bk[x, mu], self.bk[x, nu]
+        c = self.bk[a, nu]
+        r = r + dagger(U[c, nu] @ U[a, mu]) @ U[c, mu] @ U[b, nu]
+        a = self.bk[x, nu]
+        b = self.fw[a, mu]
+        return r + dagger(U[a, nu]) @ U[a, mu] @ U[b, nu] @ dagger(U[x, mu])
+
+    def wf_e_plaq(self):
+        """wilsonflow.cpp:55-74: 2/V sum_x sum_{mu>nu} (N - weighted Re tr P)"""
+        s = 0.0
+        for mu in range(1, 4):
+            for nu in range(mu):
+                s += np.sum(self.nc - self.wilson_loop(mu, nu, 1, 1))
+        return 2 * s / self.V
+
+    def wf_e_sym(self):
+        """wilsonflow.cpp:76-101"""
+        norm = math.sqrt(2.0 * TF)
+        s = 0.0
+        for mu in range(1, 4):
+            for nu in range(mu):
+                s += np.sum(algebra_project(self.clover_fund(mu, nu), self.itfund, norm) ** 2)
+        return 2 * s / (16 * 4 * self.V)
+
+    def wf_charge(self):
+        """wilsonflow.cpp:103-147"""
+        norm = math.sqrt(2.0 * TF)
+        tc = 0.0
+        for (m1, n1), (m2, n2) in (((0, 3), (1, 2)), ((0, 2), (3, 1)), ((0, 1), (2, 3))):
+            a1 = algebra_project(self.clover_fund(m1, n1), self.itfund, norm)
+            a2 = algebra_project(self.clover_fund(m2, n2), self.itfund, norm)
+            tc += np.sum(a1 * a2)
+        return 2 * tc / (16 * 16 * math.pi * math.pi)
+
+    # ---- observables/fermionflow.cpp
+    def wf_laplacian(self, src):
+        """fermionflow.cpp:11-26: -8 s(x) + sum_mu U(x,mu) s(x+mu) + U(x-mu,mu)^dag s(x-mu),
+        represented links (with the antiperiodic sign), every site"""
+        x = np.arange(self.V)
+        out = -8.0 * src
+        for mu in range(4):
+            fw, bk = self.fw[x, mu], self.bk[x, mu]
+            out = out + np.einsum("vij,vjs->vis", self.links[x, mu], src[fw])
+            out = out + np.einsum("vji,vjs->vis", np.conj(self.links[bk, mu]), src[bk])
+        return out
+
+    def wf_fermion_init(self, phis):
+        """fermionflow.cpp:76-92: phis are flowed in place"""
+        self.wf_phi0 = phis
+        self.wf_phi1 = [self.new_field() for _ in phis]
+        self.wf_phi2 = [self.new_field() for _ in phis]
+        self.wf_init()
+
+    def wf_fermion_iterate(self, eps):
+        """fermionflow.cpp:28-74; spinor_copy copies whole fields (linalg.cpp:71-76), the
+        other vector updates cover the default view, as the reference's spinor_* calls do"""
+        lo, hi = self.default_range()
+        p0, p1, p2 = self.wf_phi0, self.wf_phi1, self.wf_phi2
+        self.represent_gauge_field()
+        for i in range(len(p0)):
+            d = self.wf_laplacian(p0[i])
+            p1[i][:] = p0[i]
+            p1[i][lo:hi] += (eps / 4.0) * d[lo:hi]
+        self.wf_zeta(eps / 4.0)
+        self.wf_update(-17.0 / 9.0)
+        self.represent_gauge_field()
+        for i in range(len(p0)):
+            d = self.wf_laplacian(p1[i])
+            p2[i][lo:hi] = (-8.0 / 9.0) * p1[i][lo:hi]
+            p2[i][lo:hi] += (17.0 / 9.0) * p0[i][lo:hi]
+            p2[i][lo:hi] += (8.0 * eps / 9.0) * d[lo:hi]
+        self.wf_zeta(8.0 * eps / 9.0)
+        self.wf_update(-1.0)
+        self.represent_gauge_field()
+        for i in range(len(p0)):
+            d = self.wf_laplacian(p2[i])
+            p0[i][:] = p1[i]
+            p0[i][lo:hi] += (3.0 * eps / 4.0) * d[lo:hi]
+        self.wf_zeta(3.0 * eps / 4.0)
+        self.wf_update(0.0)
+
     def update_links(self, eps):
         """update.cpp:228-247: U <- exp(eps P) U with the boundary conditions.  As there, the
         represented field is rebuilt only by represent_gauge_field()."""

@@ -309,3 +309,44 @@ def test_sources_and_propagator(name):
     O.calc_propagator(-0.3, 1e-24, do, so)
     assert _rel(yo.spinor_from_raw(dr, d), do) < 1e-12
     assert np.array_equal(yo.spinor_from_raw(sr, d), so)
+
+
+@pytest.mark.parametrize("name", ["su3_fund_ap", "su3_fund_open", "su3_fund_sf", "su2_adj_ap", "su3_fund_ap_full",
+                                  "su4_fund_ap"])
+def test_wilson_flow(name):
+    """wf_iterate, wf_e_plaq, wf_e_sym, wf_charge (wilsonflow.cpp) and wf_fermion_iterate
+    (fermionflow.cpp) on a smooth field: links, observables and flowed fields to rounding."""
+    R, O, rng, src = _setup(name, 12)
+    nc = O.nc
+    U = yo.exp_algebra(nc, rng.normal(0, 0.5, (O.V, 4, nc * nc - 1)), 1.0)
+    O.fund = U
+    O.bcs_on_gauge()
+    U = O.fund.copy()
+    R.set_links(fields.complex_to_raw(U))
+    O.set_links(U)
+
+    def check_obs():
+        r = np.zeros(3)
+        R.call("wf_observables", r)
+        o = np.array([O.wf_e_plaq(), O.wf_e_sym(), O.wf_charge()])
+        assert np.all(np.abs(r - o) < 1e-12 * np.maximum(np.abs(o), 1.0)), (r, o)
+
+    check_obs()
+    R.call("wf_init")
+    O.wf_init()
+    for _ in range(2):
+        R.call("wf_iterate", 0.02)
+        O.wf_iterate(0.02)
+    assert _rel(yo.mat_from_raw(R.get_links(), nc).reshape(O.V, 4, nc, nc), O.fund) < 1e-13
+    check_obs()
+    phis = [fields.gaussian_spinor(O.V, O.d, rng) for _ in range(2)]
+    raws = [yo.spinor_to_raw(p).copy() for p in phis]
+    ptrs = np.array([r.ctypes.data for r in raws], dtype=np.uint64)
+    R.lib.yref_wf_fermion_init(ptrs.ctypes.data_as(ref.ctypes.c_void_p), 2)
+    O.wf_fermion_init(phis)
+    for _ in range(2):
+        R.call("wf_fermion_iterate", 0.02)
+        O.wf_fermion_iterate(0.02)
+    for r, p in zip(raws, phis):
+        assert _rel(yo.spinor_from_raw(r, O.d), p) < 1e-13
+    assert _rel(yo.mat_from_raw(R.get_links(), nc).reshape(O.V, 4, nc, nc), O.fund) < 1e-13

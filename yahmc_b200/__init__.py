@@ -110,6 +110,8 @@ _SIGNATURES = {
     "yg_create_point_source": [_P, _I, _I, _P], "yg_create_semwall_source": [_P, _I, _I, _P, _P],
     "yg_calc_propagator": [_P, _D, _D, _P, _P, _P], "yg_calc_propagator_multi": [_P, _D, _D, _I, _P, _P, _I, _P],
     "yg_meson_contract": [_P, _I, _I, _P, _I, _P],
+    "yg_wf_init": [_P], "yg_wf_zeta": [_P, _D], "yg_wf_update": [_P, _D], "yg_wf_iterate": [_P, _D],
+    "yg_wf_observables": [_P, _P, _P, _P], "yg_wf_fermion_init": [_P, _I], "yg_wf_fermion_iterate": [_P, _D, _P, _I],
     "yg_gauge_save_cfg": [_P, ctypes.c_char_p, _I, _I], "yg_gauge_load_cfg": [_P, ctypes.c_char_p, _P, _P, _P],
     "yg_gauge_save_hirep": [_P, ctypes.c_char_p], "yg_gauge_load_hirep": [_P, ctypes.c_char_p, _P, _P],
     "yg_momenta_upload": [_P, _P], "yg_momenta_download": [_P, _P], "yg_momenta_zero": [_P],
@@ -461,6 +463,32 @@ class Lattice:
         pp = (ctypes.c_void_p * len(props))(*[f.ptr for f in props])
         self._check(self.lib.yg_meson_contract(self.h, int(method), int(tau), pp, len(props), _ptr(corr)))
         return corr
+
+    # ---- Wilson and fermion flow (observables/wilsonflow.cpp, fermionflow.cpp)
+    def wf_init(self):
+        self._check(self.lib.yg_wf_init(self.h))
+
+    def wf_zeta(self, alpha):
+        self._check(self.lib.yg_wf_zeta(self.h, alpha))
+
+    def wf_update(self, val):
+        self._check(self.lib.yg_wf_update(self.h, val))
+
+    def wf_iterate(self, eps):
+        self._check(self.lib.yg_wf_iterate(self.h, eps))
+
+    def wf_observables(self):
+        """(E_plaq, E_sym, topological charge) as wf_e_plaq, wf_e_sym, wf_charge"""
+        e, s, q = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.yg_wf_observables(self.h, ctypes.byref(e), ctypes.byref(s), ctypes.byref(q)))
+        return e.value, s.value, q.value
+
+    def wf_fermion_init(self, n):
+        self._check(self.lib.yg_wf_fermion_init(self.h, int(n)))
+
+    def wf_fermion_iterate(self, eps, phis):
+        pp = (ctypes.c_void_p * len(phis))(*[f.ptr for f in phis])
+        self._check(self.lib.yg_wf_fermion_iterate(self.h, eps, pp, len(phis)))
 
     # ---- gauge configuration files (gaugefield.cpp:44-179, hirep.cpp:56-212)
     def gauge_field_save(self, path, num_cnfg=0, num_accept=0):

@@ -323,6 +323,23 @@ int yg_meson_contract(yg_lattice *l, int method, int tau, const double *const *p
   return guard([&] { need(props, "props"); need(corr, "corr"); yg::meson_contract(lat(l), method, tau, props, nprops, corr); });
 }
 
+// ---- Wilson and fermion flow
+int yg_wf_init(yg_lattice *l) { return guard([&] { yg::wf_init(lat(l)); }); }
+int yg_wf_zeta(yg_lattice *l, double alpha) { return guard([&] { yg::wf_zeta(lat(l), alpha); }); }
+int yg_wf_update(yg_lattice *l, double val) { return guard([&] { yg::wf_update(lat(l), val); }); }
+int yg_wf_iterate(yg_lattice *l, double eps) { return guard([&] { yg::wf_iterate(lat(l), eps); }); }
+int yg_wf_observables(yg_lattice *l, double *e_plaq, double *e_sym, double *charge) {
+  return guard([&] { yg::wf_observables(lat(l), e_plaq, e_sym, charge); });
+}
+int yg_wf_fermion_init(yg_lattice *l, int n) { return guard([&] { yg::wf_fermion_init(lat(l), n); }); }
+int yg_wf_fermion_iterate(yg_lattice *l, double eps, double *const *phi, int n) {
+  return guard([&] {
+    need(phi, "phi");
+    for (int i = 0; i < n; i++) need(phi[i], "phi[i]");
+    yg::wf_fermion_iterate(lat(l), eps, phi, n);
+  });
+}
+
 // ---- gauge configuration files
 int yg_gauge_save_cfg(yg_lattice *l, const char *path, int num_cnfg, int num_accept) {
   return guard([&] { need(path, "path"); yg::gauge_save_cfg(lat(l), path, num_cnfg, num_accept); });

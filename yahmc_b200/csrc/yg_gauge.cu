@@ -685,4 +685,244 @@ void gauge_restore(Lattice &L) {
   YG_CUDA(cudaMemcpyAsync(L.fund.p, L.fund_backup.p, L.fund.bytes, cudaMemcpyDeviceToDevice, L.stream));
 }
 
+// ------------------------------------------------------------------ Wilson and fermion flow
+// observables/wilsonflow.cpp:8-157 (the gradient flow of the Wilson action, third-order
+// Runge-Kutta, with the plaquette and clover energy densities and the clover charge) and
+// observables/fermionflow.cpp:11-97 (fields flowed with the gauge-covariant Laplacian).
+
+__global__ void k_scale(double *v, long n, double s) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) v[i] *= s;
+}
+
+// clover_fund(id, mu, nu), wilsonloop.cpp:33-54: the four plaquette leaves at x, summed
+template <int N>
+__device__ __noinline__ void clover_fund(double2 (&C)[N * N], const double2 *U, const Geom &g, const Pos &x, int mu, int nu) {
+  double2 A[N * N], B[N * N], P[N * N], Q[N * N];
+  const Pos xm = step(g, x, mu, +1), xn = step(g, x, nu, +1);
+  const Pos bm = step(g, x, mu, -1), bn = step(g, x, nu, -1);
+  const Pos bmn = step(g, bm, nu, +1), bmbn = step(g, bm, nu, -1), bnm = step(g, bn, mu, +1);
+  // U(x,mu) U(x+mu,nu) [U(x,nu) U(x+nu,mu)]^dag
+  ldU<N>(A, U, g, x, mu); ldU<N>(B, U, g, xm, nu); mat_mul<N>(P, A, B);
+  ldU<N>(A, U, g, x, nu); ldU<N>(B, U, g, xn, mu); mat_mul<N>(Q, A, B);
+  mul_dag<N>(C, P, Q);
+  // U(x,nu) [U(x-mu,nu) U(x-mu+nu,mu)]^dag U(x-mu,mu)
+  ldU<N>(A, U, g, bm, nu); ldU<N>(B, U, g, bmn, mu); mat_mul<N>(Q, A, B);
+  ldU<N>(A, U, g, x, nu); mul_dag<N>(P, A, Q);
+  ldU<N>(A, U, g, bm, mu); mat_mul<N>(Q, P, A);
+#pragma unroll
+  for (int k = 0; k < N * N; k++) C[k] = make_double2(C[k].x + Q[k].x, C[k].y + Q[k].y);
+  // [U(x-mu-nu,nu) U(x-mu,mu)]^dag U(x-mu-nu,mu) U(x-nu,nu)
+  ldU<N>(A, U, g, bmbn, nu); ldU<N>(B, U, g, bm, mu); mat_mul<N>(P, A, B);
+  ldU<N>(A, U, g, bmbn, mu); dag_mul<N>(Q, P, A);
+  ldU<N>(A, U, g, bn, nu); mat_mul<N>(P, Q, A);
+#pragma unroll
+  for (int k = 0; k < N * N; k++) C[k] = make_double2(C[k].x + P[k].x, C[k].y + P[k].y);
+  // U(x-nu,nu)^dag U(x-nu,mu) U(x-nu+mu,nu) U(x,mu)^dag
+  ldU<N>(A, U, g, bn, nu); ldU<N>(B, U, g, bn, mu); dag_mul<N>(P, A, B);
+  ldU<N>(A, U, g, bnm, nu); mat_mul<N>(Q, P, A);
+  ldU<N>(A, U, g, x, mu); mul_dag<N>(P, Q, A);
+#pragma unroll
+  for (int k = 0; k < N * N; k++) C[k] = make_double2(C[k].x + P[k].x, C[k].y + P[k].y);
+}
+
+// algebra_project(clover_fund(x, mu, nu), sqrt(2 TF)) into av
+template <int N>
+__device__ __forceinline__ void clover_algebra(double (&av)[N * N - 1], const double2 *U, const Geom &g, const Pos &x,
+                                               int mu, int nu, const double2 *itfund) {
+  double2 C[N * N];
+  clover_fund<N>(C, U, g, x, mu, nu);
+#pragma unroll
+  for (int a = 0; a < N * N - 1; a++) av[a] = 0.0;
+  project_add<N>(av, C, itfund, N * N - 1, 2.0);      // sqrt(2 TF) = 2
+}
+
+// per-site terms of wf_e_plaq (sum of N - w Re tr P over the six planes), wf_e_sym (sum of
+// |algebra_project(clover, sqrt(2 TF))|^2 over the six planes) and wf_charge (the three
+// products of dual planes): out[id], out[V + id], out[2V + id]
+template <int N>
+__global__ void __launch_bounds__(64) k_wf_densities(double *out, const double2 *U, Geom g, const double2 *itfund) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= g.V) return;
+  const Pos x = pos_of(g, id);
+  double ep = 0.0, es = 0.0, tc = 0.0;
+#pragma unroll 1
+  for (int mu = 1; mu < 4; mu++)
+#pragma unroll 1
+    for (int nu = 0; nu < mu; nu++) {
+      ep += N - wilson_loop<N>(U, g, x, mu, nu, 1, 1);
+      double av[N * N - 1];
+      clover_algebra<N>(av, U, g, x, mu, nu, itfund);
+#pragma unroll
+      for (int a = 0; a < N * N - 1; a++) es += av[a] * av[a];
+    }
+  const int pairs[3][4] = {{0, 3, 1, 2}, {0, 2, 3, 1}, {0, 1, 2, 3}};
+#pragma unroll 1
+  for (int k = 0; k < 3; k++) {
+    double a1[N * N - 1], a2[N * N - 1];
+    clover_algebra<N>(a1, U, g, x, pairs[k][0], pairs[k][1], itfund);
+    clover_algebra<N>(a2, U, g, x, pairs[k][2], pairs[k][3], itfund);
+#pragma unroll
+    for (int a = 0; a < N * N - 1; a++) tc += a1[a] * a2[a];
+  }
+  out[id] = ep;
+  out[(long)g.V + id] = es;
+  out[2L * g.V + id] = tc;
+}
+
+// wf_laplacian, fermionflow.cpp:11-26: dst(x) = -8 src(x) + sum_mu U(x,mu) src(x+mu)
+// + U(x-mu,mu)^dag src(x-mu) with the represented links, on every site; one thread per
+// (site, spin)
+template <int D>
+__global__ void __launch_bounds__(128) k_wf_laplacian(double2 *dst, const double2 *src, const double2 *U, Geom g) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= 4L * g.V) return;
+  const int id = (int)(t >> 2), sp = (int)(t & 3);
+  int c[4];
+  coords_of(g, id, c);
+  double2 acc[D], v[D];
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    const double2 s = src[fidx(g, id, sp * D + i, 4 * D)];
+    acc[i] = make_double2(-8.0 * s.x, -8.0 * s.y);
+  }
+#pragma unroll 1
+  for (int mu = 0; mu < 4; mu++) {
+    const int fw = neighbour(g, c, mu, +1), bk = neighbour(g, c, mu, -1);
+#pragma unroll
+    for (int j = 0; j < D; j++) v[j] = src[fidx(g, fw, sp * D + j, 4 * D)];
+#pragma unroll
+    for (int i = 0; i < D; i++) {
+      double2 s = make_double2(0, 0);
+#pragma unroll
+      for (int j = 0; j < D; j++) cfma(s, U[fidx(g, id, mu * D * D + i * D + j, 4 * D * D)], v[j]);
+      acc[i] = make_double2(acc[i].x + s.x, acc[i].y + s.y);
+    }
+#pragma unroll
+    for (int j = 0; j < D; j++) v[j] = src[fidx(g, bk, sp * D + j, 4 * D)];
+#pragma unroll
+    for (int i = 0; i < D; i++) {
+      double2 s = make_double2(0, 0);
+#pragma unroll
+      for (int j = 0; j < D; j++) cfmac(s, U[fidx(g, bk, mu * D * D + j * D + i, 4 * D * D)], v[j]);
+      acc[i] = make_double2(acc[i].x + s.x, acc[i].y + s.y);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < D; i++) dst[fidx(g, id, sp * D + i, 4 * D)] = acc[i];
+}
+
+template <int D>
+static void launch_wf_laplacian(Lattice &L, double *dst, const double *src) {
+  k_wf_laplacian<D><<<nblk(4L * L.V, 128), 128, 0, L.stream>>>((double2 *)dst, (const double2 *)src,
+                                                                L.links.as<double2>(), L.g);
+}
+
+// wf_init, wilsonflow.cpp:149-157
+void wf_init(Lattice &L) { YG_CUDA(cudaMemsetAsync(L.mom.p, 0, L.mom.bytes, L.stream)); }
+
+// wf_zeta, wilsonflow.cpp:8-23: P -= algebra_project(U staple, alpha), which is
+// wilson_gauge_force with dt = alpha and beta = N
+void wf_zeta(Lattice &L, double alpha) { wilson_gauge_force(L, alpha, (double)L.nc); }
+
+// wf_update, wilsonflow.cpp:25-41: U <- exp(P) U (no momentum boundary conditions), then
+// P <- val P; the boundary links take their fixed values
+void wf_update(Lattice &L, double val) {
+  const SFLinks sf = sf_links(L);
+  YG_GAUGE_N(L.nc, k_update_links<GN><<<nblk(4L * L.V, 64), 64, 0, L.stream>>>(L.fund.as<double2>(),
+                                                                               L.mom.as<double>(), L.g, 1.0, sf));
+  YG_LAUNCHED();
+  const long n = 4L * L.V * L.ng;
+  k_scale<<<nblk(n, 256) < 1184 ? nblk(n, 256) : 1184, 256, 0, L.stream>>>(L.mom.as<double>(), n, val);
+  YG_LAUNCHED();
+}
+
+// wf_iterate, wilsonflow.cpp:43-53: one Runge-Kutta step of size eps
+void wf_iterate(Lattice &L, double eps) {
+  wf_zeta(L, eps / 4.0);
+  wf_update(L, -17.0 / 9.0);
+  wf_zeta(L, 8.0 * eps / 9.0);
+  wf_update(L, -1.0);
+  wf_zeta(L, 3.0 * eps / 4.0);
+  wf_update(L, 0.0);
+}
+
+// wf_e_plaq, wf_e_sym, wf_charge (wilsonflow.cpp:55-147) from one pass over the sites
+void wf_observables(Lattice &L, double *e_plaq, double *e_sym, double *charge) {
+  double *tmp = L.scratch_field(kFlowDensities);
+  YG_GAUGE_N(L.nc, k_wf_densities<GN><<<nblk(L.V, 64), 64, 0, L.stream>>>(tmp, L.fund.as<double2>(), L.g, L.rt.itfund));
+  YG_LAUNCHED();
+  const double V = (double)L.V;
+  const double ep = sum_device(L, tmp, L.V), es = sum_device(L, tmp + L.V, L.V), tc = sum_device(L, tmp + 2 * L.V, L.V);
+  if (e_plaq) *e_plaq = 2 * ep / V;
+  if (e_sym) *e_sym = (2 * es) / (16 * 4 * V);
+  if (charge) *charge = (2 * tc) / (16 * 16 * M_PI * M_PI);
+}
+
+// wf_laplacian on the represented links
+void wf_laplacian(Lattice &L, double *dst, const double *src) {
+  switch (L.d) {
+    case 1: launch_wf_laplacian<1>(L, dst, src); break;
+    case 2: launch_wf_laplacian<2>(L, dst, src); break;
+    case 3: launch_wf_laplacian<3>(L, dst, src); break;
+    case 4: launch_wf_laplacian<4>(L, dst, src); break;
+    case 6: launch_wf_laplacian<6>(L, dst, src); break;
+    case 8: launch_wf_laplacian<8>(L, dst, src); break;
+    case 10: launch_wf_laplacian<10>(L, dst, src); break;
+    case 15: launch_wf_laplacian<15>(L, dst, src); break;
+    default: throw Error(YG_ERR_ARG, "unsupported representation dimension");
+  }
+  YG_LAUNCHED();
+}
+
+// wf_fermion_init, fermionflow.cpp:76-92: the stage fields start at zero, the momenta too
+void wf_fermion_init(Lattice &L, int n) {
+  if (n < 1 || n > kFlowMaxFields) throw Error(YG_ERR_ARG, "1..32 flowed fields");
+  for (int i = 0; i < n; i++) {
+    blas_zero(L, L.scratch_field(kFlowPhi1 + i), 0, L.V);
+    blas_zero(L, L.scratch_field(kFlowPhi2 + i), 0, L.V);
+  }
+  wf_init(L);
+}
+
+// wf_fermion_iterate, fermionflow.cpp:28-74: the fields phi0[i] and the gauge field flow
+// together.  As in the reference, spinor_copy copies whole fields (linalg.cpp:71-76) while
+// the other vector updates cover the default view (the even sites with even-odd
+// preconditioning); the Laplacian covers all sites.
+void wf_fermion_iterate(Lattice &L, double eps, double *const *phi0, int n) {
+  if (n < 1 || n > kFlowMaxFields) throw Error(YG_ERR_ARG, "1..32 flowed fields");
+  long lo, cnt;
+  L.view_range(YG_VIEW_DEFAULT, lo, cnt);
+  double *dphi = L.scratch_field(kFlowDphi);
+  const double2 one = make_double2(1, 0), zero = make_double2(0, 0);
+  auto re = [](double v) { return make_double2(v, 0); };
+  represent_and_clover(L);
+  for (int i = 0; i < n; i++) {
+    double *p1 = L.scratch_field(kFlowPhi1 + i);
+    wf_laplacian(L, dphi, phi0[i]);
+    blas_copy(L, p1, phi0[i]);
+    blas_axpby(L, p1, one, re(eps / 4.0), dphi, lo, cnt);
+  }
+  wf_zeta(L, eps / 4.0);
+  wf_update(L, -17.0 / 9.0);
+  represent_and_clover(L);
+  for (int i = 0; i < n; i++) {
+    double *p1 = L.scratch_field(kFlowPhi1 + i), *p2 = L.scratch_field(kFlowPhi2 + i);
+    wf_laplacian(L, dphi, p1);
+    blas_axpby(L, p2, zero, re(-8.0 / 9.0), p1, lo, cnt);
+    blas_axpby(L, p2, one, re(17.0 / 9.0), phi0[i], lo, cnt);
+    blas_axpby(L, p2, one, re(8.0 * eps / 9.0), dphi, lo, cnt);
+  }
+  wf_zeta(L, 8.0 * eps / 9.0);
+  wf_update(L, -1.0);
+  represent_and_clover(L);
+  for (int i = 0; i < n; i++) {
+    double *p1 = L.scratch_field(kFlowPhi1 + i), *p2 = L.scratch_field(kFlowPhi2 + i);
+    wf_laplacian(L, dphi, p2);
+    blas_copy(L, phi0[i], p1);
+    blas_axpby(L, phi0[i], one, re(3.0 * eps / 4.0), dphi, lo, cnt);
+  }
+  wf_zeta(L, 3.0 * eps / 4.0);
+  wf_update(L, 0.0);
+}
+
 }  // namespace yg

@@ -208,6 +208,18 @@ void gauge_load_cfg(Lattice &L, const char *path, int *num_cnfg, int *num_accept
 void gauge_save_hirep(Lattice &L, const char *path);
 void gauge_load_hirep(Lattice &L, const char *path, int *num_cnfg, double *plaq_diff);
 
+// Wilson and fermion flow (yg_gauge.cu); scratch slots of the flow
+constexpr int kFlowDensities = 190, kFlowDphi = 191, kFlowPhi1 = 200, kFlowMaxFields = 32,
+              kFlowPhi2 = kFlowPhi1 + kFlowMaxFields;
+void wf_init(Lattice &L);
+void wf_zeta(Lattice &L, double alpha);
+void wf_update(Lattice &L, double val);
+void wf_iterate(Lattice &L, double eps);
+void wf_observables(Lattice &L, double *e_plaq, double *e_sym, double *charge);
+void wf_laplacian(Lattice &L, double *dst, const double *src);
+void wf_fermion_init(Lattice &L, int n);
+void wf_fermion_iterate(Lattice &L, double eps, double *const *phi0, int n);
+
 // sources, propagators and meson contractions (yg_mesons.cu)
 void create_point_source(Lattice &L, int n, int tau, double *src);
 void create_semwall_source(Lattice &L, int n, int tau, const double *z2, double *src);
