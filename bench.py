@@ -35,6 +35,8 @@ import time
 
 import numpy as np
 
+from yahmc_b200 import replicas
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
@@ -141,7 +143,7 @@ def make_inputs(dims, seed, rank=0, trajectories=None, cache=None):
             np.savez(cache, U=U, plaquette=plaq, acceptance=acc)
     T, X, Y, Z = dims
     V = T * X * Y * Z
-    rng = np.random.default_rng(seed + 7919 * rank)
+    rng = np.random.default_rng(replicas.rank_seed(seed, rank))
     b = fields.gaussian_spinor(V, 3, rng)
     return U, b, {"plaquette": plaq, "acceptance": acc,
                   "trajectories": THERM["trajectories"] if trajectories is None else trajectories}
@@ -267,9 +269,7 @@ def run_ours(a, rank, world, dist):
     x = lat.field()
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
+        replicas.barrier(dist, torch.cuda.synchronize)
 
     def timed(fn, k):
         """k calls of fn bracketed by a barrier + synchronize on both sides, CUDA events on the
@@ -281,11 +281,7 @@ def run_ours(a, rank, world, dist):
         e1.record()
         torch.cuda.synchronize()
         barrier()
-        ms = e0.elapsed_time(e1) / k
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = replicas.max_over_ranks(e0.elapsed_time(e1) / k, dist, "cuda")
         return ms, out
 
     def mixed():
@@ -441,7 +437,7 @@ def run_ours(a, rank, world, dist):
 
     if rank != 0:
         return
-    value = ms_mixed / world          # whole-job time per solve: world solves run concurrently
+    value = replicas.job_time_per_solve(ms_mixed, world)
     line = {
         "metric": "CG time-to-solution (true rel. residual 1e-12), mixed precision",
         "value": value, "unit": "ms", "n_gpus": world, "steps": a.steps, "warmup": max(3, a.warmup),
@@ -462,7 +458,7 @@ def run_ours(a, rank, world, dist):
                      "peak_kind": peak_kind, "traffic": None, "ms_per_launch": ms_inner,
                      "bytes_per_launch": inner_bytes,
                      "bytes_per_site": inner_bytes / (V // 2)},
-        "e2e": {"value": ms_e2e / world, "unit": "ms", "h2d_bytes_per_step": field_bytes,
+        "e2e": {"value": replicas.job_time_per_solve(ms_e2e, world), "unit": "ms", "h2d_bytes_per_step": field_bytes,
                 "d2h_bytes_per_step": field_bytes},
         "gpu_launches": int(launches),
         "clocks": clocks,
