@@ -80,7 +80,7 @@ def parse():
 INNER = {"generic-f32": (0, 18, 0, 0), "f32-l18": (32, 18, 0, 0), "f32-l12": (32, 12, 0, 0),
          "f16-l18": (16, 18, 0, 0), "f16-l12": (16, 12, 0, 0),
          "f32-i16links-l12": (32, 12, 15, 32), "f32-i16-l12": (32, 12, 15, 15), "f16-i16-l12": (16, 12, 15, 15),
-         "f16spinor-l12": (16, 12, 32, 32)}
+         "f16spinor-l12": (16, 12, 32, 32), "f16spinor-l8": (16, 8, 32, 32), "f32-l8": (32, 8, 32, 32)}
 
 
 DTYPE = {"generic-f32": "f32 inner / f64 reliable updates and residual",
@@ -91,7 +91,9 @@ DTYPE = {"generic-f32": "f32 inner / f64 reliable updates and residual",
          "f32-i16links-l12": "f32 inner (int16 12-real links) / f64 reliable updates and residual",
          "f32-i16-l12": "f32 inner (int16 12-real links and clover) / f64 reliable updates and residual",
          "f16-i16-l12": "f32 inner arithmetic on f16 spinors, int16 links and clover / f64 reliable updates and residual",
-         "f16spinor-l12": "f32 inner arithmetic on f16 spinors, f32 12-real links and clover / f64 reliable updates and residual"}
+         "f16spinor-l12": "f32 inner arithmetic on f16 spinors, f32 12-real links and clover / f64 reliable updates and residual",
+         "f16spinor-l8": "f32 inner arithmetic on f16 spinors, f32 8-real links, f32 clover / f64 reliable updates and residual",
+         "f32-l8": "f32 inner (8-real links) / f64 reliable updates and residual"}
 
 
 def solve_mixed(lat, x, b, inner, delta):

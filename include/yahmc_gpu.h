@@ -209,7 +209,10 @@ int yg_inner_hop_profile(yg_lattice *lat, double mass, int reps, double *ms_per_
 /* No reference counterpart: options of the mixed-precision solver.
  *   inner_precision  32 (FP32 storage) or 16 (FP16 storage with per-site norms), FP32
  *                    arithmetic; 0 selects the generic FP32 operator of yg_cg_mixed (any d)
- *   link_reals       18, or 12 (two rows, third rebuilt; SU(3) fundamental only)
+ *   link_reals       18, or 12 (two rows, third rebuilt; SU(3) fundamental only), or 8 (SU(3)
+ *                    fundamental, FP32 link storage, periodic or antiperiodic boundaries: one row
+ *                    and the smaller of two first-column entries in full, two phases; rebuilt
+ *                    from unitarity and det = 1)
  *   delta            reliable update when |r| falls below delta * |r| at the last update
  *   link_storage,    storage of the inner operator's links and clover blocks; the combinations
  *   clover_storage   built are all-FP32, FP32 spinors with int16 links (FP32 or int16 clover),

@@ -31,7 +31,10 @@ CASES = [("su3_fund_ap", 32, 12, 0, 0), ("su3_fund_ap", 32, 18, 0, 0), ("su3_fun
          # int16 fixed-point links / clover blocks (storage 15)
          ("su3_fund_ap", 32, 12, 15, 32), ("su3_fund_ap", 32, 12, 15, 15), ("su3_fund_open", 32, 12, 15, 15),
          ("su3_fund_sf", 32, 18, 15, 15), ("su3_fund_ap_nocl", 32, 12, 15, 15), ("su2_adj_ap", 32, 18, 15, 15),
-         ("su3_fund_ap", 16, 12, 15, 15), ("su3_fund_ap", 16, 12, 32, 32)]
+         ("su3_fund_ap", 16, 12, 15, 15), ("su3_fund_ap", 16, 12, 32, 32),
+         # 8-real FP32 links (periodic / antiperiodic lattices)
+         ("su3_fund_ap", 32, 8, 0, 0), ("su3_fund_ap", 16, 8, 32, 32), ("su3_fund_per", 16, 8, 32, 32),
+         ("su3_fund_ap_nocl", 32, 8, 0, 0)]
 
 
 @pytest.mark.parametrize("name,inner,reals,lfmt,cfmt", CASES)
@@ -62,6 +65,13 @@ def test_storage_format_errors():
         with pytest.raises(YGError):
             lat.cg_mixed("Hphi_sq", -0.4, 1e-20, x, b, inner_precision=32, link_reals=12, link_storage=lfmt,
                          clover_storage=cfmt)
+    with pytest.raises(YGError):                                       # 8-real links are FP32 only
+        lat.cg_mixed("Hphi_sq", -0.4, 1e-20, x, b, inner_precision=16, link_reals=8, link_storage=16,
+                     clover_storage=16)
+    lat2, O2, rng2 = make_pair("su3_fund_open", (4, 4, 4, 4), seed=38)
+    with pytest.raises(YGError):                                       # not for open / SF boundaries
+        lat2.cg_mixed("Hphi_sq", -0.4, 1e-20, lat2.field(), lat2.field(source(O2, rng2)), inner_precision=32,
+                      link_reals=8)
 
 
 @pytest.mark.parametrize("delta", [0.01, 0.3, 1e-4])

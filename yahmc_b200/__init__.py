@@ -540,8 +540,8 @@ class Lattice:
                  link_storage=0, clover_storage=0, escalate=False):
         """Mixed-precision CG (true FP64 stopping criterion).  inner_precision None: the
         library's choice (yg_cg_mixed); 0: the generic FP32 inner operator; 32 or 16: the
-        compressed d = 3 inner operator with link_reals 18 or 12 and reliable-update
-        threshold delta; link_storage / clover_storage 0 (as the spinors), 32, 16 or 15
+        compressed d = 3 inner operator with link_reals 18, 12 or 8 (8: FP32 links,
+        periodic or antiperiodic lattices) and reliable-update threshold delta; link_storage / clover_storage 0 (as the spinors), 32, 16 or 15
         (int16 fixed point)."""
         st = SolveStats()
         par = self._par(op, mass, prec, log, maxiter)

@@ -150,6 +150,37 @@ __device__ __forceinline__ void link_load(float2 (&u)[9], const void *U, int blk
     u[7] = cscale(cconj(csub(cmul(a2, b0), cmul(a0, b2))), sgn);
     u[8] = cscale(cconj(csub(cmul(a0, b1), cmul(a1, b0))), sgn);
   }
+  if (K == 4) {
+    // 8 reals of an SU(3) link W (FP32 only), see k_pack_links: word 0 = (phase of a0 with
+    // the b0/c0 choice in its lowest mantissa bit, phase of the other first-column entry
+    // with the column shift in its two lowest bits), words 1-3 = a1, a2 and the smaller of
+    // b0, c0 in full.  Rows from |row 0| = |column 0| = 1, then b1, b2 from unitarity and
+    // det = 1, c = conj(a x b); finally the columns are shifted back and the sign applied.
+    const float2 w = u[0], a1 = u[1], a2 = u[2], st = u[3];
+    const bool cstored = (__float_as_uint(w.x) & 1u) != 0u;
+    const int shift = (int)(__float_as_uint(w.y) & 3u);
+    const float n = a1.x * a1.x + a1.y * a1.y + a2.x * a2.x + a2.y * a2.y;
+    float sa, ca, so, co;                     // |phase| <= pi: the SFU forms are accurate to ~4e-7
+    __sincosf(w.x, &sa, &ca);
+    __sincosf(w.y, &so, &co);
+    const float ma = sqrtf(fmaxf(1.f - n, 0.f)), mo = sqrtf(fmaxf(n - (st.x * st.x + st.y * st.y), 0.f));
+    const float2 a0 = make_float2(ma * ca, ma * sa), oth = make_float2(mo * co, mo * so);
+    const float2 b0 = cstored ? oth : st, c0 = cstored ? st : oth;
+    const float inv = n > 0.f ? __frcp_rn(n) : 0.f;
+    const float2 b1 = cscale(cadd(cmul(cmulc(a0, a1), b0), cmulc(a2, cconj(c0))), -inv);
+    const float2 b2 = cscale(csub(cmulc(a1, cconj(c0)), cmul(cmulc(a0, a2), b0)), inv);
+    const float2 c1 = cconj(csub(cmul(a2, b0), cmul(a0, b2)));
+    const float2 c2 = cconj(csub(cmul(a0, b1), cmul(a1, b0)));
+    const float2 r[3][3] = {{a0, a1, a2}, {b0, b1, b2}, {c0, c1, c2}};
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        // W[i][k] = R[i][(k - shift) mod 3]
+        const float2 v = shift == 0 ? r[i][k] : shift == 1 ? r[i][(k + 2) % 3] : r[i][(k + 1) % 3];
+        u[i * 3 + k] = cscale(v, sgn);
+      }
+  }
 }
 
 // Packed Hermitian blocks: 72 reals per site (block b: 6 diagonal reals, then the 15
@@ -439,8 +470,45 @@ __global__ void k_pack_links(void *dst, const double2 *links, Geom g) {
   if (r >= 4L * g.V) return;
   int id = (int)(r >> 2), mu = (int)(r & 3);
   int blk = id >= g.Vh, h = id - blk * g.Vh;
-  for (int k = 0; k < K; k++)
-    lstore<LP>(dst, ((long)(blk * 4 + mu) * K + k) * g.Vh + h, links[fidx(g, id, mu * 9 + k, 36)]);
+  if (K != 4) {
+    for (int k = 0; k < K; k++)
+      lstore<LP>(dst, ((long)(blk * 4 + mu) * K + k) * g.Vh + h, links[fidx(g, id, mu * 9 + k, 36)]);
+    return;
+  }
+  // 8 reals (FP32): W = s V with s = sign det V (the antiperiodic sign), columns shifted
+  // cyclically so that a0 is the largest entry of row 0 (|a0|^2 >= 1/3), then the smaller
+  // of b0, c0 stored in full and the phases of a0 and of the other one (link_load)
+  double2 V[9];
+  for (int k = 0; k < 9; k++) V[k] = links[fidx(g, id, mu * 9 + k, 36)];
+  auto m = [](double2 x, double2 y) { return make_double2(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x); };
+  auto sb = [](double2 x, double2 y) { return make_double2(x.x - y.x, x.y - y.y); };
+  const double2 d0 = m(V[0], sb(m(V[4], V[8]), m(V[5], V[7])));
+  const double2 d1 = m(V[1], sb(m(V[5], V[6]), m(V[3], V[8])));
+  const double2 d2 = m(V[2], sb(m(V[3], V[7]), m(V[4], V[6])));
+  const double s = (d0.x + d1.x + d2.x) < 0.0 ? -1.0 : 1.0;
+  double best = -1.0;
+  int shift = 0;
+  for (int j = 0; j < 3; j++) {
+    const double a = V[j].x * V[j].x + V[j].y * V[j].y;
+    if (a > best) { best = a; shift = j; }
+  }
+  double2 R[9];                               // R[i][k] = W[i][(k + shift) mod 3]
+  for (int i = 0; i < 3; i++)
+    for (int k = 0; k < 3; k++) {
+      const double2 v = V[i * 3 + (k + shift) % 3];
+      R[i * 3 + k] = make_double2(s * v.x, s * v.y);
+    }
+  const double b2n = R[3].x * R[3].x + R[3].y * R[3].y, c2n = R[6].x * R[6].x + R[6].y * R[6].y;
+  const bool cstored = c2n < b2n;
+  const double2 other = cstored ? R[3] : R[6], kept = cstored ? R[6] : R[3];
+  const float pa = __uint_as_float((__float_as_uint((float)atan2(R[0].y, R[0].x)) & ~1u) | (cstored ? 1u : 0u));
+  const float po = __uint_as_float((__float_as_uint((float)atan2(other.y, other.x)) & ~3u) | (unsigned)shift);
+  float2 *f = reinterpret_cast<float2 *>(dst);
+  const long base = (long)(blk * 4 + mu) * 4;
+  f[(base + 0) * g.Vh + h] = make_float2(pa, po);
+  f[(base + 1) * g.Vh + h] = make_float2((float)R[1].x, (float)R[1].y);
+  f[(base + 2) * g.Vh + h] = make_float2((float)R[2].x, (float)R[2].y);
+  f[(base + 3) * g.Vh + h] = make_float2((float)kept.x, (float)kept.y);
 }
 
 template <int CP>
@@ -669,6 +737,9 @@ static int sgrid(long n) {
   if (prec_ == P_ && lf_ == L_ && cf_ == C_) {                                               \
     constexpr int SP = P_, SL = L_, SC = C_;                                                 \
     if (reals_ == 12) { constexpr int SK = 6; __VA_ARGS__; }                                 \
+    else if (reals_ == 8) {                                                                  \
+      if constexpr (L_ == 32) { constexpr int SK = 4; __VA_ARGS__; }                         \
+    }                                                                                        \
     else { constexpr int SK = 9; __VA_ARGS__; }                                              \
     done_ = true;                                                                            \
   }
@@ -699,13 +770,18 @@ static int matrix_format(int requested, int prec) { return requested == 0 ? prec
 void ensure_sloppy(Lattice &L, double mass, int prec, int reals, int lfmt, int cfmt) {
   lfmt = matrix_format(lfmt, prec);
   cfmt = matrix_format(cfmt, prec);
-  if ((prec != 32 && prec != 16) || (reals != 18 && reals != 12))
-    throw Error(YG_ERR_ARG, "inner precision must be 32 or 16 and link reals 18 or 12");
+  if ((prec != 32 && prec != 16) || (reals != 18 && reals != 12 && reals != 8))
+    throw Error(YG_ERR_ARG, "inner precision must be 32 or 16 and link reals 18, 12 or 8");
+  if (reals == 8 && matrix_format(lfmt, prec) != ST_F32)
+    throw Error(YG_ERR_ARG, "8-real links are stored FP32");
+  if (reals == 8 && L.p.bc != YG_BC_PERIODIC && L.p.bc != YG_BC_ANTIPERIODIC)
+    throw Error(YG_ERR_ARG, "8-real links need periodic or antiperiodic boundaries (open and SF boundary links are "
+                            "not of the parametrised form)");
   for (int f : {lfmt, cfmt})
     if (f != ST_F32 && f != ST_F16 && f != ST_I16) throw Error(YG_ERR_ARG, "matrix storage must be 32, 16 or 15");
   if (L.d != 3) throw Error(YG_ERR_ARG, "the compressed inner operator exists for d = 3 representations");
-  if (reals == 12 && !(L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL))
-    throw Error(YG_ERR_ARG, "12-real links need SU(3) fundamental links");
+  if (reals != 18 && !(L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL))
+    throw Error(YG_ERR_ARG, "12- and 8-real links need SU(3) fundamental links");
   if (!L.p.eo) throw Error(YG_ERR_ARG, "the mixed-precision solver needs even-odd preconditioning");
   if (!L.sl_hist) {
     // mapped host words: [0], [1] the |r|^2 of the last two iterations, [4] their counter
