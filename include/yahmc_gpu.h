@@ -177,8 +177,9 @@ int yg_rational_calc(yg_lattice *lat, const yg_inv_par *par, double a0, int orde
                      const double *residues, double *x, double *b, int *iters);
 /* No reference counterpart: CG on the same operator with FP32 inner iterations and FP64
  * reliable updates; stops on the TRUE FP64 squared residual |b-Ax|^2 < prec*|b|^2.  Uses
- * the compressed inner operator for d = 3 (FP16 spinors with per-site norms, FP32 links --
- * 12-real for SU(3) fundamental -- and clover blocks, delta 0.1; if that stalls, the inner
+ * the compressed inner operator for d = 3 (FP16 spinors with per-site norms, FP32 links in
+ * the format yg_tune_inner_links measures fastest on the lattice at the first call, FP32
+ * clover blocks, delta 0.1; if that stalls, the inner
  * solve restarts with FP32 spinors from its best iterate) and the generic FP32 operator
  * otherwise.  stats->fallback: bit 0 the FP64 CG finished the solve, bit 1 the inner
  * storage was raised to FP32. */
@@ -229,6 +230,13 @@ typedef struct {
 } yg_mixed_opts;
 int yg_cg_mixed_opts(yg_lattice *lat, const yg_inv_par *par, const yg_mixed_opts *opts, double *x, double *b,
                      yg_solve_stats *stats);
+
+/* No reference counterpart (autotuning): times the step-1 hop of the compressed inner operator
+ * for each FP32 link format allowed on this lattice (18 reals; 12 for SU(3) fundamental; 8 as
+ * well on periodic / antiperiodic lattices) and keeps the fastest for yg_cg_mixed, which runs
+ * this itself at its first call on a lattice.  ms_per_hop (may be NULL): 3 doubles, the mean
+ * hop time of the 18-, 12- and 8-real formats, 0 where not a candidate. */
+int yg_tune_inner_links(yg_lattice *lat, double mass, int *link_reals, double *ms_per_hop);
 
 /* ---- propagators and mesons (observables/propagator.cpp, observables/mesons.cpp) ---- */
 enum { YG_MESON_SEMWALL = 0x01, YG_MESON_POINT = 0x02 };   /* include/spectrum.h:7-8 */

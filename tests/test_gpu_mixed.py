@@ -146,3 +146,19 @@ def test_precision_ladder():
     st = lat.cg_mixed("Hphi_sq", -0.4, 1e-26, x, b)
     assert st["status"] == 0 and st["fallback"] == 0, st
     assert _true_residual(lat, "Hphi_sq", -0.4, x, b) < 1e-26
+
+
+@pytest.mark.parametrize("name", ["su3_fund_ap", "su3_fund_open", "su2_adj_ap"])
+def test_link_format_autotuner(name):
+    """yg_tune_inner_links times the FP32 link formats allowed on the lattice and keeps the
+    fastest; the default mixed solve then uses it and meets the true FP64 residual"""
+    dims = (8, 8, 8, 8) if name.startswith("su3") else (4, 6, 4, 8)
+    lat, O, rng = make_pair(name, dims, seed=39)
+    reals, ms = lat.tune_inner_links(-0.4)
+    allowed = {"su3_fund_ap": {18, 12, 8}, "su3_fund_open": {18, 12}, "su2_adj_ap": {18}}[name]
+    assert {r for r, t in ms.items() if t > 0} == allowed
+    assert reals in allowed and ms[reals] == min(t for t in ms.values() if t > 0)
+    b, x = lat.field(source(O, rng)), lat.field()
+    st = lat.cg_mixed("Hphi_sq", -0.4, 1e-24, x, b)
+    assert st["status"] == 0 and st["true_residual"] < 1e-24
+    assert _true_residual(lat, "Hphi_sq", -0.4, x, b) < 1e-24

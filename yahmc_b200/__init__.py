@@ -110,6 +110,7 @@ _SIGNATURES = {
     "yg_create_point_source": [_P, _I, _I, _P], "yg_create_semwall_source": [_P, _I, _I, _P, _P],
     "yg_calc_propagator": [_P, _D, _D, _P, _P, _P], "yg_calc_propagator_multi": [_P, _D, _D, _I, _P, _P, _I, _P],
     "yg_meson_contract": [_P, _I, _I, _P, _I, _P],
+    "yg_tune_inner_links": [_P, _D, _P, _P],
     "yg_wf_init": [_P], "yg_wf_zeta": [_P, _D], "yg_wf_update": [_P, _D], "yg_wf_iterate": [_P, _D],
     "yg_wf_observables": [_P, _P, _P, _P], "yg_wf_fermion_init": [_P, _I], "yg_wf_fermion_iterate": [_P, _D, _P, _I],
     "yg_gauge_save_cfg": [_P, ctypes.c_char_p, _I, _I], "yg_gauge_load_cfg": [_P, ctypes.c_char_p, _P, _P, _P],
@@ -413,6 +414,14 @@ class Lattice:
         if rc not in (0, 4):
             self._check(rc)
         return list(its)
+
+    def tune_inner_links(self, mass):
+        """times the FP32 link formats of the compressed inner operator on this lattice and
+        keeps the fastest for cg_mixed's default; returns (link_reals, {reals: ms per hop})"""
+        r = ctypes.c_int()
+        ms = np.zeros(3)
+        self._check(self.lib.yg_tune_inner_links(self.h, mass, ctypes.byref(r), _ptr(ms)))
+        return r.value, {18: ms[0], 12: ms[1], 8: ms[2]}
 
     # ---- sources, propagators, meson contractions (observables/propagator.cpp, mesons.cpp)
     def create_point_source(self, n, tau, src):

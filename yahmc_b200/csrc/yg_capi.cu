@@ -281,14 +281,24 @@ int yg_cg_mixed(yg_lattice *l, const yg_inv_par *p, double *x, double *b, yg_sol
     check_par(p); need(x, "x"); need(b, "b");
     yg::Lattice &L = lat(l);
     // the compressed inner operator where it exists (d = 3, even-odd): FP16 spinors with
-    // per-site norms, FP32 links (12-real for SU(3) fundamental) and clover blocks, delta
-    // 0.1 -- 16-bit spinors only add noise to each inner step, while 16-bit matrices would
-    // change the operator itself; else the generic FP32 operator
+    // per-site norms, FP32 links and clover blocks, delta 0.1 -- 16-bit spinors only add
+    // noise to each inner step, while 16-bit matrices would change the operator itself; the
+    // link format (18, 12 or 8 reals) is the fastest one measured on this lattice at the
+    // first call; else the generic FP32 operator
     if (L.d == 3 && L.p.eo) {
-      int reals = (L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL) ? 12 : 18;
+      const int reals = yg::tuned_inner_links(L, p->mass);
       return yg::cg_mixed_sloppy(L, *p, 16, reals, 32, 32, 0.1, x, b, st, /*escalate=*/true);
     }
     return yg::cg_mixed(L, *p, x, b, st);
+  });
+}
+
+int yg_tune_inner_links(yg_lattice *l, double mass, int *link_reals, double *ms_per_hop) {
+  return guard([&] {
+    yg::Lattice &L = lat(l);
+    if (L.d != 3 || !L.p.eo) throw yg::Error(YG_ERR_ARG, "the compressed inner operator needs d = 3 and even-odd");
+    const int r = yg::tune_inner_links(L, mass, ms_per_hop);
+    if (link_reals) *link_reals = r;
   });
 }
 

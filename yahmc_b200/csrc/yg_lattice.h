@@ -91,6 +91,7 @@ struct Lattice {
   DevBuf sl_cnorm;     // per-site scales of int16 clover records
   double sl_mass = 0;
   bool sl_valid = false;
+  int sl_tuned_reals = 0;  // link format of the default mixed solve (tune_inner_links), 0 = not yet
   DevBuf sl_part;      // per-block partial sums of the device-scalar reductions
   int sl_grid_nrm = 0; // blocks of the hop that forms <p, A p> (resident-grid size)
   int sl_grid_vec = 0; // blocks of the inner vector kernels
@@ -236,6 +237,8 @@ int cg_mixed_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *x
 // the compressed inner operator's matrices (yg_sloppy.cu); formats 32 / 16 / 15, 0 = as prec
 void ensure_sloppy(Lattice &L, double mass, int prec, int reals, int lfmt, int cfmt);
 void inner_hop_profile(Lattice &L, double mass, int reps, double *ms, double *bytes);
+int tune_inner_links(Lattice &L, double mass, double *ms);
+int tuned_inner_links(Lattice &L, double mass);
 
 // chronological initial guess (yg_mre.cu)
 struct Mre;

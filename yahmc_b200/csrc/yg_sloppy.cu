@@ -1083,9 +1083,9 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int 
 // operator (the kernel that dominates cg_mixed) with the solver's default storage, timed
 // with CUDA events on the lattice's stream, and the compulsory bytes one launch moves
 // (neighbour spinors read once, links, clover blocks, output spinor).
-void inner_hop_profile(Lattice &L, double mass, int reps, double *ms, double *bytes) {
+// mean time of the inner operator's step-1 hop (FP16 spinors, FP32 matrices, `reals` per link)
+static void hop_time(Lattice &L, double mass, int reals, int reps, double *ms, double *bytes) {
   if (reps < 1) throw Error(YG_ERR_ARG, "reps must be >= 1");
-  const int reals = (L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL) ? 12 : 18;
   ensure_sloppy(L, mass, 16, reals, 32, 32);
   SField src = sfield(L, 41), dst = sfield(L, 44);
   sloppy_from_d(L, src, L.scratch_field(3));
@@ -1118,6 +1118,38 @@ void inner_hop_profile(Lattice &L, double mass, int reps, double *ms, double *by
   const double link = (reals / 2) * (L.sl_lfmt == ST_F32 ? 8.0 : 4.0);
   const double clov = 72.0 * (L.sl_cfmt == ST_F32 ? 4.0 : 2.0) + (L.sl_cfmt == ST_I16 ? 4.0 : 0.0);
   *bytes = (double)L.Vh * (spinor + 8.0 * link + clov + spinor);
+}
+
+void inner_hop_profile(Lattice &L, double mass, int reps, double *ms, double *bytes) {
+  hop_time(L, mass, (L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL) ? 12 : 18, reps, ms, bytes);
+}
+
+// No reference counterpart: the link format of the default mixed solve chosen by measurement.
+// The candidates carry FP32 matrices (the formats whose rounding leaves the operator accurate
+// enough on rough fields): 18 reals always, 12 for SU(3) fundamental links, 8 in addition on
+// periodic / antiperiodic lattices.  Each is timed over 20 step-1 hops on this lattice; the
+// fastest is kept for the lattice (ms[0..2] = 18, 12, 8 real, 0 where not a candidate).
+int tune_inner_links(Lattice &L, double mass, double *ms) {
+  const bool su3 = L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL;
+  const bool pbc = L.p.bc == YG_BC_PERIODIC || L.p.bc == YG_BC_ANTIPERIODIC;
+  const int cand[3] = {18, 12, 8};
+  const bool ok[3] = {true, su3, su3 && pbc};
+  int best = 18;
+  double best_ms = 0.0;
+  for (int k = 0; k < 3; k++) {
+    double t = 0.0, bytes = 0.0;
+    if (ok[k]) {
+      hop_time(L, mass, cand[k], 20, &t, &bytes);
+      if (best_ms == 0.0 || t < best_ms) { best_ms = t; best = cand[k]; }
+    }
+    if (ms) ms[k] = t;
+  }
+  L.sl_tuned_reals = best;
+  return best;
+}
+
+int tuned_inner_links(Lattice &L, double mass) {
+  return L.sl_tuned_reals ? L.sl_tuned_reals : tune_inner_links(L, mass, nullptr);
 }
 
 }  // namespace yg
