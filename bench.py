@@ -72,6 +72,11 @@ def parse():
                     help="time only the batched CG of --nrhs systems (for profiling; not the bench line)")
     ap.add_argument("--solve-only", action="store_true",
                     help="time only the mixed solve and print its time (for profiling; not the bench line)")
+    ap.add_argument("--mesons", action="store_true",
+                    help="time the 12 point-source propagators of one slice (one at a time and batched) and the "
+                         "16-channel contraction on 48x24x24x24 (not the bench line)")
+    ap.add_argument("--contract-only", action="store_true",
+                    help="with --mesons: only the contraction, on random propagators (for profiling)")
     return ap.parse_args()
 
 
@@ -256,6 +261,80 @@ def run_reference(a, rank, world):
 
 
 # ------------------------------------------------------------------ our arm
+def run_mesons(a):
+    """The point-source meson workload on one GPU: the 12 propagators of one source slice on a
+    thermalised 48x24^3 SU(3) field (m = -0.6, prec 1e-20), solved one at a time with
+    calc_propagator (BiCGstab, the reference's path) and through the batched CG (FP64 and
+    mixed), then the sixteen-channel contraction timed with CUDA events."""
+    import torch
+    import yahmc_b200 as yg
+    from yahmc_b200 import fields
+    from yahmc_b200.spectrum import POINT, Mesons
+    torch.cuda.set_device(0)
+    yg.set_device(0)
+    dims = (48, 24, 24, 24)
+    mass, prec, tau = -0.6, 1e-20, 5
+    out = {"workload": "12 point-source propagators of one slice + 16-channel contraction, 48x24x24x24 SU(3) "
+                       "fund even-odd Wilson-clover", "mass": mass, "prec_squared": prec}
+    lat = yg.Lattice(dims, nc=3, repr="fundamental", bc="antiperiodic", clover=True, eo=True, csw=CSW)
+    if a.contract_only:
+        rng = np.random.default_rng(a.seed)
+        lat.set_links(fields.haar_su(3, lat.V * 4, rng).reshape(lat.V, 4, 3, 3))
+        props = [lat.field(fields.gaussian_spinor(lat.V, 3, rng)) for _ in range(12)]
+    else:
+        if a.field_cache and os.path.exists(a.field_cache):
+            z = np.load(a.field_cache)
+            U, plaq = z["U"], float(z["plaquette"])
+        else:
+            U, plaq, _ = thermalised_links(dims, a.seed, trajectories=40)
+            if a.field_cache:
+                np.savez(a.field_cache, U=U, plaquette=plaq, acceptance=0.0)
+        lat.set_links(U)
+        out["links"] = f"thermalised: 40 pure-gauge HMC trajectories at beta 5.6, plaquette {plaq:.5f}"
+
+        def run(**kw):
+            M = Mesons(lat, mass, prec, 1, POINT, **kw)
+            M.measure(taus=[tau])                              # warm-up: tuning, allocations
+            for f in M.prop:
+                lat.spinor_zero(f)                             # timed solves start from zero
+            M.iterations = 0
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            M.measure(taus=[tau])
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1), M
+
+        t1, A = run()
+        t2, B = run(batched=True)
+        t3, C = run(batched=True, mixed=True)
+        va = A.values()
+        out["one_at_a_time_bicgstab"] = {"ms": t1, "iterations": A.iterations}
+        out["batched_fp64_cg"] = {"ms": t2, "iterations": B.iterations}
+        out["batched_mixed_cg"] = {"ms": t3, "iterations": C.iterations}
+        out["max_rel_diff_of_correlators"] = max(
+            float(np.abs(M.values()[k] - va[k]).max() / np.abs(va[k]).max()) for M in (B, C) for k in va)
+        props = A.prop
+    corr = np.zeros((16, dims[0]))
+    for _ in range(3):
+        lat.meson_contract(POINT, tau, props, corr)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        lat.meson_contract(POINT, tau, props, corr)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.steps
+    nbytes = 12 * lat.field_doubles * 8
+    pk, kind = hbm_peak()
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    out["contraction"] = {"ms_per_call_incl_readback": ms, "algorithmic_bytes": nbytes, "GB_s": gbs,
+                          "peak_GB_s": pk, "peak_kind": kind, "frac": gbs / pk}
+    print(json.dumps(out))
+
+
 def run_ours(a, rank, world, dist):
     import torch
     import yahmc_b200 as yg
@@ -488,7 +567,9 @@ def main():
         dist_mod.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
         dist = dist_mod
     try:
-        if a.impl == "reference":
+        if a.mesons:
+            run_mesons(a)
+        elif a.impl == "reference":
             run_reference(a, rank, world)
         else:
             run_ours(a, rank, world, dist)
