@@ -264,8 +264,9 @@ def run_reference(a, rank, world):
 def run_mesons(a):
     """The point-source meson workload on one GPU: the 12 propagators of one source slice on a
     thermalised 48x24^3 SU(3) field (m = -0.6, prec 1e-20), solved one at a time with
-    calc_propagator (BiCGstab, the reference's path) and through the batched CG (FP64 and
-    mixed), then the sixteen-channel contraction timed with CUDA events."""
+    calc_propagator (BiCGstab, the reference's path) and through the batched solvers (BiCGstab
+    on D; CG on Hphi_sq, mixed and FP64), then the sixteen-channel contraction timed with CUDA
+    events."""
     import torch
     import yahmc_b200 as yg
     from yahmc_b200 import fields
@@ -307,14 +308,16 @@ def run_mesons(a):
             return e0.elapsed_time(e1), M
 
         t1, A = run()
-        t2, B = run(batched=True)
-        t3, C = run(batched=True, mixed=True)
+        t2, B = run(batched=True, solver="bicgstab")
+        t3, C = run(batched=True, solver="cg_mixed")
+        t4, D = run(batched=True, solver="cg")
         va = A.values()
         out["one_at_a_time_bicgstab"] = {"ms": t1, "iterations": A.iterations}
-        out["batched_fp64_cg"] = {"ms": t2, "iterations": B.iterations}
+        out["batched_bicgstab"] = {"ms": t2, "iterations": B.iterations}
         out["batched_mixed_cg"] = {"ms": t3, "iterations": C.iterations}
+        out["batched_fp64_cg"] = {"ms": t4, "iterations": D.iterations}
         out["max_rel_diff_of_correlators"] = max(
-            float(np.abs(M.values()[k] - va[k]).max() / np.abs(va[k]).max()) for M in (B, C) for k in va)
+            float(np.abs(M.values()[k] - va[k]).max() / np.abs(va[k]).max()) for M in (B, C, D) for k in va)
         props = A.prop
     corr = np.zeros((16, dims[0]))
     for _ in range(3):

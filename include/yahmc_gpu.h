@@ -193,6 +193,11 @@ int yg_cg_mixed(yg_lattice *lat, const yg_inv_par *par, double *x, double *b, yg
  * Sources must vanish on the open/SF boundary slices, as spinor_random's do. */
 int yg_cg_inverter_multi(yg_lattice *lat, const yg_inv_par *par, int nrhs, double *const *xs, double *const *bs,
                          int *iters);
+/* No reference counterpart: nrhs <= 16 bicgstab_inverter solves on Dphi (bicgstab.cpp:9-97,
+ * each system with its own scalars, stopping test and iteration count) sharing every operator
+ * application; even-odd lattices with d = 3 */
+int yg_bicgstab_inverter_multi(yg_lattice *lat, const yg_inv_par *par, int nrhs, double *const *xs,
+                               double *const *bs, int *iters);
 
 /* No reference counterpart: nrhs solves of Hphi_sq with FP32 inner iterations (the compressed
  * operator with FP32 links and clover blocks) and FP64 reliable updates, advanced together;
@@ -250,10 +255,12 @@ int yg_create_point_source(yg_lattice *lat, int n, int tau, double *src);
 int yg_create_semwall_source(yg_lattice *lat, int n, int tau, const double *z2, double *src);
 /* calc_propagator (propagator.cpp:75-166): dst holds the initial guess */
 int yg_calc_propagator(yg_lattice *lat, double mass, double prec, double *dst, double *src, int *iters);
-/* No reference counterpart: n <= 16 propagators of one source slice through the batched CG
- * (mixed = 1: FP32 inner iterations, d = 3), same stopping rule; dst[i] need no initial guess */
+/* No reference counterpart: n <= 16 propagators of one source slice (d = 3) with every operator
+ * application shared.  solver 0: batched BiCGstab on the even-site system (the reference's
+ * recurrence per system, dst[i] the initial guess); 1: batched mixed-precision CG on Hphi_sq;
+ * 2: batched FP64 CG on Hphi_sq (both from zero).  Same stopping rule as calc_propagator. */
 int yg_calc_propagator_multi(yg_lattice *lat, double mass, double prec, int n, double *const *dst,
-                             double *const *src, int mixed, int *iters);
+                             double *const *src, int solver, int *iters);
 /* contract_all_correlators (mesons.cpp:105-128): corr[16*T] += the slice sums of the sixteen
  * channels (order id g1 g2 g3 g5 g5g1 g5g2 g5g3 g0g1 g0g2 g0g3 g0g5 g0g5g1 g0g5g2 g0g5g3
  * g5_g0g5) at t - tau; props: 4 (SEMWALL) or 4*d (POINT, index spin*d + colour) fields */

@@ -97,14 +97,14 @@ def test_meson_measure(name, method, hits):
     assert len(M.lines()) == 16 and M.lines()[12].startswith("g0g5g1: ")
 
 
-@pytest.mark.parametrize("mixed", [False, True])
-def test_batched_propagators(mixed):
-    """the twelve point-source propagators of a slice through the batched CG agree with the
-    one-at-a-time BiCGstab solves, and so do the correlators"""
+@pytest.mark.parametrize("solver", ["bicgstab", "cg_mixed", "cg"])
+def test_batched_propagators(solver):
+    """the twelve point-source propagators of a slice through the batched solvers agree with
+    the one-at-a-time BiCGstab solves, and so do the correlators"""
     lat, O, rng = make_pair("su3_fund_ap", (8, 8, 8, 8), seed=75)
     A = Mesons(lat, -0.3, 1e-24, 1, POINT)
     A.measure(taus=[3])
-    B = Mesons(lat, -0.3, 1e-24, 1, POINT, batched=True, mixed=mixed)
+    B = Mesons(lat, -0.3, 1e-24, 1, POINT, batched=True, solver=solver)
     B.measure(taus=[3])
     assert lat.last_status == 0
     for n in (0, 5, 11):

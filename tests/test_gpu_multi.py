@@ -107,3 +107,36 @@ def test_mixed_multi_true_residuals(name):
             assert _true_residual(lat, "Hphi_sq", mass, xs[i], bs[i]) < prec
         if prec == 1e-24:
             assert sts[0]["iterations"] <= 1.5 * it64 + 10, (sts[0], it64)
+
+
+@pytest.mark.parametrize("name", ["su3_fund_ap", "su3_fund_open", "su3_fund_ap_nocl", "su2_adj_ap"])
+def test_bicgstab_multi_matches_single(name):
+    """Batched bicgstab_inverter on Dphi (yg_bicgstab_inverter_multi): each system reproduces
+    the single-system BiCGstab (bicgstab.cpp:9-97) to the accuracy its stopping rule implies,
+    with about its iteration count (the batched reductions add in another order), and system
+    0 matches the oracle."""
+    dims = (8, 8, 8, 8) if name.startswith("su3") else (4, 6, 4, 8)
+    lat, O, rng = make_pair(name, dims, seed=56)
+    nb, mass, prec = 5, -0.4, 1e-24
+    srcs = [source(O, rng) for _ in range(nb)]
+    guess = 0.01 * source(O, rng)
+    bs = [lat.field(s) for s in srcs]
+    xs = [lat.field() for _ in range(nb)]
+    lat.upload(xs[3], guess)
+    its = lat.bicgstab_inverter_multi("Dphi", mass, prec, xs, bs)
+    assert lat.last_status == 0
+    lo, hi = O.default_range()
+    for i in range(nb):
+        x1 = lat.field()
+        if i == 3:
+            lat.upload(x1, guess)
+        it1 = lat.bicgstab_inverter("Dphi", mass, prec, x1, bs[i])
+        assert abs(its[i] - it1) <= 4, (i, its, it1)
+        assert rel(lat.download(xs[i])[lo:hi], lat.download(x1)[lo:hi]) < 1e-8
+        assert _true_residual(lat, "Dphi", mass, xs[i], bs[i]) < 10 * prec
+    x_o = np.zeros_like(srcs[0])
+    it_o = O.bicgstab("Dphi", mass, prec, x_o, srcs[0].copy())
+    assert abs(its[0] - it_o) <= 4
+    assert rel(lat.download(xs[0])[lo:hi], x_o[lo:hi]) < 1e-8
+    with pytest.raises(Exception):
+        lat.bicgstab_inverter_multi("Hphi_sq", mass, prec, xs[:1], bs[:1])

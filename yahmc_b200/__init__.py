@@ -102,7 +102,7 @@ _SIGNATURES = {
     "yg_rational_calc": [_P, ctypes.POINTER(InvPar), _D, _I, _P, _P, _P, _P, ctypes.POINTER(_I)],
     "yg_cg_mixed": [_P, ctypes.POINTER(InvPar), _P, _P, ctypes.POINTER(SolveStats)],
     "yg_cg_mixed_opts": [_P, ctypes.POINTER(InvPar), ctypes.POINTER(MixedOpts), _P, _P, ctypes.POINTER(SolveStats)],
-    "yg_cg_inverter_multi": [_P, _P, _I, _P, _P, _P],
+    "yg_cg_inverter_multi": [_P, _P, _I, _P, _P, _P], "yg_bicgstab_inverter_multi": [_P, _P, _I, _P, _P, _P],
     "yg_cg_mixed_multi": [_P, _P, _I, _P, _P, _D, _P],
     "yg_inner_hop_profile": [_P, _D, _I, _P, _P],
     "yg_mre_init": [_P, _I, _I, _D, _P], "yg_mre_store": [_P, _P], "yg_mre_guess": [_P, _P, _P],
@@ -415,6 +415,22 @@ class Lattice:
             self._check(rc)
         return list(its)
 
+    def bicgstab_inverter_multi(self, op, mass, prec, xs, bs, log=0, maxiter=0):
+        """len(xs) bicgstab_inverter solves on Dphi sharing every operator application;
+        returns the iteration count of each system (2 per iteration, as the reference)"""
+        n = len(xs)
+        if n != len(bs):
+            raise ValueError("xs and bs differ in length")
+        par = self._par(op, mass, prec, log, maxiter)
+        px = (ctypes.c_void_p * n)(*[x.ptr for x in xs])
+        pb = (ctypes.c_void_p * n)(*[b.ptr for b in bs])
+        its = (ctypes.c_int * n)()
+        rc = self.lib.yg_bicgstab_inverter_multi(self.h, ctypes.byref(par), n, px, pb, its)
+        self.last_status = rc
+        if rc not in (0, 4):
+            self._check(rc)
+        return list(its)
+
     def tune_inner_links(self, mass):
         """times the FP32 link formats of the compressed inner operator on this lattice and
         keeps the fastest for cg_mixed's default; returns (link_reals, {reals: ms per hop})"""
@@ -448,15 +464,18 @@ class Lattice:
             self._check(rc)
         return it.value
 
-    def calc_propagator_multi(self, mass, prec, dsts, srcs, mixed=False):
-        """len(dsts) <= 16 propagators through the batched CG; returns the iteration counts"""
+    def calc_propagator_multi(self, mass, prec, dsts, srcs, solver="bicgstab"):
+        """len(dsts) <= 16 propagators with shared operator applications: solver "bicgstab"
+        (batched BiCGstab on the even-site system, dsts hold the initial guesses), "cg_mixed"
+        or "cg" (batched CG on Hphi_sq); returns the iteration counts"""
+        code = {"bicgstab": 0, "cg_mixed": 1, "cg": 2}[solver]
         n = len(dsts)
         if n != len(srcs):
             raise ValueError("dsts and srcs differ in length")
         pd = (ctypes.c_void_p * n)(*[x.ptr for x in dsts])
         ps = (ctypes.c_void_p * n)(*[b.ptr for b in srcs])
         its = (ctypes.c_int * n)()
-        rc = self.lib.yg_calc_propagator_multi(self.h, mass, prec, n, pd, ps, int(bool(mixed)), its)
+        rc = self.lib.yg_calc_propagator_multi(self.h, mass, prec, n, pd, ps, code, its)
         self.last_status = rc
         if rc not in (0, 4):
             self._check(rc)

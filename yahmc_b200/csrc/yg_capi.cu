@@ -265,6 +265,14 @@ int yg_cg_inverter_multi(yg_lattice *l, const yg_inv_par *p, int nrhs, double *c
     return yg::cg_multi(lat(l), *p, nrhs, xs, bs, iters);
   });
 }
+int yg_bicgstab_inverter_multi(yg_lattice *l, const yg_inv_par *p, int nrhs, double *const *xs, double *const *bs,
+                               int *iters) {
+  return guard_status([&] {
+    check_par(p); need(xs, "xs"); need(bs, "bs"); need(iters, "iters");
+    for (int i = 0; i < nrhs; i++) { need(xs[i], "xs[i]"); need(bs[i], "bs[i]"); }
+    return yg::bicgstab_multi(lat(l), *p, nrhs, xs, bs, iters);
+  });
+}
 int yg_cg_mixed_multi(yg_lattice *l, const yg_inv_par *p, int nrhs, double *const *xs, double *const *bs,
                       double delta, yg_solve_stats *stats) {
   return guard_status([&] {
@@ -319,11 +327,11 @@ int yg_calc_propagator(yg_lattice *l, double mass, double prec, double *dst, dou
   });
 }
 int yg_calc_propagator_multi(yg_lattice *l, double mass, double prec, int n, double *const *dst, double *const *src,
-                             int mixed, int *iters) {
+                             int solver, int *iters) {
   return guard_status([&] {
     need(dst, "dst"); need(src, "src");
     std::vector<int> it(n > 0 ? n : 1, 0);
-    const int st = yg::calc_propagator_multi(lat(l), mass, prec, n, dst, src, mixed != 0, it.data());
+    const int st = yg::calc_propagator_multi(lat(l), mass, prec, n, dst, src, solver, it.data());
     if (iters)
       for (int i = 0; i < n; i++) iters[i] = it[i];
     return st;

@@ -226,11 +226,13 @@ void create_point_source(Lattice &L, int n, int tau, double *src);
 void create_semwall_source(Lattice &L, int n, int tau, const double *z2, double *src);
 int calc_propagator(Lattice &L, double mass, double prec, double *dst, double *src, int *iters);
 int calc_propagator_multi(Lattice &L, double mass, double prec, int n, double *const *dst, double *const *src,
-                          bool mixed, int *iters);
+                          int solver, int *iters);
 void meson_contract(Lattice &L, int method, int tau, const double *const *props, int nprops, double *corr);
 
 // several cg_inverter solves sharing every operator application (yg_multi.cu)
 int cg_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, double *const *bs, int *iters);
+// several bicgstab_inverter solves on Dphi sharing every operator application (yg_multi.cu)
+int bicgstab_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, double *const *bs, int *iters);
 // the same systems with FP32 inner iterations and FP64 reliable updates (yg_multi.cu)
 int cg_mixed_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, double *const *bs, double delta,
                    yg_solve_stats *stats);

@@ -297,41 +297,48 @@ int calc_propagator(Lattice &L, double mass, double prec, double *dst, double *s
   return st;
 }
 
-// No reference counterpart: the nprop propagators of one source time slice solved together.
-// D x = b on the even sites is Hphi_sq y = g5 b with x = Hphi y (Hphi = g5 D is Hermitian), so
-// the systems go to the batched CG (FP32 inner iterations with FP64 reliable updates when
-// `mixed`), with the same |r|^2 / |b|^2 < prec as BiCGstab's; the odd sites as calc_propagator.
+// No reference counterpart: the n propagators of one source time slice solved together, with
+// every operator application shared.  solver 0: BiCGstab on the even-site system D x_e = b'
+// (the reference's recurrence per system, dst as the initial guess); 1, 2: CG on Hphi_sq y = g5 b'
+// with x_e = Hphi y (Hphi = g5 D is Hermitian), mixed precision (1) or FP64 (2), from zero.  All
+// stop on |r|^2 / |b'|^2 < prec; the odd sites follow as in calc_propagator.
 int calc_propagator_multi(Lattice &L, double mass, double prec, int n, double *const *dst, double *const *src,
-                          bool mixed, int *iters) {
+                          int solver, int *iters) {
   if (!L.p.eo) throw Error(YG_ERR_ARG, "the batched propagator needs even-odd preconditioning");
   if (n < 1 || n > 16) throw Error(YG_ERR_ARG, "1..16 propagators");
+  if (solver < 0 || solver > 2) throw Error(YG_ERR_ARG, "solver: 0 BiCGstab, 1 mixed CG, 2 FP64 CG");
   double *tmp = L.scratch_field(kPropTmp);
   std::vector<double *> rhs(n), y(n);
   for (int i = 0; i < n; i++) {
     if (!dst[i] || !src[i]) throw Error(YG_ERR_ARG, "null field");
     rhs[i] = L.scratch_field(kPropPool + i);
-    y[i] = L.scratch_field(kPropPool + 16 + i);
     eo_source(L, mass, rhs[i], src[i], tmp);
-    blas_g5(L, rhs[i], 0, L.Vh);
-    blas_zero(L, y[i], 0, L.V);
   }
   yg_inv_par par{};
-  par.op = YG_OP_HPHI_SQ;
   par.mass = mass;
   par.prec = prec;
   int st;
-  if (mixed) {
-    std::vector<yg_solve_stats> ss(n);
-    st = cg_mixed_multi(L, par, n, y.data(), rhs.data(), 0.1, ss.data());
-    if (iters)
-      for (int i = 0; i < n; i++) iters[i] = ss[i].iterations;
+  if (solver == 0) {
+    par.op = YG_OP_DPHI;
+    st = bicgstab_multi(L, par, n, dst, rhs.data(), iters);
   } else {
-    st = cg_multi(L, par, n, y.data(), rhs.data(), iters);
+    for (int i = 0; i < n; i++) {
+      y[i] = L.scratch_field(kPropPool + 16 + i);
+      blas_g5(L, rhs[i], 0, L.Vh);
+      blas_zero(L, y[i], 0, L.V);
+    }
+    par.op = YG_OP_HPHI_SQ;
+    if (solver == 1) {
+      std::vector<yg_solve_stats> ss(n);
+      st = cg_mixed_multi(L, par, n, y.data(), rhs.data(), 0.1, ss.data());
+      if (iters)
+        for (int i = 0; i < n; i++) iters[i] = ss[i].iterations;
+    } else {
+      st = cg_multi(L, par, n, y.data(), rhs.data(), iters);
+    }
+    for (int i = 0; i < n; i++) hphi(L, mass, dst[i], y[i]);
   }
-  for (int i = 0; i < n; i++) {
-    hphi(L, mass, dst[i], y[i]);
-    odd_sites(L, mass, dst[i], src[i], tmp);
-  }
+  for (int i = 0; i < n; i++) odd_sites(L, mass, dst[i], src[i], tmp);
   return st;
 }
 

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <vector>
 #include "yg_dirac_impl.cuh"
@@ -429,8 +430,10 @@ struct Multi {
 
 }  // namespace
 
-// dst = Hphi src (one Schur operator with gamma5) on batched fields; tmp takes the odd sites
-static void hphi_multi(Lattice &L, int nb, double mass, double2 *dst, const double2 *src, double2 *tmp) {
+// dst = Hphi src (one Schur operator with gamma5; g5 = 0: Dphi) on batched fields; tmp takes the
+// odd sites
+static void hphi_multi(Lattice &L, int nb, double mass, double2 *dst, const double2 *src, double2 *tmp,
+                       int g5 = 1) {
   if (L.d != 3) throw Error(YG_ERR_ARG, "the batched operator is built for d = 3");
   MultiHopArgs a{};
   a.g = L.g;
@@ -456,7 +459,7 @@ static void hphi_multi(Lattice &L, int nb, double mass, double2 *dst, const doub
   s2.coeff = -0.5;
   s2.lo = 0;
   s2.n = (int)L.Vh;
-  s2.g5 = 1;
+  s2.g5 = g5;
   s2.diag = a.clover ? 4.0 + mass : (4.0 + mass) * (4.0 + mass);
   // blocks of S sites x nb systems (about 192 threads), shared memory for S sites
   const int S = std::min(24, std::max(1, 192 / nb));      // <= 24 sites: 42 KB of shared memory
@@ -569,6 +572,189 @@ int cg_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, dou
       for (int i = 0; i < nb; i++)
         fprintf(stderr, "[INVERTER][30]cg_multi[%d]: iterations = %d, precision = %1.4e\n", i, it[i],
                 rr[i] / norm[i]);
+  } catch (...) {
+    for (double2 *b : bufs) cudaFree(b);
+    throw;
+  }
+  for (double2 *b : bufs) cudaFree(b);
+  return status;
+}
+
+// ---- batched BiCGstab (complex per-system scalars)
+struct MultiC {
+  double2 c[kMaxRhs];
+};
+
+// <a_i, b_i> = sum a conj(b): per-system partials of the real and imaginary parts
+__global__ void k_multi_cdot(double *part_re, double *part_im, const double2 *a, const double2 *b, long w0, long cnt,
+                             int nb) {
+  const long n = cnt * nb, base = w0 * nb;
+  double re = 0, im = 0;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const double2 x = a[base + e], y = b[base + e];
+    re = fma(x.x, y.x, fma(x.y, y.y, re));
+    im = fma(x.y, y.x, fma(-x.x, y.y, im));
+  }
+  block_partials(re, part_re, nb);
+  __syncthreads();
+  block_partials(im, part_im, nb);
+}
+
+// y_i += c_i x_i (c_i = 0 leaves system i alone)
+__global__ void k_multi_caxpy(double2 *y, const double2 *x, MultiC c, long w0, long cnt, int nb) {
+  const long n = cnt * nb, base = w0 * nb;
+  const double2 k = c.c[threadIdx.x % nb];
+  if (k.x == 0.0 && k.y == 0.0) return;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const double2 xv = x[base + e];
+    double2 yv = y[base + e];
+    yv.x = fma(k.x, xv.x, fma(-k.y, xv.y, yv.x));
+    yv.y = fma(k.x, xv.y, fma(k.y, xv.x, yv.y));
+    y[base + e] = yv;
+  }
+}
+
+// p_i = beta_i p_i + r_i - (beta_i omega_i) v_i for the systems flagged in `on`
+__global__ void k_multi_bicg_p(double2 *p, const double2 *r, const double2 *v, MultiC beta, MultiC bw,
+                               MultiScalars on, long w0, long cnt, int nb) {
+  const long n = cnt * nb, base = w0 * nb;
+  const int i = threadIdx.x % nb;
+  if (on.a[i] == 0.0) return;
+  const double2 be = beta.c[i], w = bw.c[i];
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const double2 pv = p[base + e], rv = r[base + e], vv = v[base + e];
+    double2 o;
+    o.x = be.x * pv.x - be.y * pv.y + rv.x - (w.x * vv.x - w.y * vv.y);
+    o.y = be.x * pv.y + be.y * pv.x + rv.y - (w.x * vv.y + w.y * vv.x);
+    p[base + e] = o;
+  }
+}
+
+// nrhs bicgstab_inverter solves on Dphi (bicgstab.cpp:9-97, each system with its own complex
+// scalars and stopping test) sharing every operator application; iters[i] = 2 x the system's
+// iterations, as the reference counts them
+int bicgstab_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, double *const *bs, int *iters) {
+  using zc = std::complex<double>;
+  if (nrhs < 1 || nrhs > kMaxRhs) throw Error(YG_ERR_ARG, "1..16 right-hand sides");
+  if (!L.p.eo) throw Error(YG_ERR_ARG, "the batched BiCGstab needs even-odd preconditioning");
+  if (L.d != 3) throw Error(YG_ERR_ARG, "the batched operator is built for d = 3");
+  if (par.op != YG_OP_DPHI) throw Error(YG_ERR_ARG, "the batched BiCGstab solves Dphi systems");
+  Multi m(L, nrhs);
+  const int nb = nrhs;
+  double2 *X = m.field(), *B = m.field(), *R = m.field(), *R0 = m.field(), *P = m.field(), *V = m.field(),
+          *T = m.field(), *TMP = m.field();
+  std::vector<double2 *> bufs = {X, B, R, R0, P, V, T, TMP};
+  DevBuf part_im;
+  int status = YG_OK;
+  try {
+    part_im.alloc(sizeof(double) * (size_t)m.grid * nb);
+    auto dphi = [&](double2 *dst, double2 *src) {
+      hphi_multi(L, nb, par.mass, dst, src, TMP, 0);
+      bc_zero_multi(L, nb, src);
+    };
+    auto cdot = [&](const double2 *a, const double2 *b) {
+      k_multi_cdot<<<m.grid, m.threads, 0, L.stream>>>(m.part.as<double>(), part_im.as<double>(), a, b, m.w0, m.cnt,
+                                                       nb);
+      YG_LAUNCHED();
+      std::vector<double> hi((size_t)m.grid * nb);
+      YG_CUDA(cudaMemcpyAsync(hi.data(), part_im.p, sizeof(double) * hi.size(), cudaMemcpyDeviceToHost, L.stream));
+      std::vector<double> re = m.sums();          // synchronises the stream
+      std::vector<zc> out(nb);
+      for (int i = 0; i < nb; i++) {
+        double im = 0;
+        for (int blk = 0; blk < m.grid; blk++) im += hi[(size_t)blk * nb + i];
+        out[i] = zc(re[i], im);
+      }
+      return out;
+    };
+    auto caxpy = [&](double2 *y, const double2 *x, const std::vector<zc> &c) {
+      MultiC k{};
+      for (int i = 0; i < nb; i++) k.c[i] = make_double2(c[i].real(), c[i].imag());
+      k_multi_caxpy<<<m.grid, m.threads, 0, L.stream>>>(y, x, k, m.w0, m.cnt, nb);
+      YG_LAUNCHED();
+    };
+    FieldPtrs fx{}, fb{};
+    for (int i = 0; i < nb; i++) {
+      fx.f[i] = (double2 *)xs[i];
+      fb.f[i] = (double2 *)bs[i];
+    }
+    const long wall = (long)L.V * 4 * L.d;
+    k_multi_pack<<<nblk(wall * nb, 256), 256, 0, L.stream>>>(X, fx, 0, wall, nb, 0);
+    YG_LAUNCHED();
+    k_multi_pack<<<nblk(wall * nb, 256), 256, 0, L.stream>>>(B, fb, 0, wall, nb, 0);
+    YG_LAUNCHED();
+    // r = b - D x ; r0 = p = r
+    dphi(P, X);
+    k_multi_sub<<<m.grid, m.threads, 0, L.stream>>>(R, B, P, m.w0, m.cnt, nb);
+    YG_LAUNCHED();
+    YG_CUDA(cudaMemcpyAsync(R0, R, sizeof(double2) * (size_t)wall * nb, cudaMemcpyDeviceToDevice, L.stream));
+    YG_CUDA(cudaMemcpyAsync(P, R, sizeof(double2) * (size_t)wall * nb, cudaMemcpyDeviceToDevice, L.stream));
+    std::vector<double> norm = m.sqnorm(B);
+    std::vector<zc> rho0 = cdot(R, R0);
+    std::vector<int> active(nb), it(nb, 0);
+    std::vector<double> res(nb);
+    int nactive = 0;
+    for (int i = 0; i < nb; i++) {
+      res[i] = rho0[i].real();
+      active[i] = !(res[i] < norm[i] * par.prec);   // bicgstab.cpp:48-53: 0 iterations
+      nactive += active[i];
+    }
+    int k = 0;
+    std::vector<zc> alpha(nb), omega(nb), zero(nb, zc(0, 0));
+    while (nactive > 0) {
+      k++;
+      if (par.maxiter > 0 && k > par.maxiter) { status = YG_MAXITER; break; }
+      dphi(V, P);
+      std::vector<zc> vr0 = cdot(V, R0);
+      for (int i = 0; i < nb; i++) {
+        alpha[i] = active[i] ? rho0[i] / vr0[i] : zc(0, 0);
+        if (active[i] && !std::isfinite(alpha[i].real())) throw Error(YG_NONFINITE, "non-finite value in bicgstab_multi");
+      }
+      std::vector<zc> nalpha(nb);
+      for (int i = 0; i < nb; i++) nalpha[i] = -alpha[i];
+      caxpy(R, V, nalpha);                          // r -= alpha v
+      dphi(T, R);
+      std::vector<zc> rt = cdot(R, T);
+      std::vector<double> tt = m.sqnorm(T);
+      for (int i = 0; i < nb; i++) omega[i] = active[i] ? rt[i] / tt[i] : zc(0, 0);
+      caxpy(X, P, alpha);                           // x += alpha p + omega r
+      caxpy(X, R, omega);
+      std::vector<zc> nomega(nb);
+      for (int i = 0; i < nb; i++) nomega[i] = -omega[i];
+      caxpy(R, T, nomega);                          // r -= omega t
+      std::vector<zc> rho1 = cdot(R, R0);
+      std::vector<double> rr = m.sqnorm(R);
+      MultiC be{}, bw{};
+      MultiScalars on{};
+      for (int i = 0; i < nb; i++) {
+        if (!active[i]) continue;
+        it[i] = k;
+        const zc beta = (rho1[i] / rho0[i]) * (alpha[i] / omega[i]);
+        res[i] = rr[i];
+        if (rr[i] < norm[i] * par.prec) {         // bicgstab.cpp:77-81: stop before rho0 = rho1
+          active[i] = 0;
+          nactive--;
+          continue;
+        }
+        be.c[i] = make_double2(beta.real(), beta.imag());
+        const zc w = beta * omega[i];
+        bw.c[i] = make_double2(w.real(), w.imag());
+        on.a[i] = 1.0;
+        rho0[i] = rho1[i];
+      }
+      if (nactive > 0) {
+        k_multi_bicg_p<<<m.grid, m.threads, 0, L.stream>>>(P, R, V, be, bw, on, m.w0, m.cnt, nb);
+        YG_LAUNCHED();
+      }
+    }
+    k_multi_pack<<<nblk(m.cnt * nb, 256), 256, 0, L.stream>>>(X, fx, m.w0, m.cnt, nb, 1);
+    YG_LAUNCHED();
+    YG_CUDA(cudaStreamSynchronize(L.stream));
+    for (int i = 0; i < nb; i++) iters[i] = 2 * it[i];
+    if (par.log)
+      for (int i = 0; i < nb; i++)
+        fprintf(stderr, "[INVERTER][30]bicgstab_multi[%d]: iterations = %d, precision = %1.4e\n", i, 2 * it[i],
+                res[i] / norm[i]);
   } catch (...) {
     for (double2 *b : bufs) cudaFree(b);
     throw;

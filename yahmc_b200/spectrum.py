@@ -27,10 +27,11 @@ SQRT2INV = 0.70710678118654752440084436210
 
 class Mesons:
     """meson_init(mass, prec, hits, method), mesons.cpp:150-209.  ``batched`` solves the
-    propagators of a source slice together (yg_calc_propagator_multi, even-odd lattices)
-    instead of one auto_inverter call each; ``mixed`` uses the batched mixed-precision CG."""
+    propagators of a source slice together (yg_calc_propagator_multi, even-odd lattices, d = 3)
+    instead of one auto_inverter call each, with ``solver`` "bicgstab" (default), "cg_mixed"
+    or "cg"; ``mixed`` = True selects "cg_mixed"."""
 
-    def __init__(self, lat, mass, prec, hits, method, rng=None, batched=False, mixed=False):
+    def __init__(self, lat, mass, prec, hits, method, rng=None, batched=False, mixed=False, solver=None):
         self.lat, self.mass, self.prec, self.hits = lat, mass, prec, int(hits)
         self.method = SEMWALL if method == SEMWALL else POINT
         self.T = lat.dims[0]
@@ -38,7 +39,8 @@ class Mesons:
         self.norm = self.vol3 if self.method == SEMWALL else 1
         self.ninv = 4 if self.method == SEMWALL else 4 * lat.d
         self.rng = rng if rng is not None else np.random.default_rng()
-        self.batched, self.mixed = batched, mixed
+        self.batched = batched
+        self.solver = solver or ("cg_mixed" if mixed else "bicgstab")
         self.source = lat.field()
         self.prop = [lat.field() for _ in range(self.ninv)]
         self.sources = [lat.field() for _ in range(self.ninv)] if batched else None
@@ -75,7 +77,7 @@ class Mesons:
         for lo in range(0, self.ninv, 16):
             hi = min(lo + 16, self.ninv)
             its = lat.calc_propagator_multi(self.mass, self.prec, self.prop[lo:hi], self.sources[lo:hi],
-                                            mixed=self.mixed)
+                                            solver=self.solver)
             self.iterations += sum(its)
 
     def measure(self, taus=None, noises=None):
