@@ -75,6 +75,9 @@ def parse():
     ap.add_argument("--mesons", action="store_true",
                     help="time the 12 point-source propagators of one slice (one at a time and batched) and the "
                          "16-channel contraction on 48x24x24x24 (not the bench line)")
+    ap.add_argument("--lattices", action="store_true",
+                    help="time FP64 CG solves on 8^4, 12^4 and 16^4 lattices one after another and "
+                         "concurrently (yg_cg_inverter_lattices; not the bench line)")
     ap.add_argument("--contract-only", action="store_true",
                     help="with --mesons: only the contraction, on random propagators (for profiling)")
     return ap.parse_args()
@@ -338,6 +341,53 @@ def run_mesons(a):
     print(json.dumps(out))
 
 
+def run_lattices(a):
+    """FP64 CG (Hphi_sq, m = -0.6, prec 1e-20) on SU(3) fundamental 8^4, 12^4 and 16^4 lattices
+    with thermalised-like fields from the engine's own HMC (20 trajectories each): the three
+    solves one after another, then through one yg_cg_inverter_lattices call."""
+    import torch
+    import yahmc_b200 as yg
+    from yahmc_b200 import fields
+    torch.cuda.set_device(0)
+    yg.set_device(0)
+    solves = []
+    for k, L in enumerate((8, 12, 16)):
+        dims = (L, L, L, L)
+        U, plaq, _ = thermalised_links(dims, a.seed + k, trajectories=20)
+        lat = yg.Lattice(dims, nc=3, repr="fundamental", bc="antiperiodic", clover=True, eo=True, csw=CSW)
+        lat.set_links(U)
+        b = lat.field(fields.gaussian_spinor(lat.V, 3, np.random.default_rng(a.seed + 100 + k)))
+        solves.append((lat, -0.6, 1e-20, lat.field(), b))
+
+    def sequential():
+        its = []
+        for lat, m, pr, x, b in solves:
+            lat.spinor_zero(x)
+            its.append(lat.cg_inverter("Hphi_sq", m, pr, x, b))
+        return its
+
+    def concurrent():
+        for lat, m, pr, x, b in solves:
+            lat.spinor_zero(x)
+        return yg.cg_inverter_lattices(solves)[0]
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            its = fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3 / a.steps, its
+
+    t_seq, it_seq = timed(sequential)
+    t_con, it_con = timed(concurrent)
+    print(json.dumps({"workload": "FP64 CG on Hphi_sq, SU(3) fund even-odd Wilson-clover 8^4 + 12^4 + 16^4",
+                      "sequential_ms": t_seq, "concurrent_ms": t_con, "speedup": t_seq / t_con,
+                      "iterations": it_seq, "iterations_concurrent": it_con,
+                      "timing": "host wall clock around the solves, synchronised, mean of --steps"}))
+
+
 def run_ours(a, rank, world, dist):
     import torch
     import yahmc_b200 as yg
@@ -572,6 +622,8 @@ def main():
     try:
         if a.mesons:
             run_mesons(a)
+        elif a.lattices:
+            run_lattices(a)
         elif a.impl == "reference":
             run_reference(a, rank, world)
         else:

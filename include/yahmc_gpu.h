@@ -193,6 +193,13 @@ int yg_cg_mixed(yg_lattice *lat, const yg_inv_par *par, double *x, double *b, yg
  * Sources must vanish on the open/SF boundary slices, as spinor_random's do. */
 int yg_cg_inverter_multi(yg_lattice *lat, const yg_inv_par *par, int nrhs, double *const *xs, double *const *bs,
                          int *iters);
+/* No reference counterpart: n <= 64 independent cg_inverter solves, one per lattice (lattices of
+ * any sizes and configurations, each at most once), run concurrently: a host thread and the
+ * lattice's own stream per solve, so small lattices that leave the GPU mostly idle overlap.
+ * Results and iteration counts are those of separate yg_cg_inverter calls; returns the worst
+ * status.  The calling thread's current device is used for all of them. */
+int yg_cg_inverter_lattices(int n, yg_lattice *const *lats, const yg_inv_par *pars, double *const *xs,
+                            double *const *bs, int *iters);
 /* No reference counterpart: nrhs <= 16 bicgstab_inverter solves on Dphi (bicgstab.cpp:9-97,
  * each system with its own scalars, stopping test and iteration count) sharing every operator
  * application; even-odd lattices with d = 3 */

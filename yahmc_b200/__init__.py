@@ -24,7 +24,7 @@ import numpy as np
 
 from .fields import complex_to_raw, raw_to_complex
 
-__all__ = ["Lattice", "Field", "YGError", "load_library", "LIB_PATH",
+__all__ = ["Lattice", "Field", "YGError", "load_library", "LIB_PATH", "cg_inverter_lattices",
            "VIEW_DEFAULT", "VIEW_EVEN", "VIEW_ODD", "VIEW_FULL", "OP_DPHI", "OP_HPHI", "OP_HPHI_SQ"]
 
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libyahmc_b200.so"
@@ -110,7 +110,7 @@ _SIGNATURES = {
     "yg_create_point_source": [_P, _I, _I, _P], "yg_create_semwall_source": [_P, _I, _I, _P, _P],
     "yg_calc_propagator": [_P, _D, _D, _P, _P, _P], "yg_calc_propagator_multi": [_P, _D, _D, _I, _P, _P, _I, _P],
     "yg_meson_contract": [_P, _I, _I, _P, _I, _P],
-    "yg_tune_inner_links": [_P, _D, _P, _P],
+    "yg_tune_inner_links": [_P, _D, _P, _P], "yg_cg_inverter_lattices": [_I, _P, _P, _P, _P, _P],
     "yg_wf_init": [_P], "yg_wf_zeta": [_P, _D], "yg_wf_update": [_P, _D], "yg_wf_iterate": [_P, _D],
     "yg_wf_observables": [_P, _P, _P, _P], "yg_wf_fermion_init": [_P, _I], "yg_wf_fermion_iterate": [_P, _D, _P, _I],
     "yg_gauge_save_cfg": [_P, ctypes.c_char_p, _I, _I], "yg_gauge_load_cfg": [_P, ctypes.c_char_p, _P, _P, _P],
@@ -175,6 +175,22 @@ def set_device(device: int) -> None:
     lib = load_library()
     if lib.yg_set_device(int(device)) != 0:
         raise YGError(1, lib.yg_last_error().decode())
+
+
+def cg_inverter_lattices(solves, op="Hphi_sq"):
+    """Independent cg_inverter solves on several lattices at once (yg_cg_inverter_lattices):
+    `solves` is a list of (lattice, mass, prec, x, b); returns (iteration counts, status)."""
+    lib = load_library()
+    n = len(solves)
+    lats = (ctypes.c_void_p * n)(*[s[0].h for s in solves])
+    pars = (InvPar * n)(*[Lattice._par(op, s[1], s[2]) for s in solves])
+    xs = (ctypes.c_void_p * n)(*[s[3].ptr for s in solves])
+    bs = (ctypes.c_void_p * n)(*[s[4].ptr for s in solves])
+    its = (ctypes.c_int * n)()
+    rc = lib.yg_cg_inverter_lattices(n, lats, pars, xs, bs, its)
+    if rc not in (0, 4):
+        raise YGError(rc, lib.yg_last_error().decode())
+    return list(its), rc
 
 
 def launch_count() -> int:

@@ -60,7 +60,7 @@ extern "C" {
 
 const char *yg_last_error(void) { return g_last_error.c_str(); }
 
-long yg_launch_count(void) { return yg::g_launch_count; }
+long yg_launch_count(void) { return yg::g_launch_count.load(); }
 
 int yg_set_device(int device) {
   return guard([&] {
@@ -263,6 +263,19 @@ int yg_cg_inverter_multi(yg_lattice *l, const yg_inv_par *p, int nrhs, double *c
     check_par(p); need(xs, "xs"); need(bs, "bs"); need(iters, "iters");
     for (int i = 0; i < nrhs; i++) { need(xs[i], "xs[i]"); need(bs[i], "bs[i]"); }
     return yg::cg_multi(lat(l), *p, nrhs, xs, bs, iters);
+  });
+}
+int yg_cg_inverter_lattices(int n, yg_lattice *const *lats, const yg_inv_par *pars, double *const *xs,
+                            double *const *bs, int *iters) {
+  return guard_status([&] {
+    need(lats, "lats"); need(pars, "pars"); need(xs, "xs"); need(bs, "bs"); need(iters, "iters");
+    if (n < 1 || n > 64) throw yg::Error(YG_ERR_ARG, "1..64 lattices");
+    std::vector<yg::Lattice *> L(n);
+    for (int i = 0; i < n; i++) {
+      check_par(&pars[i]); need(xs[i], "xs[i]"); need(bs[i], "bs[i]");
+      L[i] = &lat(lats[i]);
+    }
+    return yg::cg_lattices(n, L.data(), pars, xs, bs, iters);
   });
 }
 int yg_bicgstab_inverter_multi(yg_lattice *l, const yg_inv_par *p, int nrhs, double *const *xs, double *const *bs,

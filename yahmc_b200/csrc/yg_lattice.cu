@@ -16,7 +16,7 @@
 
 namespace yg {
 
-long g_launch_count = 0;
+std::atomic<long> g_launch_count{0};
 
 void check_cuda(cudaError_t e, const char *what) {
   if (e != cudaSuccess) {

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <string>
 #include <vector>
 #include <stdexcept>
@@ -21,8 +22,9 @@ void check_cuda(cudaError_t e, const char *what);
 #define YG_CUDA(x) ::yg::check_cuda((x), #x)
 
 // Kernels launched by this library since load (all lattices).  Every launch site is followed
-// by YG_LAUNCHED(), which checks the launch and counts it; callers are single-threaded.
-extern long g_launch_count;
+// by YG_LAUNCHED(), which checks the launch and counts it (atomically: the concurrent
+// per-lattice solves launch from several host threads).
+extern std::atomic<long> g_launch_count;
 #define YG_LAUNCHED()                                              \
   do {                                                             \
     ::yg::check_cuda(cudaGetLastError(), "kernel launch");         \
@@ -170,6 +172,8 @@ void f_xpay(Lattice &L, float *p, float b, const float *r, long cnt);
 
 // ---- yg_solvers.cu
 int cg(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
+// cg on several lattices at once, one host thread and the lattice's own stream each (yg_solvers.cu)
+int cg_lattices(int n, Lattice *const *L, const yg_inv_par *par, double *const *xs, double *const *bs, int *iters);
 int cg_mshift(Lattice &L, const yg_inv_par &par, int num, const double *shift, double *const *xs, double *b, int *iters);
 int bicgstab(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
 int minres(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);

@@ -9,6 +9,8 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <exception>
+#include <thread>
 #include <vector>
 #include "yg_lattice.h"
 
@@ -81,6 +83,40 @@ int cg(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters) {
   log_line(par, "cg", it, rr / norm);
   *iters = it;
   return status;
+}
+
+// No reference counterpart: independent cg_inverter solves on lattices of any sizes at once.
+// A small lattice's CG is bound by kernel and reduction latency and leaves most of the GPU
+// idle, so each lattice's solve runs in its own host thread on the lattice's own stream and
+// the solves overlap on the device.  Every solve is the single-lattice cg, so results and
+// iteration counts are those of one-at-a-time calls.  Returns the worst status.
+int cg_lattices(int n, Lattice *const *L, const yg_inv_par *par, double *const *xs, double *const *bs, int *iters) {
+  if (n < 1 || n > 64) throw Error(YG_ERR_ARG, "1..64 lattices");
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < i; j++)
+      if (L[i] == L[j]) throw Error(YG_ERR_ARG, "each lattice may appear once (its scratch fields are per solve)");
+  int dev = 0;
+  YG_CUDA(cudaGetDevice(&dev));
+  std::vector<int> st(n, YG_OK);
+  std::vector<std::exception_ptr> err(n);
+  std::vector<std::thread> th;
+  th.reserve(n);
+  for (int i = 0; i < n; i++)
+    th.emplace_back([&, i] {
+      try {
+        YG_CUDA(cudaSetDevice(dev));
+        st[i] = cg(*L[i], par[i], xs[i], bs[i], &iters[i]);
+      } catch (...) {
+        err[i] = std::current_exception();
+      }
+    });
+  for (auto &t : th) t.join();
+  for (int i = 0; i < n; i++)
+    if (err[i]) std::rethrow_exception(err[i]);
+  int worst = YG_OK;
+  for (int s : st)
+    if (s != YG_OK) worst = s;
+  return worst;
 }
 
 // cg_mshift, cg.cpp:11-130
