@@ -78,6 +78,9 @@ def parse():
     ap.add_argument("--lattices", action="store_true",
                     help="time FP64 CG solves on 8^4, 12^4 and 16^4 lattices one after another and "
                          "concurrently (yg_cg_inverter_lattices; not the bench line)")
+    ap.add_argument("--mshift", action="store_true",
+                    help="time a 12-shift cg_mshift on SU(2) adjoint 48x24x24x24 against the 12 shifted "
+                         "systems solved one at a time (not the bench line)")
     ap.add_argument("--contract-only", action="store_true",
                     help="with --mesons: only the contraction, on random propagators (for profiling)")
     return ap.parse_args()
@@ -339,6 +342,49 @@ def run_mesons(a):
     out["contraction"] = {"ms_per_call_incl_readback": ms, "algorithmic_bytes": nbytes, "GB_s": gbs,
                           "peak_GB_s": pk, "peak_kind": kind, "frac": gbs / pk}
     print(json.dumps(out))
+
+
+def run_mshift(a):
+    """The RHMC-shaped multishift solve: SU(2) adjoint (d = 3, real links stored complex)
+    48x24x24x24 even-odd Wilson-clover on a Haar-random field, m = -0.2, Hphi_sq + s_k for 12
+    shifts log-spaced on [1e-4, 8] (the pole range of an RHMC approximation), prec 1e-20; one
+    cg_mshift call against the 12 systems solved one at a time (one shift per call), CUDA events."""
+    import torch
+    import yahmc_b200 as yg
+    from yahmc_b200 import fields
+    torch.cuda.set_device(0)
+    yg.set_device(0)
+    dims = (48, 24, 24, 24)
+    lat = yg.Lattice(dims, nc=2, repr="adjoint", bc="antiperiodic", clover=True, eo=True, csw=CSW)
+    rng = np.random.default_rng(a.seed)
+    lat.set_links(fields.haar_su(2, lat.V * 4, rng).reshape(lat.V, 4, 2, 2))
+    b = lat.field(fields.gaussian_spinor(lat.V, 3, rng))
+    shifts = np.geomspace(1e-4, 8.0, 12)
+    xs = [lat.field() for _ in shifts]
+    mass, prec = -0.2, 1e-20
+
+    def ev_time(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), r
+
+    def together():
+        return lat.cg_mshift("Hphi_sq", mass, prec, shifts, xs, b)
+
+    def apart():
+        return [lat.cg_mshift("Hphi_sq", mass, prec, shifts[k:k + 1], xs[k:k + 1], b) for k in range(len(shifts))]
+
+    t1, it1 = ev_time(together)
+    t2, it2 = ev_time(apart)
+    print(json.dumps({"workload": "12-shift CG on Hphi_sq + s, SU(2) adjoint 48x24x24x24 even-odd Wilson-clover, "
+                                  "Haar-random links", "shifts": list(shifts), "mass": mass, "prec_squared": prec,
+                      "cg_mshift_ms": t1, "cg_mshift_iterations": it1, "one_shift_at_a_time_ms": t2,
+                      "one_shift_iterations": it2, "speedup": t2 / t1}))
 
 
 def run_lattices(a):
@@ -624,6 +670,8 @@ def main():
             run_mesons(a)
         elif a.lattices:
             run_lattices(a)
+        elif a.mshift:
+            run_mshift(a)
         elif a.impl == "reference":
             run_reference(a, rank, world)
         else:
