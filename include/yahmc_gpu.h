@@ -6,8 +6,8 @@
  * inverters, the spinor-field linear algebra and the fermion forces.  Every
  * entry point below names the reference function it replaces (file:line in
  * the YaHMC tree).  A C++ shim with YaHMC's own signatures (dirac.h,
- * inverter.h, linalg.h, clover.h, forces.h) sits on top of this ABI; see
- * INTEGRATION.md.
+ * inverter.h, linalg.h, clover.h, forces.h) sits on top of this ABI
+ * (integration/yahmc_gpu_shim.cpp).
  *
  * Conventions
  *  - Plain C types only.  Every function returns an int status (yg_status);
@@ -350,9 +350,12 @@ int yg_gauge_restore(yg_lattice *lat);                                          
  * lattice handle needed): sum of |a_i|^2 over n_words complex FP64 words at dev_words,
  * written to the device double *dev_out on the given stream (NULL = legacy default).
  * Uses a fixed 128 KiB scratch array inside the library instead of cudaMalloc, so
- * n_words <= 16,777,216 (larger sizes return YG_ERR_ARG).  The first call on a device
- * looks up that array's device address and should come before any stream capture;
- * calls that overlap on the GPU share the array and race. */
+ * n_words <= 16,777,216 (larger sizes return YG_ERR_ARG).  dev_words must be 16-byte
+ * aligned (the words are read as pairs of doubles) and dev_out 8-byte aligned; other
+ * pointers return YG_ERR_ARG before anything is launched.  The first call on a device
+ * looks up that array's device address (cached per process, safe from several host
+ * threads) and should come before any stream capture; calls that overlap on the GPU
+ * share the array and race. */
 int yg_field_sqnorm_noalloc(const double *dev_words, long n_words, double *dev_out, void *stream);
 
 #ifdef __cplusplus

@@ -27,7 +27,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-DEFAULT_SRC = Path(os.environ.get("YAHMC_REFERENCE_SRC", "/root/reference"))
+DEFAULT_SRC = Path(os.environ.get("YAHMC_REFERENCE_SRC", HERE.parent.parent / "reference"))
 
 # name -> (NC, REPR, BC, clover, even-odd)
 CONFIGS = {

@@ -46,3 +46,17 @@ def test_lattice_creation_fails_loudly_without_gpu():
     from yahmc_b200 import Lattice, YGError
     with pytest.raises(YGError):
         Lattice((4, 4, 4, 4))
+
+
+def test_noalloc_rejects_misaligned_pointers_before_any_cuda_call():
+    """yg_field_sqnorm_noalloc checks its pointers on the host first: a misaligned view is
+    an argument error even on a machine without a GPU (nothing is dereferenced)."""
+    from yahmc_b200 import LIB_PATH
+    lib = ctypes.CDLL(str(LIB_PATH))
+    lib.yg_field_sqnorm_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p]
+    lib.yg_last_error.restype = ctypes.c_char_p
+    assert lib.yg_field_sqnorm_noalloc(0x10008, 4, 0x20000, None) == 1
+    assert b"16-byte" in lib.yg_last_error()
+    assert lib.yg_field_sqnorm_noalloc(0x10000, 4, 0x20004, None) == 1
+    assert b"8-byte" in lib.yg_last_error()
+    assert lib.yg_field_sqnorm_noalloc(0x10000, 16_777_217, 0x20000, None) == 1

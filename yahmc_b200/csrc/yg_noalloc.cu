@@ -8,6 +8,10 @@
 // allocation at all: its per-block partial sums live in the file-scope array below, which
 // every GPU that loads this library holds until the process exits.
 #include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+
 #include "../../include/yahmc_gpu.h"
 
 namespace {
@@ -22,8 +26,11 @@ constexpr long kMaxWords = (long)kMaxBlocks * kWordsPerBlock;   // 16,777,216 co
 // nothing needs clearing between calls; calls that overlap on the GPU race on it.
 static __device__ __align__(256) double noalloc_partials[kMaxBlocks];
 
+// Device address of noalloc_partials, per device, looked up at the first call on that
+// device.  Atomic because several host threads may make their first call at once; they
+// all store the same address, so whichever store lands last is correct.
 constexpr int kMaxDevices = 64;
-double *g_scratch[kMaxDevices] = {};          // device address of noalloc_partials, per device
+std::atomic<double *> g_scratch[kMaxDevices] = {};
 
 __device__ __forceinline__ double block_sum(double v) {
   __shared__ double sh[kThreads / 32];
@@ -76,28 +83,37 @@ static int fail(int code, const char *msg) {
 
 // Sum of |a_i|^2 over n complex FP64 words at dev_words (a view of a field: the even
 // half of a spinor field is its first 4*d*V/2 words), written to the device double
-// *dev_out on `stream`.  Allocates nothing.  The first call on a device looks up the
-// device address of the scratch array with that device current; make that first call
-// before any stream capture.
+// *dev_out on `stream`.  Allocates nothing.  dev_words must be 16-byte aligned and dev_out
+// 8-byte aligned (YG_ERR_ARG otherwise, checked before any launch).  The first call on a
+// device looks up the device address of the scratch array with that device current and
+// caches it for the process; make that first call before any stream capture.
 extern "C" int yg_field_sqnorm_noalloc(const double *dev_words, long n_words, double *dev_out, void *stream) {
   if (!dev_words || !dev_out) return fail(YG_ERR_ARG, "yg_field_sqnorm_noalloc: null pointer");
   if (n_words < 1) return fail(YG_ERR_ARG, "yg_field_sqnorm_noalloc: n_words must be >= 1");
   if (n_words > kMaxWords)
     return fail(YG_ERR_ARG, "yg_field_sqnorm_noalloc: n_words exceeds the 16,777,216-word scratch limit");
+  // The kernel reads the words as 16-byte double2 and writes one double: a view that starts
+  // an odd number of doubles into a buffer is rejected here, before anything is launched.
+  if (reinterpret_cast<std::uintptr_t>(dev_words) % 16 != 0)
+    return fail(YG_ERR_ARG, "yg_field_sqnorm_noalloc: dev_words must be 16-byte aligned");
+  if (reinterpret_cast<std::uintptr_t>(dev_out) % 8 != 0)
+    return fail(YG_ERR_ARG, "yg_field_sqnorm_noalloc: dev_out must be 8-byte aligned");
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return fail(YG_ERR_CUDA, "yg_field_sqnorm_noalloc: no usable current device");
-  if (!g_scratch[dev]) {
+  double *scratch = g_scratch[dev].load(std::memory_order_acquire);
+  if (!scratch) {
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, noalloc_partials) != cudaSuccess || !p)
       return fail(YG_ERR_CUDA, "yg_field_sqnorm_noalloc: cudaGetSymbolAddress failed");
-    g_scratch[dev] = static_cast<double *>(p);
+    scratch = static_cast<double *>(p);
+    g_scratch[dev].store(scratch, std::memory_order_release);
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int blocks = (int)((n_words + kWordsPerBlock - 1) / kWordsPerBlock);
-  k_partials<<<blocks, kThreads, 0, s>>>(g_scratch[dev], reinterpret_cast<const double2 *>(dev_words), n_words);
+  k_partials<<<blocks, kThreads, 0, s>>>(scratch, reinterpret_cast<const double2 *>(dev_words), n_words);
   if (cudaGetLastError() != cudaSuccess) return fail(YG_ERR_CUDA, "yg_field_sqnorm_noalloc: launch failed");
-  k_final<<<1, kThreads, 0, s>>>(dev_out, g_scratch[dev], blocks);
+  k_final<<<1, kThreads, 0, s>>>(dev_out, scratch, blocks);
   if (cudaGetLastError() != cudaSuccess) return fail(YG_ERR_CUDA, "yg_field_sqnorm_noalloc: launch failed");
   return YG_OK;
 }
