@@ -13,10 +13,10 @@ metric end to end through the public API with the source uploaded from pinned ho
 memory and the solution downloaded every step, and the reference's own CPU code
 (oracle/_ref, built from the reference sources) timed on this host's cores.
 
-Synthetic inputs: a thermalised beta = 5.6 field made on the GPU before timing: pure-gauge
-HMC (Wilson action, o2mn integrator, 150 trajectories from a cold start) on 16^3x32, tiled
-2x2x2x1 to 32^4 (a periodic field with the same local action density); the source is a
-complex Gaussian, unit variance per component.  Every input (links 604 MB, clover 604 MB,
+Synthetic inputs: a thermalised beta = 5.6 field made on the host without the engine, so
+that both arms read the same field: a Wilson-action heatbath (100 sweeps from a cold start)
+on 8^4, tiled to 32^4 (a periodic field with the same local action density); the source is
+a complex Gaussian, unit variance per component.  Every input (links 604 MB, clover 604 MB,
 fields 201 MB each) is larger than the 126 MB L2, so no flush is needed between steps.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -43,6 +43,7 @@ if ROOT not in sys.path:
 
 MASS, CSW, PREC = -0.75, 1.0, 1e-24
 CPU_SAMPLE_PREC = 1e-8      # squared relative residual of the bounded CPU-baseline sample
+REF_SAMPLE_PREC = 1e-3      # squared relative residual of each step of the reference arm
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
@@ -65,8 +66,6 @@ def parse():
     ap.add_argument("--field-cache", default=None,
                     help="npz file holding the generated field: loaded when present, written otherwise "
                          "(lets a profiled run skip the field generation)")
-    ap.add_argument("--therm-trajectories", type=int, default=THERM["trajectories"],
-                    help="HMC trajectories of the field generation (fewer only to profile a few launches)")
     ap.add_argument("--nrhs", type=int, default=12, help="systems of the batched-CG measurement (<= 1: skip)")
     ap.add_argument("--batched-only", action="store_true",
                     help="time only the batched CG of --nrhs systems (for profiling; not the bench line)")
@@ -107,6 +106,21 @@ DTYPE = {"generic-f32": "f32 inner / f64 reliable updates and residual",
          "f32-l8": "f32 inner (8-real links) / f64 reliable updates and residual"}
 
 
+# DRAM bytes (read + write) of one launch of the inner operator's step 1 as ncu counted them
+# (dram__bytes_read.sum + dram__bytes_write.sum), with the output sites of that launch; the
+# bench line scales them to its own lattice by the number of output sites
+INNER_NCU = {"f16spinor-l12": (191.3e6 + 9.8e6, 262144,
+                               "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_shop<16,32,32,6,1,0> launch "
+                               "at 32x32x32x16 (262,144 output sites), scaled by output sites to this lattice")}
+
+
+def inner_traffic(inner, sites):
+    if inner not in INNER_NCU:
+        return None
+    nbytes, nsites, _ = INNER_NCU[inner]
+    return nbytes / nsites * sites
+
+
 def solve_mixed(lat, x, b, inner, delta):
     spec = INNER[inner]
     return lat.cg_mixed("Hphi_sq", MASS, PREC, x, b, inner_precision=spec[0], link_reals=spec[1], delta=delta,
@@ -124,12 +138,16 @@ def hbm_peak():
 THERM = {"beta": 5.6, "c0": 1.0, "trajectories": 150, "warmup_md": 10, "steps": 100, "length": 1.0,
          "integrator": "o2mn", "start": "cold"}
 
+# the benchmark field: Wilson-action heatbath at beta 5.6 on a small periodic lattice, tiled
+FIELD = {"beta": 5.6, "base": 8, "sweeps": 100, "overrelax": 2, "start": "cold"}
+
+METRIC = "CG time-to-solution (true rel. residual 1e-12)"
+
 
 def thermalised_links(dims, seed, trajectories=None):
-    """A thermalised SU(3) field for the workload: pure-gauge HMC (Wilson action, beta 5.6)
-    on the lattice with the spatial extents halved, from a cold start, then tiled 1x2x2x2
-    (for 32^4: a thermalised 16^3x32 field tiled 2x2x2x1, again a periodic field).
-    Generated on the GPU by the engine's molecular-dynamics kernels; returns (U, plaquette)."""
+    """A thermalised SU(3) field made on the GPU (used by --mesons): pure-gauge HMC (Wilson
+    action, beta 5.6) on the lattice with the spatial extents halved, from a cold start, then
+    tiled 1x2x2x2.  Returns (U, plaquette, acceptance)."""
     import yahmc_b200 as yg
     from yahmc_b200 import thermalize as th
     small = (dims[0],) + tuple(d // 2 if d % 4 == 0 else d for d in dims[1:])
@@ -145,28 +163,57 @@ def thermalised_links(dims, seed, trajectories=None):
     return U, plaq, acc
 
 
-def make_inputs(dims, seed, rank=0, trajectories=None, cache=None):
+def bench_field(dims, seed, cache=None):
+    """The benchmark's gauge field, made on the host without the engine so that the reference
+    arm and this arm use the same field: Cabibbo-Marinari heatbath (2 overrelaxation sweeps per
+    heatbath sweep) at beta 5.6 on a periodic 8^4 lattice from a cold start, 100 sweeps, then
+    tiled onto `dims` (again a periodic field with the same local action density).  The
+    result is cached in the temporary directory (and in `cache` when given), keyed by its
+    parameters, so the second arm on the same machine reads what the first one made.
+    Returns (U in even-odd site order, plaquette of the 8^4 field)."""
+    from yahmc_b200 import heatbath, thermalize
+    base = tuple(min(FIELD["base"], d) for d in dims)
+    key = f"{'x'.join(map(str, base))}_{'x'.join(map(str, dims))}_{FIELD['beta']}_{FIELD['sweeps']}_" \
+          f"{FIELD['overrelax']}_{seed}"
+    paths = [p for p in (cache, os.path.join(tempfile.gettempdir(), f"yahmc_bench_field_{key}.npz")) if p]
+    for p in paths:
+        if os.path.exists(p):
+            try:
+                z = np.load(p)
+                if str(z["key"]) == key:
+                    return z["U"], float(z["plaquette"])
+            except Exception:
+                pass
+    U8, hist = heatbath.thermalised_field(base, FIELD["beta"], FIELD["sweeps"], seed, n_or=FIELD["overrelax"])
+    U = thermalize.tile(U8, base, tuple(dims)) if base != tuple(dims) else U8
+    plaq = float(hist[-1])
+    for p in paths:
+        try:
+            tmp = p + f".{os.getpid()}.tmp.npz"
+            np.savez(tmp, U=U, plaquette=plaq, key=key)
+            os.replace(tmp, p)
+        except OSError:
+            pass
+    return U, plaq
+
+
+def make_inputs(dims, seed, rank=0, cache=None):
+    """(links, source, description): the shared field and this rank's Gaussian source."""
     from yahmc_b200 import fields
-    if cache and os.path.exists(cache):
-        z = np.load(cache)
-        U, plaq, acc = z["U"], float(z["plaquette"]), float(z["acceptance"])
-    else:
-        U, plaq, acc = thermalised_links(dims, seed, trajectories)
-        if cache:
-            np.savez(cache, U=U, plaquette=plaq, acceptance=acc)
+    U, plaq = bench_field(dims, seed, cache)
     T, X, Y, Z = dims
     V = T * X * Y * Z
     rng = np.random.default_rng(replicas.rank_seed(seed, rank))
     b = fields.gaussian_spinor(V, 3, rng)
-    return U, b, {"plaquette": plaq, "acceptance": acc,
-                  "trajectories": THERM["trajectories"] if trajectories is None else trajectories}
+    return U, b, {"plaquette": plaq}
 
 
-def links_desc(info):
-    return (f"thermalised: {info['trajectories']} pure-gauge HMC trajectories (Wilson action, beta "
-            f"{THERM['beta']}, {THERM['integrator']} {THERM['steps']} steps, length {THERM['length']}, first "
-            f"{THERM['warmup_md']} without accept/reject) from a cold start on the lattice with halved spatial "
-            f"extents, tiled 1x2x2x2; plaquette {info['plaquette']:.5f}, acceptance {info['acceptance']:.2f}")
+def links_desc(info, dims):
+    base = tuple(min(FIELD["base"], d) for d in dims)
+    return (f"thermalised on the host: Wilson-action heatbath (Cabibbo-Marinari, Kennedy-Pendleton, "
+            f"{FIELD['overrelax']} overrelaxation sweeps each) at beta {FIELD['beta']}, {FIELD['sweeps']} sweeps "
+            f"from a cold start on {'x'.join(map(str, base))}, tiled to {'x'.join(map(str, dims))}; "
+            f"plaquette {info['plaquette']:.6f}")
 
 
 def workload_name(dims):
@@ -215,29 +262,44 @@ class Clocks:
 
 
 # ------------------------------------------------------------------ reference (CPU) arm
-def reference_solve_ms(dims, U, b, steps, threads, prec=PREC):
-    """The reference's own cg_inverter (oracle/_ref, compiled from the reference sources) on
-    Hphi_sq with the same links and source to squared precision prec; returns (ms per
-    solve, iterations)."""
-    from oracle import ref as oref
-    from oracle import yahmc_oracle as yo
-    from yahmc_b200 import fields
-    R = oref.get("su3_fund_ap", tuple(dims), csw=CSW, cf=1.0, threads=threads)
-    R.lib.yref_set_threads(threads)
-    R.set_links(fields.complex_to_raw(U))
-    braw = yo.spinor_to_raw(b)
-    times, its = [], []
-    for _ in range(steps):
-        x = R.spinor()
-        bb = braw.copy()
+def engine_loaded():
+    """Whether this process has mapped the engine's shared library (the reference arm must not)."""
+    try:
+        with open("/proc/self/maps") as f:
+            return "libyahmc_b200.so" in f.read()
+    except OSError:
+        return None
+
+
+class ReferenceCG:
+    """The reference's own cg_inverter (cg.cpp:132-202, compiled unmodified into oracle/_ref) on
+    Hphi_sq with the benchmark's links and source, on this host's cores."""
+
+    def __init__(self, dims, U, b, threads):
+        from oracle import ref as oref
+        from oracle import yahmc_oracle as yo
+        from yahmc_b200 import fields
+        self.R = oref.get("su3_fund_ap", tuple(dims), csw=CSW, cf=1.0, threads=threads)
+        self.R.lib.yref_set_threads(threads)
+        self.R.set_links(fields.complex_to_raw(U))
+        self.braw = yo.spinor_to_raw(b)
+        self.threads = threads
+
+    def solve(self, prec):
+        """One solve from a zero guess to squared precision prec: (ms, iterations)."""
+        x = self.R.spinor()
+        bb = self.braw.copy()
         t0 = time.perf_counter()
-        it = R.call("cg", 2, MASS, prec, x, bb)
-        times.append((time.perf_counter() - t0) * 1e3)
-        its.append(it)
-    return float(np.median(times)), int(its[-1])
+        it = self.R.call("cg", 2, MASS, prec, x, bb)
+        return (time.perf_counter() - t0) * 1e3, int(it)
 
 
 def run_reference(a, rank, world):
+    """--impl reference: the reference's CPU CG on the same field and source.  One full solve to
+    prec 1e-24 gives the iteration count of the workload and its time; each warm-up and timed
+    step is then a bounded sample (the same solve stopped at squared residual 1e-3, about a tenth
+    of the iterations) whose time per iteration, times the full iteration count, is the step's
+    time-to-solution.  Runs on rank 0 only, with every host core; the engine is not loaded."""
     if rank != 0:
         return
     from oracle import ref as oref
@@ -245,23 +307,30 @@ def run_reference(a, rank, world):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (no reference sources on this host)"}))
         return
     threads = os.cpu_count() or 1
-    import yahmc_b200 as yg
-    yg.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    U, b, info = make_inputs(a.dims, a.seed, 0, a.therm_trajectories, a.field_cache)   # input preparation
-    # one full solve is the bounded sample: about a minute on 16 host cores at 32^4; the
-    # reference code has no warm-up effect worth a second minute
-    steps, warm = 1, 0
-    ms, it = reference_solve_ms(a.dims, U, b, steps, threads)
+    U, b, info = make_inputs(a.dims, a.seed, 0, a.field_cache)
+    ref = ReferenceCG(a.dims, U, b, threads)
+    full_ms, n_full = ref.solve(PREC)
+    times, sample_its = [], []
+    for i in range(a.warmup + a.steps):
+        ms, it = ref.solve(REF_SAMPLE_PREC)
+        if i >= a.warmup:
+            times.append(ms / max(it, 1) * n_full)
+            sample_its.append(it)
+    value = float(np.median(times))
     line = {
-        "impl": "reference", "metric": "CG time-to-solution (true rel. residual 1e-12)", "value": ms, "unit": "ms",
-        "n_gpus": a.gpus, "steps": steps, "warmup": warm, "ms_per_step": ms, "higher_is_better": False,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "ms",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": value, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(a.dims), "iterations": it, "threads": threads,
-                   "links": links_desc(info)},
-        "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
-                         "sample": f"{steps} full reference cg_inverter solve (prec 1e-24, {it} iterations) on "
-                                   f"{threads} OpenMP threads"},
-        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": {"workload": workload_name(a.dims), "mass": MASS, "csw": CSW, "prec_squared": PREC,
+                   "links": links_desc(info, a.dims), "parallelism": "host cores"},
+        "iterations": n_full, "full_solve_ms": full_ms, "threads": threads,
+        "cpu_baseline": {"value": value, "unit": "ms", "cores": threads, "kind": "reference",
+                         "sample": f"per step: the reference's cg_inverter stopped at squared residual "
+                                   f"{REF_SAMPLE_PREC:g} ({sample_its[-1] if sample_its else 0} iterations) on "
+                                   f"{threads} OpenMP threads, time per iteration x the {n_full} iterations of the "
+                                   f"full solve to 1e-24 (that full solve, run once first: {full_ms / 1e3:.1f} s)"},
+        "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "engine_loaded": engine_loaded(),
     }
     print(json.dumps(line))
 
@@ -440,7 +509,7 @@ def run_ours(a, rank, world, dist):
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
     dev = torch.cuda.current_device()
     yg.set_device(dev)
-    U, b, info = make_inputs(a.dims, a.seed, rank, a.therm_trajectories, a.field_cache)
+    U, b, info = make_inputs(a.dims, a.seed, rank, a.field_cache)
     lat = yg.Lattice(a.dims, nc=3, repr="fundamental", bc="antiperiodic", clover=True, eo=True, csw=CSW)
     lat.set_links(U)
     V, d = lat.V, lat.d
@@ -603,7 +672,7 @@ def run_ours(a, rank, world, dist):
             from oracle import ref as oref
             if oref.available("su3_fund_ap"):
                 threads = os.cpu_count() or 1
-                cms, cit = reference_solve_ms(a.dims, U, b, 1, threads, prec=CPU_SAMPLE_PREC)
+                cms, cit = ReferenceCG(a.dims, U, b, threads).solve(CPU_SAMPLE_PREC)
                 cpu = {"value": cms / cit * it_fp64, "unit": "ms", "cores": threads, "kind": "reference",
                        "sample": f"reference cg_inverter on the same system stopped at prec {CPU_SAMPLE_PREC:g} "
                                  f"({cit} iterations, {cms / 1e3:.1f} s on {threads} OpenMP threads), scaled to the "
@@ -619,12 +688,12 @@ def run_ours(a, rank, world, dist):
         return
     value = replicas.job_time_per_solve(ms_mixed, world)
     line = {
-        "metric": "CG time-to-solution (true rel. residual 1e-12), mixed precision",
+        "metric": METRIC,
         "value": value, "unit": "ms", "n_gpus": world, "steps": a.steps, "warmup": max(3, a.warmup),
         "ms_per_step": ms_mixed, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": DTYPE[a.inner], "data": "synthetic",
+        "dtype": "mixed precision: " + DTYPE[a.inner], "data": "synthetic",
         "config": {"workload": workload_name(a.dims), "mass": MASS, "csw": CSW, "prec_squared": PREC,
-                   "links": links_desc(info),
+                   "links": links_desc(info, a.dims),
                    "l2": "inputs larger than L2 (links 604 MB, clover 604 MB), no flush",
                    "parallelism": f"replicas x{world}"},
         "solver": {"inner": a.inner, "delta": a.delta, "iterations": st["iterations"],
@@ -635,7 +704,9 @@ def run_ours(a, rank, world, dist):
                      "kernel": "k_shop<16,32,32,6,1,0> (inner operator step 1: FP16 spinors + norms, FP32 12-real "
                                "links, FP32 packed clover; 2 of the 6 launches of an inner iteration)",
                      "achieved": inner_gbs, "peak": peak, "unit": "GB/s", "frac": inner_gbs / peak,
-                     "peak_kind": peak_kind, "traffic": None, "ms_per_launch": ms_inner,
+                     "peak_kind": peak_kind, "traffic": inner_traffic(a.inner, V // 2),
+                     "traffic_source": INNER_NCU.get(a.inner, (0, 0, "no ncu capture of this inner format"))[2],
+                     "ms_per_launch": ms_inner,
                      "bytes_per_launch": inner_bytes,
                      "bytes_per_site": inner_bytes / (V // 2)},
         "e2e": {"value": replicas.job_time_per_solve(ms_e2e, world), "unit": "ms", "h2d_bytes_per_step": field_bytes,

@@ -32,6 +32,8 @@
 #ifndef YAHMC_GPU_H
 #define YAHMC_GPU_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -109,6 +111,11 @@ int yg_lattice_query(const yg_lattice *lat, yg_info *out);
 int yg_set_stream(yg_lattice *lat, void *cuda_stream);
 int yg_synchronize(yg_lattice *lat);
 const char *yg_last_error(void);
+/* No reference counterpart: page-lock (and release) a host array that is copied to and from
+ * the device often, e.g. the host application's gfield_fund and afield_momenta, so that those
+ * copies run at full PCIe speed.  bytes > 0. */
+int yg_host_register(void *host, size_t bytes);
+int yg_host_unregister(void *host);
 /* No reference counterpart: number of kernels this library has launched since it was
  * loaded (all lattices); benchmarks difference it around a timed region. */
 long yg_launch_count(void);
@@ -124,6 +131,11 @@ int yg_field_download(yg_lattice *lat, double *host_spinors, const double *dev_f
  * (repr.cpp:107-263), rebuild the clover term (clover.cpp:330-347) and apply the
  * antiperiodic sign (bcs.cpp:264-272).  host: 4*V suNg records, index 4*id+mu. */
 int yg_gauge_upload(yg_lattice *lat, const double *host_fund_links);
+/* gfield_fund upload alone, without represent_gauge_field: the state the reference is in
+ * after update_links (update.cpp:228-247) changed the links on the host and before the
+ * next represent_gauge_field; the gauge forces read these links, the fermion operators
+ * keep the represented field and clover term of the last yg_gauge_upload. */
+int yg_gauge_upload_fund(yg_lattice *lat, const double *host_fund_links);
 int yg_gauge_download(yg_lattice *lat, double *host_fund_links);
 /* gfield_repr (4*V suNf records), cl_term (4*V suNf), cl_ldl for sigma=4+mass (V ldl_t) */
 int yg_repr_links_download(yg_lattice *lat, double *host);

@@ -4,10 +4,11 @@
  * with standard deviation sigma, drawn by the Marsaglia polar method (not
  * GSL's ziggurat, so the stream differs from a GSL build; see gsl_rng.h).
  *
- * Test infrastructure only: linked into oracle/_ref, never into the product.
+ * Both builds use this same generator, so a CPU run and a GPU run from the same seed
+ * draw the same momenta and pseudo-fermions.
  */
-#ifndef YAHMC_ORACLE_GSL_RANDIST_H
-#define YAHMC_ORACLE_GSL_RANDIST_H
+#ifndef YAHMC_GSL_COMPAT_RANDIST_H
+#define YAHMC_GSL_COMPAT_RANDIST_H
 
 #include <math.h>
 #include "gsl_rng.h"

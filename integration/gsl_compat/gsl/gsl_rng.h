@@ -1,17 +1,19 @@
 /*
  * Project-written stand-in for the two GSL headers the reference includes
- * (include/random.h:4-5).  GSL is not installed on this machine, and only the
- * oracle build of the reference needs it.  The reference uses GSL for its
+ * (include/random.h:4-5).  GSL is not installed on this machine; the builds of the
+ * reference here (the oracle's CPU build and the host application built on the engine's
+ * shim) compile against this header instead.  A YaHMC installation links the real GSL.  The reference uses GSL for its
  * random-number stream alone (library/random.cpp:20-47, include/random.h:13-16);
  * no test pins that stream, so this header supplies the same API on top of a
  * different generator (xoshiro256** seeded through splitmix64).  Random fields
  * drawn through it are therefore NOT the ones a GSL build would draw; every
  * parity test injects its fields explicitly instead.
  *
- * Test infrastructure only: linked into oracle/_ref, never into the product.
+ * Both builds use this same generator, so a CPU run and a GPU run from the same seed
+ * draw the same momenta and pseudo-fermions.
  */
-#ifndef YAHMC_ORACLE_GSL_RNG_H
-#define YAHMC_ORACLE_GSL_RNG_H
+#ifndef YAHMC_GSL_COMPAT_RNG_H
+#define YAHMC_GSL_COMPAT_RNG_H
 
 #include <stdint.h>
 #include <stdlib.h>
@@ -26,10 +28,10 @@ typedef struct {
 	uint64_t s[4];
 } gsl_rng;
 
-static const gsl_rng_type yahmc_oracle_xoshiro_type = {"xoshiro256**"};
-static const gsl_rng_type *const gsl_rng_ranlxd1 = &yahmc_oracle_xoshiro_type;
+static const gsl_rng_type yahmc_gsl_xoshiro_type = {"xoshiro256**"};
+static const gsl_rng_type *const gsl_rng_ranlxd1 = &yahmc_gsl_xoshiro_type;
 
-static inline uint64_t yahmc_oracle_splitmix64(uint64_t *x)
+static inline uint64_t yahmc_gsl_splitmix64(uint64_t *x)
 {
 	uint64_t z = (*x += 0x9E3779B97F4A7C15ULL);
 	z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
@@ -37,22 +39,22 @@ static inline uint64_t yahmc_oracle_splitmix64(uint64_t *x)
 	return z ^ (z >> 31);
 }
 
-static inline uint64_t yahmc_oracle_rotl(uint64_t x, int k)
+static inline uint64_t yahmc_gsl_rotl(uint64_t x, int k)
 {
 	return (x << k) | (x >> (64 - k));
 }
 
-static inline uint64_t yahmc_oracle_next(gsl_rng *r)
+static inline uint64_t yahmc_gsl_next(gsl_rng *r)
 {
 	uint64_t *s = r->s;
-	uint64_t result = yahmc_oracle_rotl(s[1] * 5, 7) * 9;
+	uint64_t result = yahmc_gsl_rotl(s[1] * 5, 7) * 9;
 	uint64_t t = s[1] << 17;
 	s[2] ^= s[0];
 	s[3] ^= s[1];
 	s[1] ^= s[2];
 	s[0] ^= s[3];
 	s[2] ^= t;
-	s[3] = yahmc_oracle_rotl(s[3], 45);
+	s[3] = yahmc_gsl_rotl(s[3], 45);
 	return result;
 }
 
@@ -61,7 +63,7 @@ static inline void gsl_rng_env_setup(void) {}
 static inline void gsl_rng_set(gsl_rng *r, unsigned long seed)
 {
 	uint64_t x = (uint64_t)seed;
-	for(int i = 0; i < 4; i++) r->s[i] = yahmc_oracle_splitmix64(&x);
+	for(int i = 0; i < 4; i++) r->s[i] = yahmc_gsl_splitmix64(&x);
 }
 
 static inline gsl_rng *gsl_rng_alloc(const gsl_rng_type *t)
@@ -82,7 +84,7 @@ static inline double gsl_rng_uniform_pos(gsl_rng *r)
 {
 	double u;
 	do {
-		u = (double)(yahmc_oracle_next(r) >> 11) * (1.0 / 9007199254740992.0);
+		u = (double)(yahmc_gsl_next(r) >> 11) * (1.0 / 9007199254740992.0);
 	} while(u == 0.0);
 	return u;
 }

@@ -9,7 +9,7 @@ compile-time switches of the reference's programs/Makefile:1-45 (NC, REPR_*,
 CLOVER_TERM, UPDATE_EO, BC_*; no MPI), then linked with oracle/ref_harness.cpp
 into ``oracle/_ref/libyahmc_ref_<name>.so``.  GSL (the reference's only
 external library, used for random numbers alone) is absent here, so the
-project-written headers in oracle/gsl_compat stand in for it.
+project-written headers in integration/gsl_compat stand in for it.
 
 Only outputs land in oracle/_ref/ (git-ignored, but carried to GPU boxes with
 the rest of the tree).  Nothing here is part of the product.
@@ -54,7 +54,7 @@ def lib_path(name: str) -> Path:
 def _flags(name: str, src: Path) -> list[str]:
     nc, repr_, bc, clover, eo = CONFIGS[name]
     f = ["-O3", "-fPIC", "-fopenmp", "-std=c++11", "-w",
-         f"-I{HERE / 'gsl_compat'}", f"-I{src / 'include'}",
+         f"-I{HERE.parent / 'integration' / 'gsl_compat'}", f"-I{src / 'include'}",
          f"-DNC={nc}", f"-DREPR_{repr_}", f"-DBC_{bc}"]
     if clover:
         f.append("-DCLOVER_TERM")
@@ -118,13 +118,71 @@ def build(names=None, src: Path = DEFAULT_SRC, jobs: int = 0, force: bool = Fals
     return built
 
 
+def build_program(name: str = "su3_fund_ap", src: Path = DEFAULT_SRC, program: str = "hmc") -> Path:
+    """The reference's own programs/<program>.cpp linked with the CPU build of its sources:
+    ``oracle/_ref/<program>_<name>`` (what programs/Makefile builds, with the GSL stand-in)."""
+    build([name], src)
+    flags = _flags(name, src)
+    objdir = OUT / f"obj_{name}"
+    main = src / "programs" / f"{program}.cpp"
+    extra = [src / "observables" / n for n in ("polyakov.cpp", "sf_mpcac.cpp", "md_forces.cpp")]
+    jobs = [(cpp, objdir / (str(cpp.relative_to(src)).replace("/", "__") + ".o"), flags) for cpp in [main, *extra]]
+    errs = [e for e in map(_compile, jobs) if e]
+    if errs:
+        raise RuntimeError("reference build failed:\n" + "\n".join(errs))
+    objs = [objdir / (str(c.relative_to(src)).replace("/", "__") + ".o") for c in _sources(src)] + [o for _, o, _ in jobs]
+    exe = OUT / f"{program}_{name}"
+    if not exe.exists() or exe.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+        r = subprocess.run(["g++", "-o", str(exe), *map(str, objs), "-fopenmp", "-lm"], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link of {exe} failed:\n{r.stderr[-3000:]}")
+    return exe
+
+
+def shim_lib_path(name: str) -> Path:
+    return OUT / f"libyahmc_shim_{name}.so"
+
+
+def build_shim(names=("su3_fund_ap",), src: Path = DEFAULT_SRC) -> list[Path]:
+    """The same harness over YaHMC built on the engine (integration/build.py: YaHMC's sources
+    minus the files integration/yahmc_gpu_shim.cpp replaces, plus the shim), linked against
+    libyahmc_b200.so: ``oracle/_ref/libyahmc_shim_<name>.so``.  The parity tests drive it
+    exactly like the CPU build."""
+    sys.path.insert(0, str(HERE.parent))
+    from integration import build as ib
+    built = []
+    for name in names:
+        objs = ib.objects(name, src, extra=(HERE / "ref_harness.cpp",))
+        lib = shim_lib_path(name)
+        engine = ib.ENGINE_DIR / "libyahmc_b200.so"
+        newest = max(o.stat().st_mtime for o in objs + [engine])
+        if not lib.exists() or lib.stat().st_mtime < newest:
+            OUT.mkdir(parents=True, exist_ok=True)
+            r = subprocess.run(["g++", "-shared", "-o", str(lib), *map(str, objs), *ib.link_flags()],
+                               capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"link of {lib} failed:\n{r.stderr[-3000:]}")
+        built.append(lib)
+    return built
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("names", nargs="*")
     ap.add_argument("--src", type=Path, default=DEFAULT_SRC)
     ap.add_argument("--jobs", type=int, default=0)
     ap.add_argument("--force", action="store_true")
+    ap.add_argument("--shim", action="store_true", help="build the harness over YaHMC on the engine instead")
+    ap.add_argument("--program", action="store_true", help="build the reference's own hmc program (CPU)")
     a = ap.parse_args(argv)
+    if a.program:
+        for n in a.names or ("su3_fund_ap",):
+            print(build_program(n, a.src))
+        return
+    if a.shim:
+        for p in build_shim(a.names or ("su3_fund_ap",), a.src):
+            print(p)
+        return
     for p in build(a.names or None, a.src, a.jobs, a.force):
         print(p)
 

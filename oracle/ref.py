@@ -58,10 +58,14 @@ def _ptr(a: np.ndarray):
 class RefLattice:
     """One initialised instance of the reference for (config, dims)."""
 
-    def __init__(self, name: str, dims, csw=1.0, cf=1.0, threads=0, seed=1234, log_level=-1):
-        src = REF_DIR / f"libyahmc_ref_{name}.so"
+    def __init__(self, name: str, dims, csw=1.0, cf=1.0, threads=0, seed=1234, log_level=-1, kind="ref"):
+        """kind "ref": the reference compiled for the CPU; kind "shim": the same sources with
+        the eight files integration/yahmc_gpu_shim.cpp replaces taken out, running on the
+        engine (needs a GPU)."""
+        src = REF_DIR / f"libyahmc_{kind}_{name}.so"
         if not src.exists():
-            raise FileNotFoundError(f"{src} missing: run oracle/build_ref.py")
+            raise FileNotFoundError(f"{src} missing: run oracle/build_ref.py" + (" --shim" if kind == "shim" else ""))
+        self.kind = kind
         tmpdir = Path(tempfile.mkdtemp(prefix="yref_"))
         dst = tmpdir / f"libyahmc_ref_{name}_{'x'.join(map(str, dims))}.so"
         shutil.copy(src, dst)
@@ -86,7 +90,7 @@ class RefLattice:
         self.csw = csw
         self.cf = cf
         for fn in ("yref_spinor_sqnorm", "yref_spinor_product_re", "yref_clover_logdet",
-                   "yref_timestamp", "yref_avr_wilson", "yref_hamiltonian"):
+                   "yref_timestamp", "yref_avr_wilson", "yref_hamiltonian", "yref_hmc_hamiltonian"):
             getattr(lib, fn).restype = _D
         for fn, args in {
             "yref_Dphi_ee": [_D, _P, _P], "yref_Dphi_oo": [_D, _P, _P], "yref_Dphi_oo_inv": [_D, _P, _P],
@@ -117,6 +121,10 @@ class RefLattice:
             "yref_gauge_save_hirep": [ctypes.c_char_p], "yref_gauge_load_hirep": [ctypes.c_char_p],
             "yref_mre_init": [_I, _I, _D], "yref_mre_store": [_P], "yref_mre_guess": [_P, _P], "yref_mre_reset": [],
             "yref_represent": [_P, _P, _I],
+            "yref_hmc_init": [ctypes.c_char_p], "yref_hmc_reset": [], "yref_hmc_hamiltonian": [],
+            "yref_hmc_integrate": [_D, _I, _P, _P], "yref_hmc_update": [_D], "yref_hmc_counters": [_P],
+            "yref_gauge_backup": [], "yref_gauge_restore": [], "yref_set_momenta": [_P],
+            "yref_check_group": [], "yref_check_dirac": [], "yref_check_inverters": [],
         }.items():
             getattr(lib, fn).argtypes = args
 
@@ -181,6 +189,27 @@ class RefLattice:
     def zero_momenta(self):
         self.lib.yref_zero_momenta()
 
+    def set_momenta(self, raw: np.ndarray):
+        self.lib.yref_set_momenta(_ptr(np.ascontiguousarray(raw, dtype=np.float64)))
+
+    # ---- HMC through the reference's own update.cpp / integrator.cpp / monomials
+    def hmc_init(self, cfg_text: str):
+        rc = self.lib.yref_hmc_init(cfg_text.encode())
+        if rc != 0:
+            raise RuntimeError(f"yref_hmc_init: {rc}")
+
+    def hmc_integrate(self, length, levels):
+        """levels: [(type, steps)] from the outermost level inward; type o2lf/o2mn/o4mn."""
+        code = {"o2lf": 0, "o2mn": 1, "o4mn": 2}
+        types = np.array([code[t] for t, _ in levels], dtype=np.int32)
+        steps = np.array([n for _, n in levels], dtype=np.int32)
+        self.lib.yref_hmc_integrate(length, len(levels), types.ctypes.data_as(_P), steps.ctypes.data_as(_P))
+
+    def hmc_counters(self):
+        out = np.zeros(2, dtype=np.int32)
+        self.lib.yref_hmc_counters(out.ctypes.data_as(_P))
+        return int(out[0]), int(out[1])
+
     # ---- operators / linalg / inverters
     def call(self, fn: str, *args):
         conv = [(_ptr(a) if isinstance(a, np.ndarray) else a) for a in args]
@@ -217,6 +246,10 @@ def mesons(R: "RefLattice", mass, prec, hits, method):
     with open(R._meson_log) as f:
         f.seek(off)
         return _parse_mesons(f.read())
+
+
+def shim_available(name: str = "su3_fund_ap") -> bool:
+    return (REF_DIR / f"libyahmc_shim_{name}.so").exists()
 
 
 def get(name: str, dims=(8, 8, 8, 8), **kw) -> RefLattice:

@@ -53,6 +53,8 @@
 /* defined in library/update.cpp without a header declaration */
 double hamiltonian();
 void reunitarize();
+void reset_variables();
+#include <integrator.h>
 
 static int harness_ready = 0;
 
@@ -468,5 +470,48 @@ int yref_check_dirac(void) { return check_dirac(); }
 int yref_check_inverters(void) { return check_inverters(); }
 
 double yref_timestamp(void) { return timestamp(); }
+
+/* ---- HMC with monomials (update.cpp:41-339, integrator.cpp, monomials/*.cpp) ----
+ * yref_hmc_init reads [integrator]/[monomial] sections (the cfg format of programs/hmc.cpp)
+ * and calls hmc_init(); the other calls replay the steps of update() one by one, so that a
+ * test can read H before and after the integration, integrate backwards, and count MVMs. */
+int yref_hmc_init(const char *cfg_text)
+{
+	char path[] = "/tmp/yahmc_oracle_hmcXXXXXX";
+	int fd = mkstemp(path);
+	if(fd < 0) return -2;
+	FILE *fp = fdopen(fd, "w");
+	fputs(cfg_text, fp);
+	fclose(fp);
+	var_init(path);
+	remove(path);
+	hmc_init();
+	return 0;
+}
+
+void yref_hmc_reset(void) { reset_variables(); }          /* momenta + pseudo-fermions */
+double yref_hmc_hamiltonian(void) { return hamiltonian(); }
+
+/* ipar->integrator(length, ipar) of update() (update.cpp:297-299), with the integrator chain
+ * given level by level from the outermost: type 0 o2lf, 1 o2mn, 2 o4mn */
+void yref_hmc_integrate(double length, int nlev, const int *types, const int *steps)
+{
+	int_par *chain = new int_par[nlev];
+	for(int i = 0; i < nlev; i++)
+	{
+		chain[i].level = nlev - 1 - i;
+		chain[i].steps = steps[i];
+		chain[i].integrator = types[i] == 0 ? &o2lf_multilevel : (types[i] == 1 ? &o2mn_multilevel : &o4mn_multilevel);
+		chain[i].next = (i + 1 < nlev) ? &chain[i + 1] : 0;
+	}
+	chain[0].integrator(length, &chain[0]);
+	delete[] chain;
+}
+
+/* one whole trajectory through update() (update.cpp:281-339), Metropolis step included */
+void yref_hmc_update(double length) { update(length); }
+void yref_hmc_counters(int *out) { out[0] = num_cnfg; out[1] = num_accept; }
+void yref_gauge_backup(void) { gauge_field_backup(); }
+void yref_gauge_restore(void) { gauge_field_restore(); }
 
 }

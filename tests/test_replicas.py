@@ -75,3 +75,4 @@ def test_helpers():
     assert replicas.max_over_ranks(3.25) == 3.25
     with pytest.raises(ValueError):
         replicas.job_time_per_solve(1.0, 0)
+

@@ -84,7 +84,8 @@ def test_noalloc_sqnorm_rejects_misaligned_pointers():
     assert rc == 1 and b"16-byte" in lib.yg_last_error()
     rc = lib.yg_field_sqnorm_noalloc(ctypes.c_void_p(buf.data_ptr()), 4, ctypes.c_void_p(out.data_ptr() + 4), None)
     assert rc == 1 and b"8-byte" in lib.yg_last_error()
-    got = _noalloc_sqnorm(lib, buf.data_ptr(), 4, out)          # the aligned call still works
+    one = torch.zeros(1, dtype=torch.float64, device="cuda")
+    got = _noalloc_sqnorm(lib, buf.data_ptr(), 4, one)          # the aligned call still works
     assert got == 0.0
 
 

@@ -78,6 +78,7 @@ _SIGNATURES = {
     "yg_lattice_create": [ctypes.POINTER(_Params), ctypes.POINTER(_P)], "yg_set_device": [_I],
     "yg_lattice_destroy": [_P], "yg_lattice_query": [_P, ctypes.POINTER(_Info)],
     "yg_set_stream": [_P, _P], "yg_synchronize": [_P],
+    "yg_gauge_upload_fund": [_P, _P], "yg_host_register": [_P, ctypes.c_size_t], "yg_host_unregister": [_P],
     "yg_field_alloc": [_P, ctypes.POINTER(_P)], "yg_field_free": [_P, _P],
     "yg_field_upload": [_P, _P, _P], "yg_field_download": [_P, _P, _P],
     "yg_gauge_upload": [_P, _P], "yg_gauge_download": [_P, _P], "yg_repr_links_download": [_P, _P],

@@ -130,6 +130,17 @@ int yg_field_download(yg_lattice *l, double *host, const double *dev) {
 }
 
 int yg_gauge_upload(yg_lattice *l, const double *h) { return guard([&] { need(h, "host"); yg::gauge_upload(lat(l), h); }); }
+int yg_gauge_upload_fund(yg_lattice *l, const double *h) {
+  return guard([&] { need(h, "host"); yg::gauge_upload_fund(lat(l), h); });
+}
+int yg_host_register(void *p, size_t bytes) {
+  return guard([&] {
+    need(p, "host");
+    if (bytes == 0) throw Error(YG_ERR_ARG, "yg_host_register: zero bytes");
+    YG_CUDA(cudaHostRegister(p, bytes, cudaHostRegisterDefault));
+  });
+}
+int yg_host_unregister(void *p) { return guard([&] { need(p, "host"); YG_CUDA(cudaHostUnregister(p)); }); }
 int yg_gauge_download(yg_lattice *l, double *h) { return guard([&] { need(h, "host"); yg::gauge_download(lat(l), h); }); }
 int yg_repr_links_download(yg_lattice *l, double *h) { return guard([&] { need(h, "host"); yg::repr_download(lat(l), h); }); }
 int yg_clover_term_download(yg_lattice *l, double *h) { return guard([&] { need(h, "host"); yg::clover_download(lat(l), h); }); }

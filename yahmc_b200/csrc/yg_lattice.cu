@@ -43,13 +43,15 @@ Lattice::~Lattice() {
   for (double *s : scratch) if (s) cudaFree(s);
   if (host_result) cudaFreeHost(host_result);
   if (sl_hist) cudaFreeHost(sl_hist);
+  if (mr_hist) cudaFreeHost(mr_hist);
   for (cudaEvent_t e : sl_ev) if (e) cudaEventDestroy(e);
   if (stream) {
     cudaStreamSynchronize(stream);
     cudaStreamDestroy(stream);
   }
   for (DevBuf *b : {&fund, &links, &clover, &ldl, &cl_force, &mom, &tables, &red_partial, &red_result, &links_f,
-                    &clover_f, &cinv_f, &sl_links, &sl_clover, &cpk64, &sl_part, &sl_scal, &fund_backup, &sl_cnorm})
+                    &clover_f, &cinv_f, &sl_links, &sl_clover, &cpk64, &sl_part, &sl_scal, &fund_backup, &sl_cnorm,
+                    &mr_work, &mr_scal, &mr_part})
     b->release();
 }
 
@@ -388,6 +390,14 @@ static void download_records(Lattice &L, double *host, const void *src, int rec,
 void gauge_upload(Lattice &L, const double *host) {
   upload_records(L, L.fund, host, L.nc * L.nc, 4);
   represent_and_clover(L);
+  YG_CUDA(cudaStreamSynchronize(L.stream));
+}
+
+// the fundamental links alone: what the reference's update_links leaves behind on the host
+// (update.cpp:228-247) before represent_gauge_field runs; the represented field and the
+// clover term keep the state of the last gauge_upload / represent_and_clover
+void gauge_upload_fund(Lattice &L, const double *host) {
+  upload_records(L, L.fund, host, L.nc * L.nc, 4);
   YG_CUDA(cudaStreamSynchronize(L.stream));
 }
 

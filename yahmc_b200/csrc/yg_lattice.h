@@ -101,6 +101,13 @@ struct Lattice {
   double *sl_hist = nullptr;          // mapped pinned host ring of inner |r|^2 (written by the GPU)
   cudaEvent_t sl_ev[2] = {nullptr, nullptr};
 
+  // multi-right-hand-side mixed CG (yg_mrhs.cu): per-system working storage, device
+  // scalars, reduction partials and the mapped host ring of per-system |r|^2
+  DevBuf mr_work;
+  int mr_cap = 0;
+  DevBuf mr_scal, mr_part;
+  double *mr_hist = nullptr;
+
   long field_doubles() const { return 8L * d * V; }
   size_t field_bytes() const { return sizeof(double) * field_doubles(); }
 
@@ -116,6 +123,7 @@ void represent_and_clover(Lattice &L);
 void ensure_ldl(Lattice &L, double sigma);
 constexpr int kPackedInverseMaxD = 6;   // largest d whose FP64 Schur step uses the packed inverse
 void gauge_upload(Lattice &L, const double *host);
+void gauge_upload_fund(Lattice &L, const double *host);
 void gauge_download(Lattice &L, double *host);
 void repr_download(Lattice &L, double *host);
 void clover_download(Lattice &L, double *host);
@@ -240,6 +248,10 @@ int bicgstab_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *x
 // the same systems with FP32 inner iterations and FP64 reliable updates (yg_multi.cu)
 int cg_mixed_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, double *const *bs, double delta,
                    yg_solve_stats *stats);
+// the same with the compressed FP16/FP32 inner operator applied to a tile of systems per
+// thread, device-side scalars and one-iteration-late host reads (yg_mrhs.cu)
+int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, double *const *bs, double delta,
+                  yg_solve_stats *stats);
 // the compressed inner operator's matrices (yg_sloppy.cu); formats 32 / 16 / 15, 0 = as prec
 void ensure_sloppy(Lattice &L, double mass, int prec, int reals, int lfmt, int cfmt);
 void inner_hop_profile(Lattice &L, double mass, int reps, double *ms, double *bytes);
