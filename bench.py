@@ -80,6 +80,10 @@ def parse():
     ap.add_argument("--mshift", action="store_true",
                     help="time a 12-shift cg_mshift on SU(2) adjoint 48x24x24x24 against the 12 shifted "
                          "systems solved one at a time (not the bench line)")
+    ap.add_argument("--hmc", action="store_true",
+                    help="configuration 2: Nf=2 HMC + Hasenbusch trajectories on 16^3x32 through YaHMC's own hmc "
+                         "program built on the engine, FP64 and mixed-precision solvers (not the bench line)")
+    ap.add_argument("--hmc-trajectories", type=int, default=4)
     ap.add_argument("--contract-only", action="store_true",
                     help="with --mesons: only the contraction, on random propagators (for profiling)")
     return ap.parse_args()
@@ -456,6 +460,148 @@ def run_mshift(a):
                       "one_shift_iterations": it2, "speedup": t2 / t1}))
 
 
+HMC_CFG = """[lattice]
+dim_t = {T}
+dim_x = {X}
+dim_y = {Y}
+dim_z = {Z}
+[parallel]
+threads = 0
+np_t = 1
+np_x = 1
+np_y = 1
+np_z = 1
+[log]
+level = 30
+[rand]
+seed = {seed}
+[cnfg]
+dir = {dir}
+prefix = {prefix}
+start = {start}
+last = {last}
+freq = {freq}
+[clover]
+csw = 1.0
+cf = 1.0
+[traj]
+length = 1.0
+[observables]
+plaq_freq = 1
+poly_freq = 0
+mes_freq = 0
+"""
+
+GAUGE_ONLY = """[integrator]
+level = 0
+type = o2mn
+steps = 10
+[monomial]
+level = 0
+type = gauge
+beta = 5.6
+c0 = 1.0
+"""
+
+NF2 = """[integrator]
+level = 0
+type = o2mn
+steps = 1
+[integrator]
+level = 1
+type = o2mn
+steps = 10
+[monomial]
+level = 0
+type = gauge
+beta = 5.6
+c0 = 1.0
+[monomial]
+level = 1
+type = hmc
+mass = -0.75
+dm = 0.2
+prec = 1e-24
+mre_past = 5
+[monomial]
+level = 1
+type = hasenbusch
+mass = -0.75
+dm = 0.2
+prec = 1e-24
+"""
+
+
+def _hmc_log(path):
+    import re
+    text = open(path).read()
+    traj = [(float(t), int(m)) for t, m in re.findall(r"Trajectory finished in ([0-9.]+) seconds \(MVM = (\d+)\)", text)]
+    dh = [float(x) for x in re.findall(r"dH = ([-+0-9.e]+)", text)]
+    acc = re.findall(r"Configuration (accepted|rejected)", text)
+    plaq = [float(x) for x in re.findall(r"Plaquette: ([-+0-9.e]+)", text)]
+    return {"seconds": [t for t, _ in traj], "mvm": [m for _, m in traj], "dH": dh, "accepted": [x == "accepted" for x in acc],
+            "plaquette": plaq}
+
+
+def run_hmc(a):
+    """Configuration 2 through YaHMC's own hmc program (programs/hmc.cpp and every library file
+    but the eight the shim replaces, unchanged) built on the engine: SU(3) fundamental 16^3x32,
+    Wilson gauge action beta 5.6, clover csw 1, an HMC monomial (m = -0.75, dm = 0.2) and a
+    Hasenbusch monomial (m = -0.75, dm = 0.2) on level 1 with 10 o2mn steps, the gauge monomial
+    on level 0 with 1 step, trajectory length 1, prec 1e-24 (relative residual 1e-12).  The
+    start is 20 pure-gauge trajectories from the reference's random start (seed given).  Then
+    --hmc-trajectories trajectories with the reference's FP64 solvers and the same number with
+    the mixed-precision CG for the Hphi_sq solves (YAHMC_GPU_SOLVER=mixed); the program's own
+    log gives trajectory times, MVM counts, dH and acceptance.  The CPU build of the same
+    program (oracle/_ref) runs one trajectory from the same start for comparison."""
+    exe = os.path.join(ROOT, "integration", "_build", "hmc_su3_fund_ap")
+    cpu_exe = os.path.join(ROOT, "oracle", "_ref", "hmc_su3_fund_ap")
+    if not os.path.exists(exe):
+        print(json.dumps({"hmc": "unavailable", "why": "integration/_build/hmc_su3_fund_ap not built"}))
+        return
+    T, X, Y, Z = 32, 16, 16, 16
+    work = tempfile.mkdtemp(prefix="yahmc_hmc_")
+    dims = dict(T=T, X=X, Y=Y, Z=Z, dir=work)
+
+    def run(exe_path, cfg_text, name, env=None):
+        cfg = os.path.join(work, f"{name}.cfg")
+        with open(cfg, "w") as f:
+            f.write(cfg_text)
+        log = os.path.join(work, f"{name}.log")
+        t0 = time.perf_counter()
+        r = subprocess.run([exe_path, "-i", cfg, "-o", log], cwd=work, capture_output=True, text=True,
+                           env={**os.environ, **(env or {})})
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            raise RuntimeError(f"{name}: rc {r.returncode}: {r.stderr[-1000:]}")
+        out = _hmc_log(log)
+        out["wall_s"] = wall
+        return out
+
+    seed = a.seed % 100000
+    therm = run(exe, HMC_CFG.format(seed=seed, prefix="therm", start="random", last=20, freq=20, **dims) + GAUGE_ONLY,
+                "therm")
+    start = f"therm_{T}x{X}x{Y}x{Z}_nc3_n0020"
+    n = a.hmc_trajectories
+    res = {"workload": "Nf=2 HMC + Hasenbusch trajectory, 16^3x32 SU(3) fund clover even-odd, YaHMC's hmc program "
+                       "on the engine", "start": f"20 pure-gauge trajectories from the random start, plaquette "
+                       f"{therm['plaquette'][-1]:.6f}", "thermalisation_s": therm["wall_s"]}
+    for solver, env in (("fp64", None), ("mixed", {"YAHMC_GPU_SOLVER": "mixed"})):
+        r = run(exe, HMC_CFG.format(seed=seed + 1, prefix="nf2", start=start, last=n, freq=0, **dims) + NF2,
+                f"nf2_{solver}", env)
+        dh = np.array(r["dH"])
+        res[solver] = {"trajectory_s": r["seconds"], "mean_trajectory_s": float(np.mean(r["seconds"])),
+                       "mvm": r["mvm"], "dH": r["dH"], "exp_minus_dH_mean": float(np.mean(np.exp(-dh))),
+                       "acceptance": float(np.mean(r["accepted"])), "plaquette": r["plaquette"]}
+    if os.path.exists(cpu_exe) and not a.no_cpu_baseline:
+        r = run(cpu_exe, HMC_CFG.format(seed=seed + 1, prefix="cpu", start=start, last=1, freq=0, **dims) + NF2, "cpu")
+        res["cpu_reference"] = {"trajectory_s": r["seconds"], "mvm": r["mvm"], "dH": r["dH"],
+                                "threads": os.cpu_count(), "plaquette": r["plaquette"]}
+        res["speedup_fp64_vs_cpu"] = r["seconds"][0] / res["fp64"]["trajectory_s"][0]
+        res["dH_first_trajectory_gpu_minus_cpu"] = res["fp64"]["dH"][0] - r["dH"][0]
+    print(json.dumps(res))
+
+
 def run_lattices(a):
     """FP64 CG (Hphi_sq, m = -0.6, prec 1e-20) on SU(3) fundamental 8^4, 12^4 and 16^4 lattices
     with thermalised-like fields from the engine's own HMC (20 trajectories each): the three
@@ -741,6 +887,8 @@ def main():
             run_mesons(a)
         elif a.lattices:
             run_lattices(a)
+        elif a.hmc:
+            run_hmc(a)
         elif a.mshift:
             run_mshift(a)
         elif a.impl == "reference":

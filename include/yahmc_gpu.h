@@ -314,6 +314,43 @@ int yg_gauge_load_cfg(yg_lattice *lat, const char *path, int *num_cnfg, int *num
 int yg_gauge_save_hirep(yg_lattice *lat, const char *path);
 int yg_gauge_load_hirep(yg_lattice *lat, const char *path, int *num_cnfg, double *plaquette_diff);
 
+/* ---- learned preconditioner (no reference counterpart) ------------------
+ * A gauge-covariant parallel-transport convolution network: each layer maps Ci channels of
+ * spinor fields on the whole lattice to Co channels,
+ *     out[x, o] = sum_p sum_i W[p, o, i] (T_p in_i)(x),
+ * over nine paths p (0 the site, 1..4 a hop forward along mu = p-1 through U_mu(x), 5..8 a hop
+ * backward through U_mu(x-mu)^dag, the represented links the Dirac operator uses), W[p, o, i]
+ * a complex 4x4 spin matrix.  Colour meets only the links, so the network commutes with gauge
+ * transformations exactly.  Channels 1 -> C -> ... -> C -> 1 with C = 8 or 16, d = 3; layers
+ * are linear.  The per-site channel mixing runs as BF16 products with FP32 accumulation on the
+ * tensor cores (forward, adjoint and weight gradient).
+ * Weights: 9*Co*Ci*4*4 complex numbers as (re, im) doubles, index ((p*Co + o)*Ci + i)*16 + s*4 + s'.
+ * Activation planes (yg_ptc_layer): float, plane ((ch*12 + spin*3 + colour)*2 + re/im) of V
+ * values in the reference's site order. */
+typedef struct yg_ptc yg_ptc;
+int yg_ptc_create(yg_lattice *lat, int nlayers, const int *channels, yg_ptc **out);
+int yg_ptc_destroy(yg_ptc *net);
+int yg_ptc_set_weights(yg_ptc *net, int layer, const double *w);
+int yg_ptc_get_weights(yg_ptc *net, int layer, double *w);
+/* one layer on device activation planes; adjoint = 1: the input-gradient layer (Co -> Ci) */
+int yg_ptc_layer(yg_ptc *net, int layer, int adjoint, const float *dev_in, float *dev_out);
+/* dst (even sites) = the network applied to the even-site field src embedded with zero odd
+ * sites (the even-even block of D^-1 is the inverse of the Schur operator Dphi) */
+int yg_ptc_apply(yg_ptc *net, double *dst, const double *src);
+/* training: loss = sum_k |N(r_k) - e_k|^2 / |e_k|^2 over even-site pairs with Dphi e_k = r_k,
+ * and its gradient d loss / d conj(W), all layers' weights concatenated in the layout above */
+int yg_ptc_gradient(yg_ptc *net, int npairs, double *const *r, double *const *e, double *loss, double *grads);
+/* flexible GCR on Dphi with the network as right preconditioner (net may be NULL: plain GCR),
+ * restarted every `restart` directions; the true FP64 residual |b - Dphi x|^2 < prec |b|^2 ends
+ * the solve; no progress over four restart cycles hands over to the plain even-odd CG on the
+ * normal equations (stats->fallback = 1) */
+int yg_fgcr(yg_lattice *lat, yg_ptc *net, const yg_inv_par *par, int restart, double *x, double *b,
+            yg_solve_stats *stats);
+/* Hphi_sq x = b as two such Dphi solves (gamma5 D gamma5 D, as auto_inverter, inverter.cpp:27-34);
+ * the true Hphi_sq residual decides, and the FP64 CG finishes if it is not met (fallback bit 1) */
+int yg_solve_learned(yg_lattice *lat, yg_ptc *net, const yg_inv_par *par, int restart, double *x, double *b,
+                     yg_solve_stats *stats);
+
 /* ---- chronological initial guess (mre.h) -------------------------------- */
 /* The past solutions live on the device.  op is YG_OP_DPHI / HPHI / HPHI_SQ (mre_par.mvm),
  * max <= 15 (MRE_MAX); max = 0 disables the extrapolation (yg_mre_guess leaves dst alone). */

@@ -24,7 +24,7 @@ import numpy as np
 
 from .fields import complex_to_raw, raw_to_complex
 
-__all__ = ["Lattice", "Field", "YGError", "load_library", "LIB_PATH", "cg_inverter_lattices",
+__all__ = ["Lattice", "Field", "YGError", "load_library", "LIB_PATH", "cg_inverter_lattices", "Ptc",
            "VIEW_DEFAULT", "VIEW_EVEN", "VIEW_ODD", "VIEW_FULL", "OP_DPHI", "OP_HPHI", "OP_HPHI_SQ"]
 
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libyahmc_b200.so"
@@ -126,6 +126,11 @@ _SIGNATURES = {
     "yg_reunitarize": [_P], "yg_momenta_gaussian": [_P, ctypes.c_ulonglong], "yg_momenta_action": [_P, _P],
     "yg_gauge_backup": [_P], "yg_gauge_restore": [_P],
     "yg_field_sqnorm_noalloc": [_P, ctypes.c_long, _P, _P],
+    "yg_ptc_create": [_P, _I, _P, _P], "yg_ptc_destroy": [_P], "yg_ptc_set_weights": [_P, _I, _P],
+    "yg_ptc_get_weights": [_P, _I, _P], "yg_ptc_layer": [_P, _I, _I, _P, _P], "yg_ptc_apply": [_P, _P, _P],
+    "yg_ptc_gradient": [_P, _I, _P, _P, _P, _P],
+    "yg_fgcr": [_P, _P, ctypes.POINTER(InvPar), _I, _P, _P, ctypes.POINTER(SolveStats)],
+    "yg_solve_learned": [_P, _P, ctypes.POINTER(InvPar), _I, _P, _P, ctypes.POINTER(SolveStats)],
 }
 
 
@@ -168,6 +173,68 @@ class Mre:
     def __del__(self):
         if getattr(self, "h", None):
             self.lib.yg_mre_free(self.h)
+            self.h = None
+
+
+class Ptc:
+    """The learned preconditioner (yg_ptc_*): a linear gauge-covariant parallel-transport
+    network with channels 1 -> C -> ... -> 1 on a lattice.  Weights per layer are complex
+    arrays of shape (9, Co, Ci, 4, 4): path, output channel, input channel, spin, spin."""
+
+    def __init__(self, lat, channels):
+        self.lat, self.lib = lat, lat.lib
+        self.channels = tuple(int(c) for c in channels)
+        ch = (ctypes.c_int * len(self.channels))(*self.channels)
+        h = ctypes.c_void_p()
+        lat._check(self.lib.yg_ptc_create(lat.h, len(self.channels) - 1, ch, ctypes.byref(h)))
+        self.h = h
+
+    def shapes(self):
+        return [(9, co, ci, 4, 4) for ci, co in zip(self.channels[:-1], self.channels[1:])]
+
+    def set_weights(self, Ws):
+        for l, W in enumerate(Ws):
+            W = np.ascontiguousarray(np.asarray(W, dtype=complex).reshape(self.shapes()[l]))
+            raw = np.ascontiguousarray(W.view(np.float64))
+            self.lat._check(self.lib.yg_ptc_set_weights(self.h, l, _ptr(raw)))
+
+    def get_weights(self):
+        out = []
+        for l, shp in enumerate(self.shapes()):
+            raw = np.empty(int(np.prod(shp)) * 2)
+            self.lat._check(self.lib.yg_ptc_get_weights(self.h, l, _ptr(raw)))
+            out.append(raw.view(complex).reshape(shp).copy())
+        return out
+
+    def layer(self, l, adjoint, dev_in: int, dev_out: int):
+        """One layer on device activation planes (raw device pointers)."""
+        self.lat._check(self.lib.yg_ptc_layer(self.h, int(l), int(adjoint), ctypes.c_void_p(dev_in),
+                                              ctypes.c_void_p(dev_out)))
+
+    def apply(self, dst, src):
+        self.lat._check(self.lib.yg_ptc_apply(self.h, dst.ptr, src.ptr))
+
+    def gradient(self, pairs):
+        """(loss, per-layer complex gradients d loss / d conj(W)) over (r, e) field pairs."""
+        n = len(pairs)
+        pr = (ctypes.c_void_p * n)(*[r.ptr for r, _ in pairs])
+        pe = (ctypes.c_void_p * n)(*[e.ptr for _, e in pairs])
+        sizes = [int(np.prod(s)) for s in self.shapes()]
+        raw = np.zeros(2 * sum(sizes))
+        loss = ctypes.c_double()
+        self.lat._check(self.lib.yg_ptc_gradient(self.h, n, pr, pe, ctypes.byref(loss), _ptr(raw)))
+        grads, off = [], 0
+        for shp, sz in zip(self.shapes(), sizes):
+            grads.append(raw[2 * off:2 * (off + sz)].view(complex).reshape(shp).copy())
+            off += sz
+        return loss.value, grads
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            try:
+                self.lib.yg_ptc_destroy(self.h)
+            except Exception:
+                pass
             self.h = None
 
 
@@ -600,6 +667,28 @@ class Lattice:
             self._check(rc)
         return {"status": rc, "iterations": st.iterations, "reliable_updates": st.reliable_updates,
                 "fallback": st.fallback, "true_residual": st.true_residual, "seconds": st.seconds}
+
+    def fgcr(self, mass, prec, x, b, net=None, restart=16, log=0, maxiter=0):
+        """Flexible GCR on Dphi with the network `net` (a Ptc, or None) as right preconditioner."""
+        st = SolveStats()
+        par = self._par("Dphi", mass, prec, log, maxiter)
+        rc = self.lib.yg_fgcr(self.h, net.h if net is not None else None, ctypes.byref(par), int(restart), x.ptr,
+                              b.ptr, ctypes.byref(st))
+        if rc not in (0, 4, 5):
+            self._check(rc)
+        return {"status": rc, "iterations": st.iterations, "fallback": st.fallback,
+                "true_residual": st.true_residual, "seconds": st.seconds}
+
+    def solve_learned(self, mass, prec, x, b, net=None, restart=16, maxiter=0):
+        """Hphi_sq x = b as two preconditioned Dphi solves (yg_solve_learned)."""
+        st = SolveStats()
+        par = self._par("Hphi_sq", mass, prec, 0, maxiter)
+        rc = self.lib.yg_solve_learned(self.h, net.h if net is not None else None, ctypes.byref(par), int(restart),
+                                       x.ptr, b.ptr, ctypes.byref(st))
+        if rc not in (0, 4, 5):
+            self._check(rc)
+        return {"status": rc, "iterations": st.iterations, "fallback": st.fallback,
+                "true_residual": st.true_residual, "seconds": st.seconds}
 
     # ---- forces.h
     def momenta(self):

@@ -302,7 +302,7 @@ int yg_cg_mixed_multi(yg_lattice *l, const yg_inv_par *p, int nrhs, double *cons
   return guard_status([&] {
     check_par(p); need(xs, "xs"); need(bs, "bs"); need(stats, "stats");
     for (int i = 0; i < nrhs; i++) { need(xs[i], "xs[i]"); need(bs[i], "bs[i]"); }
-    return yg::cg_mixed_multi(lat(l), *p, nrhs, xs, bs, delta, stats);
+    return yg::cg_mixed_mrhs(lat(l), *p, nrhs, xs, bs, delta, stats);
   });
 }
 int yg_inner_hop_profile(yg_lattice *l, double mass, int reps, double *ms, double *bytes) {
@@ -400,6 +400,68 @@ int yg_gauge_load_hirep(yg_lattice *l, const char *path, int *num_cnfg, double *
 struct yg_mre {
   yg::Mre *m;
 };
+// ---- learned preconditioner (yg_ptc.cu)
+struct yg_ptc {
+  yg::Ptc *n;
+};
+static yg::Ptc &ptc(yg_ptc *h) {
+  if (!h || !h->n) throw Error(YG_ERR_ARG, "null network handle");
+  return *h->n;
+}
+int yg_ptc_create(yg_lattice *l, int nlayers, const int *channels, yg_ptc **out) {
+  return guard([&] {
+    need(out, "out");
+    need(channels, "channels");
+    *out = nullptr;
+    *out = new yg_ptc{yg::ptc_create(lat(l), nlayers, channels)};
+  });
+}
+int yg_ptc_destroy(yg_ptc *h) {
+  return guard([&] {
+    if (!h) return;
+    yg::ptc_destroy(h->n);
+    delete h;
+  });
+}
+int yg_ptc_set_weights(yg_ptc *h, int layer, const double *w) {
+  return guard([&] { need(w, "w"); yg::ptc_set_weights(ptc(h), layer, w); });
+}
+int yg_ptc_get_weights(yg_ptc *h, int layer, double *w) {
+  return guard([&] { need(w, "w"); yg::ptc_get_weights(ptc(h), layer, w); });
+}
+int yg_ptc_layer(yg_ptc *h, int layer, int adjoint, const float *in, float *out) {
+  return guard([&] {
+    need(in, "in");
+    need(out, "out");
+    yg::Ptc &n = ptc(h);
+    yg::ptc_layer(n, layer, adjoint, in, out);
+    YG_CUDA(cudaStreamSynchronize(yg::ptc_lattice(n).stream));
+  });
+}
+int yg_ptc_apply(yg_ptc *h, double *dst, const double *src) {
+  return guard([&] { need(dst, "dst"); need(src, "src"); yg::ptc_apply(ptc(h), dst, src); });
+}
+int yg_ptc_gradient(yg_ptc *h, int npairs, double *const *r, double *const *e, double *loss, double *grads) {
+  return guard([&] {
+    need(r, "r"); need(e, "e"); need(loss, "loss"); need(grads, "grads");
+    for (int k = 0; k < npairs; k++) { need(r[k], "r[k]"); need(e[k], "e[k]"); }
+    *loss = yg::ptc_gradient(ptc(h), npairs, r, e, grads);
+  });
+}
+int yg_fgcr(yg_lattice *l, yg_ptc *h, const yg_inv_par *p, int restart, double *x, double *b, yg_solve_stats *st) {
+  return guard_status([&] {
+    check_par(p); need(x, "x"); need(b, "b"); need(st, "stats");
+    return yg::fgcr(lat(l), h ? &ptc(h) : nullptr, *p, restart, x, b, st);
+  });
+}
+int yg_solve_learned(yg_lattice *l, yg_ptc *h, const yg_inv_par *p, int restart, double *x, double *b,
+                     yg_solve_stats *st) {
+  return guard_status([&] {
+    check_par(p); need(x, "x"); need(b, "b"); need(st, "stats");
+    return yg::solve_learned(lat(l), h ? &ptc(h) : nullptr, *p, restart, x, b, st);
+  });
+}
+
 int yg_mre_init(yg_lattice *l, int max, int op, double mass, yg_mre **out) {
   return guard([&] {
     need(out, "out");

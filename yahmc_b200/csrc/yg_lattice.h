@@ -107,6 +107,7 @@ struct Lattice {
   int mr_cap = 0;
   DevBuf mr_scal, mr_part;
   double *mr_hist = nullptr;
+  int mr_tile[17] = {};   // measured systems-per-thread tile of the inner operator, per system count
 
   long field_doubles() const { return 8L * d * V; }
   size_t field_bytes() const { return sizeof(double) * field_doubles(); }
@@ -257,6 +258,21 @@ void ensure_sloppy(Lattice &L, double mass, int prec, int reals, int lfmt, int c
 void inner_hop_profile(Lattice &L, double mass, int reps, double *ms, double *bytes);
 int tune_inner_links(Lattice &L, double mass, double *ms);
 int tuned_inner_links(Lattice &L, double mass);
+
+// learned preconditioner: gauge-covariant parallel-transport network (yg_ptc.cu)
+constexpr int kPtcMaxLayers = 8;
+struct Ptc;
+Ptc *ptc_create(Lattice &L, int nl, const int *ch);
+void ptc_destroy(Ptc *n);
+Lattice &ptc_lattice(Ptc &n);
+void ptc_set_weights(Ptc &n, int l, const double *w);
+void ptc_get_weights(Ptc &n, int l, double *w);
+void ptc_layer(Ptc &n, int l, int adjoint, const float *in, float *out);
+void ptc_apply(Ptc &n, double *dst, const double *src);
+double ptc_gradient(Ptc &n, int npairs, double *const *r, double *const *e, double *grads);
+int fgcr(Lattice &L, Ptc *net, const yg_inv_par &par, int restart, double *x, double *b, yg_solve_stats *st);
+int solve_learned(Lattice &L, Ptc *net, const yg_inv_par &par, int restart, double *x, double *b,
+                  yg_solve_stats *st);
 
 // chronological initial guess (yg_mre.cu)
 struct Mre;

@@ -330,7 +330,7 @@ int calc_propagator_multi(Lattice &L, double mass, double prec, int n, double *c
     par.op = YG_OP_HPHI_SQ;
     if (solver == 1) {
       std::vector<yg_solve_stats> ss(n);
-      st = cg_mixed_multi(L, par, n, y.data(), rhs.data(), 0.1, ss.data());
+      st = cg_mixed_mrhs(L, par, n, y.data(), rhs.data(), 0.1, ss.data());
       if (iters)
         for (int i = 0; i < n; i++) iters[i] = ss[i].iterations;
     } else {

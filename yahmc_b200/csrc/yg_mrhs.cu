@@ -35,7 +35,7 @@ namespace yg {
 namespace {
 
 constexpr int kMR = 16;       // systems per call (kMaxRhs of the batched solvers)
-constexpr int kTile = 4;      // systems per thread in the inner operator
+constexpr int kTiles[3] = {1, 2, 4};   // systems per thread in the inner operator (autotuned)
 constexpr int kHopThreads = 128;
 constexpr int kVecThreads = 256;
 
@@ -393,6 +393,29 @@ SysBufs sys_bufs(Lattice &L, int i) {
 
 int vec_grid(int sms) { return sms * 4; }
 
+// the two Schur steps of the inner operator for a launch's systems, R systems per thread
+template <int K, int R>
+void launch_mhop_r(Lattice &L, const MHopArgs &a, const MHopArgs &b, bool nrm, int nsb) {
+  const int grid = a.ntile * nsb;
+  k_mhop<K, R, 1, 0><<<grid, kHopThreads, 0, L.stream>>>(a);
+  YG_LAUNCHED();
+  if (nrm) k_mhop<K, R, 2, 1><<<grid, kHopThreads, 0, L.stream>>>(b);
+  else k_mhop<K, R, 2, 0><<<grid, kHopThreads, 0, L.stream>>>(b);
+  YG_LAUNCHED();
+}
+
+void launch_mhop(Lattice &L, int reals, int tile, const MHopArgs &a, const MHopArgs &b, bool nrm, int nsb) {
+  if (reals == 12) {
+    if (tile == 1) launch_mhop_r<6, 1>(L, a, b, nrm, nsb);
+    else if (tile == 2) launch_mhop_r<6, 2>(L, a, b, nrm, nsb);
+    else launch_mhop_r<6, 4>(L, a, b, nrm, nsb);
+  } else {
+    if (tile == 1) launch_mhop_r<9, 1>(L, a, b, nrm, nsb);
+    else if (tile == 2) launch_mhop_r<9, 2>(L, a, b, nrm, nsb);
+    else launch_mhop_r<9, 4>(L, a, b, nrm, nsb);
+  }
+}
+
 }  // namespace
 
 int cg(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
@@ -405,10 +428,12 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
   if (!L.p.eo) throw Error(YG_ERR_ARG, "the multi-system mixed CG needs even-odd preconditioning");
   if (L.d != 3) throw Error(YG_ERR_ARG, "the compressed inner operator exists for d = 3 representations");
   if (!(delta > 0.0 && delta < 1.0)) throw Error(YG_ERR_ARG, "reliable-update delta must lie in (0,1)");
-  for (int i = 0; i < nrhs; i++)
+  for (int i = 0; i < nrhs; i++) {
+    if (xs[i] == bs[i]) throw Error(YG_ERR_ARG, "a solution field must differ from its source");
     for (int k = 0; k < i; k++)
       if (xs[i] == xs[k] || xs[i] == bs[k] || bs[i] == xs[k])
         throw Error(YG_ERR_ARG, "solution fields must be distinct from each other and from the sources");
+  }
   const int nb = nrhs;
   const int reals = (L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL) ? 12 : 18;
   ensure_sloppy(L, par.mass, 16, reals, 32, 32);
@@ -489,13 +514,14 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
       v.sys[j] = act[j];
     }
   };
+  int tile = 4;
   auto hphi = [&](bool nrm, bool second) {   // t = Hphi p (first) or q = Hphi t (second), o the odd sites
     MHopArgs a{};
     a.g = L.g;
     a.U = L.sl_links.p;
     a.C = L.sl_clover.p;
     a.nsys = (int)act.size();
-    a.ntile = (a.nsys + kTile - 1) / kTile;
+    a.ntile = (a.nsys + tile - 1) / tile;
     a.nsb = nsb;
     a.part = part_pq;
     MHopArgs b = a;
@@ -510,19 +536,7 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
     }
     a.coeff = 0.5f; a.lo = Vh; a.n = Vh;
     b.coeff = -0.5f; b.lo = 0; b.n = Vh;
-    const int grid = a.ntile * nsb;
-    if (reals == 12) {
-      k_mhop<6, kTile, 1, 0><<<grid, kHopThreads, 0, L.stream>>>(a);
-      YG_LAUNCHED();
-      if (nrm) k_mhop<6, kTile, 2, 1><<<grid, kHopThreads, 0, L.stream>>>(b);
-      else k_mhop<6, kTile, 2, 0><<<grid, kHopThreads, 0, L.stream>>>(b);
-    } else {
-      k_mhop<9, kTile, 1, 0><<<grid, kHopThreads, 0, L.stream>>>(a);
-      YG_LAUNCHED();
-      if (nrm) k_mhop<9, kTile, 2, 1><<<grid, kHopThreads, 0, L.stream>>>(b);
-      else k_mhop<9, kTile, 2, 0><<<grid, kHopThreads, 0, L.stream>>>(b);
-    }
-    YG_LAUNCHED();
+    launch_mhop(L, reals, tile, a, b, nrm, nsb);
     L.mvm += 2 * a.nsys;
   };
   auto wait_iteration = [&](unsigned long long k) {
@@ -545,6 +559,36 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
     fill(v);
     k_m_p_from_r<<<dim3(gv, v.nsys), kVecThreads, 0, L.stream>>>(v, Vh);
     YG_LAUNCHED();
+  }
+  // the tile (systems per thread) of the inner operator: measured once per lattice and system
+  // count on the current fields (one Hphi of each candidate, after a warm-up launch)
+  if (!act.empty()) {
+    const int ns = (int)act.size();
+    if (L.mr_tile[ns] == 0) {
+      cudaEvent_t e0, e1;
+      YG_CUDA(cudaEventCreate(&e0));
+      YG_CUDA(cudaEventCreate(&e1));
+      float best_ms = 0.f;
+      int best_tile = 4, calls = 0;
+      for (int cand : kTiles) {
+        if (cand > 1 && cand >= 2 * ns) continue;
+        tile = cand;
+        calls += 4;
+        hphi(false, false);                      // warm-up; t only (p untouched)
+        YG_CUDA(cudaEventRecord(e0, L.stream));
+        for (int rep = 0; rep < 3; rep++) hphi(false, false);
+        YG_CUDA(cudaEventRecord(e1, L.stream));
+        YG_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        YG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (best_ms == 0.f || ms < best_ms) { best_ms = ms; best_tile = cand; }
+      }
+      YG_CUDA(cudaEventDestroy(e0));
+      YG_CUDA(cudaEventDestroy(e1));
+      L.mvm -= 2 * ns * calls;                   // the timing launches are not MVMs of the solve
+      L.mr_tile[ns] = best_tile;
+    }
+    tile = L.mr_tile[ns];
   }
   const double d2 = delta * delta;
   constexpr int kStagnate = 100;   // as the single-system solver: force an update after 100 flat iterations
@@ -578,7 +622,7 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
     std::vector<int> upd;
     for (int i : act) {
       if (skip[i]) { skip[i] = 0; continue; }
-      const double rp = hist[2 * i + (it & 1)];
+      const double rp = hist[2 * i + ((it - 1) & 1)];   // written by iteration it - 2
       if (!std::isfinite(rp)) throw Error(YG_NONFINITE, "non-finite value in cg_mixed_multi");
       if (rp < 0.25 * min_cycle[i]) { min_cycle[i] = rp; since[i] = 0; }
       else since[i]++;
