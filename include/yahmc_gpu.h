@@ -325,14 +325,14 @@ int yg_gauge_load_hirep(yg_lattice *lat, const char *path, int *num_cnfg, double
  * are linear.  The per-site channel mixing runs as BF16 products with FP32 accumulation on the
  * tensor cores (forward, adjoint and weight gradient).
  * Weights: 9*Co*Ci*4*4 complex numbers as (re, im) doubles, index ((p*Co + o)*Ci + i)*16 + s*4 + s'.
- * Activation planes (yg_ptc_layer): float, plane ((ch*12 + spin*3 + colour)*2 + re/im) of V
- * values in the reference's site order. */
+ * Activations (yg_ptc_layer): float site blocks, channel ch of site id (the reference's site
+ * order) is 24 floats at (ch*V + id)*24, float (spin*3 + colour)*2 + re/im. */
 typedef struct yg_ptc yg_ptc;
 int yg_ptc_create(yg_lattice *lat, int nlayers, const int *channels, yg_ptc **out);
 int yg_ptc_destroy(yg_ptc *net);
 int yg_ptc_set_weights(yg_ptc *net, int layer, const double *w);
 int yg_ptc_get_weights(yg_ptc *net, int layer, double *w);
-/* one layer on device activation planes; adjoint = 1: the input-gradient layer (Co -> Ci) */
+/* one layer on device activations; adjoint = 1: the input-gradient layer (Co -> Ci) */
 int yg_ptc_layer(yg_ptc *net, int layer, int adjoint, const float *dev_in, float *dev_out);
 /* dst (even sites) = the network applied to the even-site field src embedded with zero odd
  * sites (the even-even block of D^-1 is the inverse of the Schur operator Dphi) */
@@ -340,6 +340,9 @@ int yg_ptc_apply(yg_ptc *net, double *dst, const double *src);
 /* training: loss = sum_k |N(r_k) - e_k|^2 / |e_k|^2 over even-site pairs with Dphi e_k = r_k,
  * and its gradient d loss / d conj(W), all layers' weights concatenated in the layout above */
 int yg_ptc_gradient(yg_ptc *net, int npairs, double *const *r, double *const *e, double *loss, double *grads);
+/* weight gradients d loss / d conj(W) for any loss whose derivative with respect to conj(N(src))
+ * (on the even sites) is the field gout: forward on src, backward from gout */
+int yg_ptc_backward(yg_ptc *net, const double *src, const double *gout, double *grads);
 /* flexible GCR on Dphi with the network as right preconditioner (net may be NULL: plain GCR),
  * restarted every `restart` directions; the true FP64 residual |b - Dphi x|^2 < prec |b|^2 ends
  * the solve; no progress over four restart cycles hands over to the plain even-odd CG on the
@@ -371,6 +374,11 @@ int yg_end_fermion_force(yg_lattice *lat, double dt);                           
 int yg_wilson_fermion_force(yg_lattice *lat, double dt, double mass, double residue, double *lhs, double *rhs); /* forces.cpp:175-227 */
 int yg_wilson_fermion_force_q(yg_lattice *lat, double dt, double mass, double residue, double *rhs);            /* forces.cpp:230-236 */
 int yg_clover_fermion_force(yg_lattice *lat, double residue, double *lhs, double *rhs);             /* forces.cpp:122-172 */
+/* The pole loop of MonomialRHMC::update (monomials/rhmc.cpp:100-103): wilson_fermion_force_q(dt, mass,
+ * residues[k], rhs[k]) for k < n <= 32, as one batched force (the links are read, and cl_force and the
+ * momenta written, once for all poles); the odd halves of rhs[k] are replaced as by the reference */
+int yg_wilson_fermion_force_q_multi(yg_lattice *lat, double dt, double mass, int n, const double *residues,
+                                    double *const *rhs);
 int yg_clover_logdet_force(yg_lattice *lat, double mass, double residue);                           /* forces.cpp:109-119 */
 int yg_wilson_gauge_force(yg_lattice *lat, double dt, double beta);                                 /* forces.cpp:262-283 */
 int yg_avr_plaquette(yg_lattice *lat, double *out);                                                 /* wilsonloop.cpp:116-133 (1x1) */

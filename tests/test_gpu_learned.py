@@ -16,19 +16,19 @@ TOL = 2e-2
 
 
 def _planes(x):
-    """oracle field (V, C, d, 4) complex -> activation planes ((ch*12 + s*3 + a)*2 + re/im, V) float32"""
-    V, C, d, _ = x.shape
-    p = np.empty((C, 4, d, 2, V), dtype=np.float32)
-    t = np.transpose(x, (1, 3, 2, 0))          # (C, 4, d, V)
-    p[..., 0, :] = t.real
-    p[..., 1, :] = t.imag
+    """oracle field (V, C, d, 4) complex -> activation site blocks: channel ch of site id is 24
+    floats at (ch*V + id)*24, float (spin*3 + colour)*2 + re/im"""
+    t = np.transpose(x, (1, 0, 3, 2))          # (C, V, 4, d)
+    p = np.empty(t.shape + (2,), dtype=np.float32)
+    p[..., 0] = t.real
+    p[..., 1] = t.imag
     return p.reshape(-1)
 
 
 def _from_planes(p, V, C, d=3):
-    p = p.reshape(C, 4, d, 2, V)
-    z = p[..., 0, :] + 1j * p[..., 1, :]
-    return np.transpose(z, (3, 0, 2, 1))       # (V, C, d, 4)
+    p = p.reshape(C, V, 4, d, 2)
+    z = p[..., 0] + 1j * p[..., 1]
+    return np.transpose(z, (1, 0, 3, 2))       # (V, C, d, 4)
 
 
 def _rand(rng, shape):
@@ -141,24 +141,24 @@ def test_fgcr_meets_true_residual_and_falls_back_with_a_useless_network():
     assert _rel(c, a) < 1e-8
 
 
-def test_training_cuts_fgcr_iterations():
-    """Ablation: the identity-initialised network before training is plain GCR; after a short
-    training on CG errors of this lattice's own solves it needs fewer GCR iterations."""
-    from yahmc_b200 import Ptc, learned
+def test_trained_network_cuts_fgcr_iterations():
+    """Ablation: the network, started from the first-order hopping expansion of the Schur
+    inverse and trained on CG errors of this lattice's own solves, needs fewer flexible-GCR
+    iterations than GCR without it (both stop on the same true residual)."""
+    from yahmc_b200 import Ptc, heatbath, learned
     lat, O, rng = make_pair("su3_fund_ap", (8, 8, 8, 8), seed=85)
-    from yahmc_b200 import heatbath
-    U, _ = heatbath.thermalised_field((8, 8, 8, 8), 5.6, 10, 2)
+    U, _ = heatbath.thermalised_field((8, 8, 8, 8), 5.6, 30, 2)
     lat.set_links(U)
-    mass, prec = -0.6, 1e-20
-    net = Ptc(lat, (1, 8, 8, 1))
-    net.set_weights(learned.near_identity(net.shapes(), rng, noise=0.0))
+    mass, prec = -0.7, 1e-20
     b = lat.field(source(O, rng))
-    x = lat.field()
-    st_id = lat.fgcr(mass, prec, x, b, net=net)
-    pairs = learned.training_pairs(lat, mass, 2, rng)
-    hist = learned.train(net, pairs, steps=60, lr=3e-3, batch=4, rng=rng)
-    assert hist[-1] < hist[0]
-    x2 = lat.field()
-    st_tr = lat.fgcr(mass, prec, x2, b, net=net)
-    assert st_tr["status"] == 0 and st_tr["true_residual"] < prec
-    assert st_tr["iterations"] < st_id["iterations"], (st_tr, st_id)
+    plain = lat.fgcr(mass, prec, lat.field(), b, net=None)
+    net = Ptc(lat, (1, 8, 8, 1))
+    net.set_weights(learned.hopping_start(net.shapes(), mass, rng))
+    start = lat.fgcr(mass, prec, lat.field(), b, net=net)
+    pairs = learned.training_pairs(lat, mass, 3, rng, stops=(10, 25, 50, 100), random_pairs=2)
+    hist = learned.train(net, pairs, steps=100, lr=1e-4, batch=4, rng=rng)
+    assert np.mean(hist[-10:]) < np.mean(hist[:10])
+    trained = lat.fgcr(mass, prec, lat.field(), b, net=net)
+    for st in (plain, start, trained):
+        assert st["status"] == 0 and st["fallback"] == 0 and st["true_residual"] < prec
+    assert trained["iterations"] < plain["iterations"], (trained, start, plain)

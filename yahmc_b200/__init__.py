@@ -126,9 +126,10 @@ _SIGNATURES = {
     "yg_reunitarize": [_P], "yg_momenta_gaussian": [_P, ctypes.c_ulonglong], "yg_momenta_action": [_P, _P],
     "yg_gauge_backup": [_P], "yg_gauge_restore": [_P],
     "yg_field_sqnorm_noalloc": [_P, ctypes.c_long, _P, _P],
+    "yg_wilson_fermion_force_q_multi": [_P, _D, _D, _I, _P, _P],
     "yg_ptc_create": [_P, _I, _P, _P], "yg_ptc_destroy": [_P], "yg_ptc_set_weights": [_P, _I, _P],
     "yg_ptc_get_weights": [_P, _I, _P], "yg_ptc_layer": [_P, _I, _I, _P, _P], "yg_ptc_apply": [_P, _P, _P],
-    "yg_ptc_gradient": [_P, _I, _P, _P, _P, _P],
+    "yg_ptc_gradient": [_P, _I, _P, _P, _P, _P], "yg_ptc_backward": [_P, _P, _P, _P],
     "yg_fgcr": [_P, _P, ctypes.POINTER(InvPar), _I, _P, _P, ctypes.POINTER(SolveStats)],
     "yg_solve_learned": [_P, _P, ctypes.POINTER(InvPar), _I, _P, _P, ctypes.POINTER(SolveStats)],
 }
@@ -207,7 +208,7 @@ class Ptc:
         return out
 
     def layer(self, l, adjoint, dev_in: int, dev_out: int):
-        """One layer on device activation planes (raw device pointers)."""
+        """One layer on device activations (site blocks; raw device pointers)."""
         self.lat._check(self.lib.yg_ptc_layer(self.h, int(l), int(adjoint), ctypes.c_void_p(dev_in),
                                               ctypes.c_void_p(dev_out)))
 
@@ -228,6 +229,17 @@ class Ptc:
             grads.append(raw[2 * off:2 * (off + sz)].view(complex).reshape(shp).copy())
             off += sz
         return loss.value, grads
+
+    def backward(self, src, gout):
+        """Per-layer gradients d loss / d conj(W) given gout = d loss / d conj(N(src))."""
+        sizes = [int(np.prod(s)) for s in self.shapes()]
+        raw = np.zeros(2 * sum(sizes))
+        self.lat._check(self.lib.yg_ptc_backward(self.h, src.ptr, gout.ptr, _ptr(raw)))
+        grads, off = [], 0
+        for shp, sz in zip(self.shapes(), sizes):
+            grads.append(raw[2 * off:2 * (off + sz)].view(complex).reshape(shp).copy())
+            off += sz
+        return grads
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -715,6 +727,13 @@ class Lattice:
 
     def wilson_fermion_force_q(self, dt, mass, residue, rhs):
         self._check(self.lib.yg_wilson_fermion_force_q(self.h, dt, mass, residue, rhs.ptr))
+
+    def wilson_fermion_force_q_multi(self, dt, mass, residues, rhs):
+        """The pole loop of MonomialRHMC::update as one batched force (yg_wilson_fermion_force_q_multi)."""
+        n = len(rhs)
+        res = np.ascontiguousarray(residues, dtype=np.float64)
+        pr = (ctypes.c_void_p * n)(*[f.ptr for f in rhs])
+        self._check(self.lib.yg_wilson_fermion_force_q_multi(self.h, dt, mass, n, _ptr(res), pr))
 
     def clover_fermion_force(self, residue, lhs, rhs):
         self._check(self.lib.yg_clover_fermion_force(self.h, residue, lhs.ptr, rhs.ptr))

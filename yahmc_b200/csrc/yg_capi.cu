@@ -448,6 +448,9 @@ int yg_ptc_gradient(yg_ptc *h, int npairs, double *const *r, double *const *e, d
     *loss = yg::ptc_gradient(ptc(h), npairs, r, e, grads);
   });
 }
+int yg_ptc_backward(yg_ptc *h, const double *src, const double *gout, double *grads) {
+  return guard([&] { need(src, "src"); need(gout, "gout"); need(grads, "grads"); yg::ptc_backward(ptc(h), src, gout, grads); });
+}
 int yg_fgcr(yg_lattice *l, yg_ptc *h, const yg_inv_par *p, int restart, double *x, double *b, yg_solve_stats *st) {
   return guard_status([&] {
     check_par(p); need(x, "x"); need(b, "b"); need(st, "stats");
@@ -499,6 +502,15 @@ int yg_wilson_fermion_force(yg_lattice *l, double dt, double m, double res, doub
 }
 int yg_wilson_fermion_force_q(yg_lattice *l, double dt, double m, double res, double *rhs) {
   return guard([&] { need(rhs, "rhs"); yg::wilson_fermion_force_q(lat(l), dt, m, res, rhs); });
+}
+int yg_wilson_fermion_force_q_multi(yg_lattice *l, double dt, double mass, int n, const double *residues,
+                                    double *const *rhs) {
+  return guard([&] {
+    need(residues, "residues");
+    need(rhs, "rhs");
+    for (int k = 0; k < n; k++) need(rhs[k], "rhs[k]");
+    yg::wilson_fermion_force_q_multi(lat(l), dt, mass, n, residues, rhs);
+  });
 }
 int yg_clover_fermion_force(yg_lattice *l, double res, double *lhs, double *rhs) {
   return guard([&] { need(lhs, "lhs"); need(rhs, "rhs"); yg::clover_fermion_force(lat(l), res, lhs, rhs); });

@@ -39,6 +39,44 @@ void wilson_fermion_force_q(Lattice &L, double dt, double mass, double residue, 
   wilson_fermion_force(L, dt, mass, residue, tmp, rhs);
 }
 
+// the loop of MonomialRHMC::update (rhmc.cpp:100-103) over the poles of a rational
+// approximation, as one batched force: for every pole n the fields of
+// wilson_fermion_force_q(dt, mass, residue_n, rhs_n) are formed (tmp_n = Hphi rhs_n, and with
+// even-odd preconditioning the odd halves of both replaced by A_oo^-1 H_oe, in place like the
+// reference), then the clover force and the hopping force of all poles are summed in one
+// launch each, reading the links and writing cl_force and the momenta once
+static constexpr int kPoleSlot = 400;   // scratch fields kPoleSlot .. kPoleSlot + n - 1
+
+void wilson_fermion_force_q_multi(Lattice &L, double dt, double mass, int n, const double *residue,
+                                  double *const *rhs) {
+  if (n < 1 || n > kMaxPoles) throw Error(YG_ERR_ARG, "1..32 poles");
+  PoleSet ps{};
+  ps.n = n;
+  for (int k = 0; k < n; k++) {
+    double *tmp = L.scratch_field(kPoleSlot + k);
+    hphi(L, mass, tmp, rhs[k]);
+    if (L.p.eo) {
+      hop(L, rhs[k], rhs[k], 2, 1.0, false);
+      hop(L, tmp, tmp, 2, 1.0, false);
+      if (L.p.clover) {
+        clover_inv_apply(L, mass, rhs[k], rhs[k], 2, false);
+        clover_inv_apply(L, mass, tmp, tmp, 2, false);
+      }
+    }
+    ps.lhs[k] = (const double2 *)tmp;
+    ps.rhs[k] = (const double2 *)rhs[k];
+  }
+  if (L.p.clover) {
+    for (int k = 0; k < n; k++) ps.w[k] = residue[k];
+    YG_DISPATCH_D(L.d, K::clover_fermion_force_multi(L.cl_force.as<double2>(), ps, L.g, L.stream));
+    YG_LAUNCHED();
+  }
+  for (int k = 0; k < n; k++) ps.w[k] = (L.p.eo ? -1.0 : 1.0) * dt * residue[k];
+  YG_DISPATCH_D(L.d, K::hopping_force_multi(L.mom.as<double>(), ps, L.links.as<double2>(), L.g, L.rt.itrepr, L.ng,
+                                            L.stream));
+  YG_LAUNCHED();
+}
+
 void begin_fermion_force(Lattice &L) {
   if (!L.p.clover) return;
   YG_CUDA(cudaMemsetAsync(L.cl_force.p, 0, L.cl_force.bytes, L.stream));

@@ -280,7 +280,95 @@ __global__ void k_clover_force_core(double *mom, const double2 *clf, const doubl
   }
 }
 
+// ---- the same two forces summed over the poles of a rational approximation
+// (rhmc.cpp:86-106 calls wilson_fermion_force_q once per pole): one thread per (site, slot)
+// accumulates sum_n w_n fmat_n in registers and updates cl_force once; one thread per
+// (site, mu) accumulates sum_n c_n fmat_n, multiplies by U once and projects once.  The
+// projection is linear, so the result equals the sum of the per-pole forces up to rounding.
+template <int D>
+__global__ void k_clover_fermion_force_multi(double2 *clf, PoleSet ps, Geom g) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= 6L * g.V) return;
+  const int id = (int)(t / 6), slot = (int)(t % 6);
+  double2 f[D * D];
+  YG_UNROLL_DF
+  for (int k = 0; k < D * D; k++) f[k] = make_double2(0, 0);
+#pragma unroll 1
+  for (int n = 0; n < ps.n; n++) {
+    double2 l[4][D], r[4][D], sl[4][D], sr[4][D], fn[D * D];
+    ld_spinor64<D>(l, ps.lhs[n], g, id);
+    ld_spinor64<D>(r, ps.rhs[n], g, id);
+    g5_sigma<D>(sl, l, slot);
+    g5_sigma<D>(sr, r, slot);
+    YG_UNROLL_DF
+    for (int k = 0; k < D * D; k++) fn[k] = make_double2(0, 0);
+    outer_acc<D>(fn, sl, r);
+    outer_acc<D>(fn, sr, l);
+    YG_UNROLL_DF
+    for (int k = 0; k < D * D; k++) {
+      f[k].x += ps.w[n] * fn[k].x;
+      f[k].y += ps.w[n] * fn[k].y;
+    }
+  }
+  YG_UNROLL_DF
+  for (int k = 0; k < D * D; k++) {
+    long ix = fidx(g, id, slot * D * D + k, 6 * D * D);
+    double2 o = clf[ix];
+    o.x += f[k].x;
+    o.y += f[k].y;
+    clf[ix] = o;
+  }
+}
+
+template <int D>
+__global__ void k_hopping_force_multi(double *mom, PoleSet ps, const double2 *U, Geom g, const double2 *itrepr,
+                                      int ng) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= 4L * g.V) return;
+  int id = (int)(t >> 2), mu = (int)(t & 3);
+  int c[4];
+  coords_of(g, id, c);
+  int fw = neighbour(g, c, mu, +1);
+  double2 f[D * D];
+  YG_UNROLL_DF
+  for (int k = 0; k < D * D; k++) f[k] = make_double2(0, 0);
+#pragma unroll 1
+  for (int n = 0; n < ps.n; n++) {
+    double2 a[4][D], b[4][D], tl[4][D], tr[4][D], fn[D * D];
+    ld_spinor64<D>(a, ps.lhs[n], g, fw);
+    g5_omg<D>(tl, a, mu);
+    ld_spinor64<D>(a, ps.rhs[n], g, fw);
+    g5_omg<D>(tr, a, mu);
+    ld_spinor64<D>(a, ps.rhs[n], g, id);
+    ld_spinor64<D>(b, ps.lhs[n], g, id);
+    YG_UNROLL_DF
+    for (int k = 0; k < D * D; k++) fn[k] = make_double2(0, 0);
+    outer_acc<D>(fn, tl, a);
+    outer_acc<D>(fn, tr, b);
+    YG_UNROLL_DF
+    for (int k = 0; k < D * D; k++) {
+      f[k].x += ps.w[n] * fn[k].x;
+      f[k].y += ps.w[n] * fn[k].y;
+    }
+  }
+  double2 u[D * D], m[D * D];
+  ld_mat<D>(u, U, g, id, mu, 4);
+  mat_mul<D>(m, u, f);
+  project_add<D>(mom + (4L * id + mu) * ng, m, itrepr, ng, 1.0);
+}
+
 // ------------------------------------------------------------------ launchers
+template <int D>
+void DK<D>::clover_fermion_force_multi(double2 *clf, const PoleSet &ps, Geom g, cudaStream_t s) {
+  k_clover_fermion_force_multi<D><<<nblk(6L * g.V, 64), 64, 0, s>>>(clf, ps, g);
+}
+
+template <int D>
+void DK<D>::hopping_force_multi(double *mom, const PoleSet &ps, const double2 *U, Geom g, const double2 *itrepr,
+                                int ng, cudaStream_t s) {
+  k_hopping_force_multi<D><<<nblk(4L * g.V, 64), 64, 0, s>>>(mom, ps, U, g, itrepr, ng);
+}
+
 template <int D>
 void DK<D>::clover_fermion_force(double2 *clf, const double2 *lhs, const double2 *rhs, Geom g, double residue,
                                  cudaStream_t s) {

@@ -7,6 +7,8 @@ namespace yg {
 template void DK<10>::clover_fermion_force(double2 *, const double2 *, const double2 *, Geom, double, cudaStream_t);
 template void DK<10>::hopping_force(double *, const double2 *, const double2 *, const double2 *, Geom, const double2 *, int, double, cudaStream_t);
 template void DK<10>::clover_ldl_force(double2 *, const double2 *, Geom, double, cudaStream_t);
+template void DK<10>::clover_fermion_force_multi(double2 *, const PoleSet &, Geom, cudaStream_t);
+template void DK<10>::hopping_force_multi(double *, const PoleSet &, const double2 *, Geom, const double2 *, int, cudaStream_t);
 template void DK<10>::clover_force_core(double *, const double2 *, const double2 *, Geom, const double2 *, int, double, cudaStream_t);
 template struct RK<4, 10>;
 }  // namespace yg

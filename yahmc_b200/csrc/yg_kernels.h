@@ -34,6 +34,15 @@ struct HopArgs {
   int zero_add_at_boundary;
 };
 
+// The fields of several pseudo-fermion poles for one batched force launch
+constexpr int kMaxPoles = 32;
+struct PoleSet {
+  const double2 *lhs[kMaxPoles];
+  const double2 *rhs[kMaxPoles];
+  double w[kMaxPoles];       // per-pole coefficient
+  int n;
+};
+
 // Dirac-operator and force kernels of representation dimension D
 template <int D>
 struct DK {
@@ -51,6 +60,10 @@ struct DK {
   static void hopping_force(double *mom, const double2 *lhs, const double2 *rhs, const double2 *U, Geom g,
                             const double2 *itrepr, int ng, double coeff, cudaStream_t s);
   static void clover_ldl_force(double2 *clf, const double2 *ldl, Geom g, double coeff, cudaStream_t s);
+  // sums over the poles of a PoleSet, one read-modify-write of cl_force / the momenta
+  static void clover_fermion_force_multi(double2 *clf, const PoleSet &ps, Geom g, cudaStream_t s);
+  static void hopping_force_multi(double *mom, const PoleSet &ps, const double2 *U, Geom g, const double2 *itrepr,
+                                  int ng, cudaStream_t s);
   static void clover_force_core(double *mom, const double2 *clf, const double2 *U, Geom g, const double2 *itrepr,
                                 int ng, double coeff, cudaStream_t s);
 };

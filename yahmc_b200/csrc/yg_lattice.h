@@ -197,6 +197,7 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int 
 void clover_fermion_force(Lattice &L, double residue, double *lhs, double *rhs);
 void wilson_fermion_force(Lattice &L, double dt, double mass, double residue, double *lhs, double *rhs);
 void wilson_fermion_force_q(Lattice &L, double dt, double mass, double residue, double *rhs);
+void wilson_fermion_force_q_multi(Lattice &L, double dt, double mass, int n, const double *residue, double *const *rhs);
 void begin_fermion_force(Lattice &L);
 void end_fermion_force(Lattice &L, double dt);
 void clover_logdet_force(Lattice &L, double mass, double residue);
@@ -270,6 +271,7 @@ void ptc_get_weights(Ptc &n, int l, double *w);
 void ptc_layer(Ptc &n, int l, int adjoint, const float *in, float *out);
 void ptc_apply(Ptc &n, double *dst, const double *src);
 double ptc_gradient(Ptc &n, int npairs, double *const *r, double *const *e, double *grads);
+void ptc_backward(Ptc &n, const double *src, const double *gout, double *grads);
 int fgcr(Lattice &L, Ptc *net, const yg_inv_par &par, int restart, double *x, double *b, yg_solve_stats *st);
 int solve_learned(Lattice &L, Ptc *net, const yg_inv_par &par, int restart, double *x, double *b,
                   yg_solve_stats *st);

@@ -161,8 +161,11 @@ __device__ __forceinline__ void herm_block(float2 (&y)[6], const float4 *C, int 
 // STEP 1 (odd output):  dst_j = M_o^-1 (coeff hop(src_j))
 // STEP 2 (even output): dst_j = gamma5 (M_e src2_j + coeff hop(src_j))
 // the single-system compressed operator (shop_site of yg_sloppy.cu) for a tile of systems
+// resident blocks per SM the register budget is cut for: 6 (R = 1), 4 (R = 2), 3 (R = 4)
+template <int R> struct MinBlocks { static constexpr int value = R == 1 ? 6 : R == 2 ? 4 : 3; };
+
 template <int K, int R, int STEP, int NRM>
-__global__ void __launch_bounds__(kHopThreads) k_mhop(MHopArgs a) {
+__global__ void __launch_bounds__(kHopThreads, MinBlocks<R>::value) k_mhop(MHopArgs a) {
   const int tile = blockIdx.x % a.ntile, sb = blockIdx.x / a.ntile;
   const int s0 = tile * R;
   const int rc = min(R, a.nsys - s0);

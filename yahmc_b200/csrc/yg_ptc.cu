@@ -22,8 +22,8 @@
 //     dW[p, o, i][s, s'] = sum_{x, c} g[x, o, c, s] conj((T_p in_i)[x, c, s'])
 // is the same kind of product with the sites as the reduction dimension.
 //
-// Activations are FP32 planes: plane q = ((ch * 12 + spin * 3 + colour) * 2 + re/im), value
-// of site id at q * V + id (id in the reference's site order).  Every wait on the tensor core
+// Activations are FP32 site blocks: channel ch of site id (the reference's site order) is 24
+// floats at (ch * V + id) * 24, float (spin * 3 + colour) * 2 + re/im.  Every wait on the tensor core
 // is bounded; a wait that runs out sets an error word, frees the tensor memory and returns.
 #include <cuda_bf16.h>
 #include <algorithm>
@@ -46,6 +46,7 @@ constexpr int kM = 128;                     // GEMM rows (tcgen05 M)
 constexpr int kThreads = 128;
 constexpr int kTmemCols = 256;              // >= kN, a power of two
 constexpr long kSpinLimit = 1L << 26;       // bounded waits
+constexpr int kStageLd = kN + 1;            // row stride of the epilogue's staging tile (floats)
 
 // ---- shared-memory operand layout: K-major, no swizzle.  Element (r, k) of an R x K tile
 // lives at byte (r / 8) * SBO + (k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2 with SBO = K / 8 * 128:
@@ -162,32 +163,57 @@ __device__ __forceinline__ void path_link(const PtcArgs &a, int id, int nid, int
     }
 }
 
-// transported colour vector of (channel ch, spin s) from site nid: y = u f(nid)
-template <bool IDENT>
-__device__ __forceinline__ void transport3(const float *in, int V, int ch, int s, int nid, const float2 (&u)[9],
-                                           float2 (&y)[3]) {
-  float2 f[3];
-#pragma unroll
-  for (int a = 0; a < 3; a++) {
-    const long q = (long)((ch * 12 + s * 3 + a) * 2);
-    f[a] = make_float2(__ldg(in + q * V + nid), __ldg(in + (q + 1) * V + nid));
-  }
-  if (IDENT) {
-#pragma unroll
-    for (int a = 0; a < 3; a++) y[a] = f[a];
-  } else {
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      float2 acc = make_float2(0.f, 0.f);
-#pragma unroll
-      for (int b = 0; b < 3; b++) cfma(acc, u[a * 3 + b], f[b]);
-      y[a] = acc;
-    }
-  }
-}
-
 __device__ __forceinline__ void put_bf16(unsigned char *base, uint32_t off, float v) {
   *reinterpret_cast<__nv_bfloat16 *>(base + off) = __float2bfloat16_rn(v);
+}
+
+// four consecutive BF16 (one 8-byte store): k-columns k0..k0+3 of row r, k0 a multiple of 4
+__device__ __forceinline__ void put_bf16x4(unsigned char *base, uint32_t off, float v0, float v1, float v2, float v3) {
+  __nv_bfloat162 lo = __floats2bfloat162_rn(v0, v1), hi = __floats2bfloat162_rn(v2, v3);
+  uint2 w;
+  w.x = *reinterpret_cast<uint32_t *>(&lo);
+  w.y = *reinterpret_cast<uint32_t *>(&hi);
+  *reinterpret_cast<uint2 *>(base + off) = w;
+}
+
+// Activations are site blocks: channel ch of site id is 24 floats at (ch * V + id) * 24, float
+// k2 = (spin * 3 + colour) * 2 + re/im.  A thread gathers whole blocks with 16-byte loads.
+struct Block {
+  float4 w[6];
+};
+
+__device__ __forceinline__ void load_block(Block &b, const float *act, long base) {
+  const float4 *p = reinterpret_cast<const float4 *>(act + base * 24);
+#pragma unroll
+  for (int i = 0; i < 6; i++) b.w[i] = __ldg(p + i);
+}
+
+__device__ __forceinline__ float2 blk_c(const Block &b, int s, int a) {   // complex (spin s, colour a)
+  const int k = (s * 3 + a) * 2;
+  const float4 &w = b.w[k >> 2];
+  return (k & 2) ? make_float2(w.z, w.w) : make_float2(w.x, w.y);
+}
+
+// the transported spin-colour block y[s][a] = sum_b u[a][b] f[s][b] (IDENT: y = f)
+template <bool IDENT>
+__device__ __forceinline__ void transport_block(float2 (&y)[4][3], const Block &f, const float2 (&u)[9]) {
+#pragma unroll
+  for (int s = 0; s < 4; s++) {
+    float2 v[3];
+#pragma unroll
+    for (int b = 0; b < 3; b++) v[b] = blk_c(f, s, b);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      if (IDENT) {
+        y[s][a] = v[a];
+      } else {
+        float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int b = 0; b < 3; b++) cfma(acc, u[a * 3 + b], v[b]);
+        y[s][a] = acc;
+      }
+    }
+  }
 }
 
 // ---------------------------------------------------------------- forward layer
@@ -230,7 +256,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_ptc_layer(PtcArgs a) {
       uint4 *dst = reinterpret_cast<uint4 *>(sA);
       for (int e = tid; e < kM * KP * 2 / 16; e += kThreads) dst[e] = __ldg(src + e);
     }
-    // B chunk: the transported inputs of the tile's sites
+    // B chunk: the transported inputs of the tile's sites.  Thread (site j, part) takes the
+    // channels part, part + NPART, ...; a one-channel input is split by spin pairs instead.
     if (tid < kTileSites) {
       const int id = t0 + tid;
       s_site[tid] = id < a.V ? id : -1;
@@ -238,25 +265,46 @@ __global__ void __launch_bounds__(kThreads, 1) k_ptc_layer(PtcArgs a) {
     }
     __syncthreads();
     {
-      const int j = tid % kTileSites, half = tid / kTileSites;
+      constexpr int NPART = kThreads / kTileSites;
+      const int j = tid % kTileSites, part = tid / kTileSites;
       const int id = s_site[j], nid = s_nbr[j];
       float2 u[9];
       if (id >= 0 && p > 0) path_link(a, id, nid, p, u);
-      for (int q = half; q < PAIRS; q += kThreads / kTileSites) {
-        const int ch = q >> 2, s = q & 3;
-        float2 y[3];
-        if (id < 0) {
-          y[0] = y[1] = y[2] = make_float2(0.f, 0.f);
-        } else if (p == 0) {
-          transport3<true>(a.in, a.V, ch, s, nid, u, y);
-        } else {
-          transport3<false>(a.in, a.V, ch, s, nid, u, y);
+      constexpr int NCH = CI >= NPART ? CI / NPART : 1;     // channels per thread
+      constexpr int CB = NCH < 4 ? NCH : 4;                  // gathered together
+#pragma unroll 1
+      for (int c0 = 0; c0 < NCH; c0 += CB) {
+        Block f[CB];
+#pragma unroll
+        for (int q = 0; q < CB; q++) {
+          const int ch = CI >= NPART ? part + NPART * (c0 + q) : 0;
+          if (id >= 0) load_block(f[q], a.in, (long)ch * a.V + nid);
+          else
+#pragma unroll
+            for (int i = 0; i < 6; i++) f[q].w[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-          const int r = c * kTileSites + j;
-          put_bf16(sB, kmajor_off(r, q, KP), y[c].x);
-          put_bf16(sB, kmajor_off(r, PAIRS + q, KP), y[c].y);
+        for (int q = 0; q < CB; q++) {
+          const int ch = CI >= NPART ? part + NPART * (c0 + q) : 0;
+          float2 y[4][3];
+          if (p == 0) transport_block<true>(y, f[q], u);
+          else transport_block<false>(y, f[q], u);
+          if (CI >= NPART) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+              const int r = c * kTileSites + j;
+              put_bf16x4(sB, kmajor_off(r, ch * 4, KP), y[0][c].x, y[1][c].x, y[2][c].x, y[3][c].x);
+              put_bf16x4(sB, kmajor_off(r, PAIRS + ch * 4, KP), y[0][c].y, y[1][c].y, y[2][c].y, y[3][c].y);
+            }
+          } else if (part == 0) {
+            // one input channel: columns 0..3 real, 4..7 imaginary, written by part 0
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+              const int r = c * kTileSites + j;
+              put_bf16x4(sB, kmajor_off(r, 0, KP), y[0][c].x, y[1][c].x, y[2][c].x, y[3][c].x);
+              put_bf16x4(sB, kmajor_off(r, 4, KP), y[0][c].y, y[1][c].y, y[2][c].y, y[3][c].y);
+            }
+          }
         }
       }
     }
@@ -279,24 +327,36 @@ __global__ void __launch_bounds__(kThreads, 1) k_ptc_layer(PtcArgs a) {
   }
 
   if (ok) {
-    // epilogue: row m = (o, s) real part (m < 4 CO) or imaginary part (4 CO <= m < 8 CO)
+    // epilogue: accumulator row m = (o, s) real part (m < 4 CO) or imaginary part
+    // (4 CO <= m < 8 CO), column n = (colour, site); staged through shared memory (the operand
+    // buffers are free now), then every thread writes whole 96-byte site blocks
+    float *stage = reinterpret_cast<float *>(sm);
     const int m = warp * 32 + (tid & 31);
-    const bool live = m < 8 * CO;
-    if (__any_sync(0xffffffffu, live)) {
-      const int ri = m / (4 * CO), os = m % (4 * CO), o = os >> 2, s = os & 3;
+    if (warp * 32 < 8 * CO) {
 #pragma unroll 1
       for (int cb = 0; cb < kN / 32; cb++) {
         float v[32];
         tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + cb * 32, v);
-        if (live) {
-          const int c = (cb * 32) / kTileSites, j0 = (cb * 32) % kTileSites;
-          const long q = (long)((o * 12 + s * 3 + c) * 2 + ri);
-          float *dst = a.out + q * a.V + t0 + j0;
 #pragma unroll
-          for (int i = 0; i < 32; i++)
-            if (t0 + j0 + i < a.V) dst[i] = v[i];
-        }
+        for (int i = 0; i < 32; i++) stage[m * kStageLd + cb * 32 + i] = v[i];
       }
+    }
+    __syncthreads();
+    for (int e = tid; e < kTileSites * CO; e += kThreads) {
+      const int j = e % kTileSites, o = e / kTileSites;
+      if (t0 + j >= a.V) continue;
+      float4 w[6];
+      float *wf = reinterpret_cast<float *>(w);
+#pragma unroll
+      for (int s = 0; s < 4; s++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          wf[(s * 3 + c) * 2] = stage[(o * 4 + s) * kStageLd + c * kTileSites + j];
+          wf[(s * 3 + c) * 2 + 1] = stage[(4 * CO + o * 4 + s) * kStageLd + c * kTileSites + j];
+        }
+      float4 *dst = reinterpret_cast<float4 *>(a.out + ((long)o * a.V + t0 + j) * 24);
+#pragma unroll
+      for (int i = 0; i < 6; i++) dst[i] = w[i];
     }
   }
   tc_fence_before();
@@ -343,20 +403,25 @@ __global__ void __launch_bounds__(kThreads, 1) k_ptc_wgrad(PtcArgs a, int ntiles
 
   for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
     const int t0 = tile * kTileSites;
-    // B: the output gradients of the tile (the same for every path)
-    for (int e = tid; e < OPAIRS * kN; e += kThreads) {
-      const int os = e / kN, n = e % kN, c = n / kTileSites, j = n % kTileSites;
-      const int id = t0 + j, o = os >> 2, s = os & 3;
-      float gr = 0.f, gi = 0.f;
-      if (id < a.V) {
-        const long q = (long)((o * 12 + s * 3 + c) * 2);
-        gr = __ldg(a.gin + q * a.V + id);
-        gi = __ldg(a.gin + (q + 1) * a.V + id);
-      }
-      put_bf16(sB, kmajor_off(os, n, KW), gr);
-      put_bf16(sB, kmajor_off(os, kN + n, KW), gi);
-      put_bf16(sB, kmajor_off(OPAIRS + os, n, KW), -gi);
-      put_bf16(sB, kmajor_off(OPAIRS + os, kN + n, KW), gr);
+    // B: the output gradients of the tile (the same for every path), site blocks of gin
+    for (int e = tid; e < kTileSites * CO; e += kThreads) {
+      const int j = e % kTileSites, o = e / kTileSites, id = t0 + j;
+      Block gb;
+      if (id < a.V) load_block(gb, a.gin, (long)o * a.V + id);
+      else
+#pragma unroll
+        for (int i = 0; i < 6; i++) gb.w[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int sp = 0; sp < 4; sp++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const float2 gv = blk_c(gb, sp, c);
+          const int os = o * 4 + sp, n = c * kTileSites + j;
+          put_bf16(sB, kmajor_off(os, n, KW), gv.x);
+          put_bf16(sB, kmajor_off(os, kN + n, KW), gv.y);
+          put_bf16(sB, kmajor_off(OPAIRS + os, n, KW), -gv.y);
+          put_bf16(sB, kmajor_off(OPAIRS + os, kN + n, KW), gv.x);
+        }
     }
     for (int pp = 0; pp < PG && ok; pp++) {
       const int p = p0 + pp;
@@ -367,21 +432,39 @@ __global__ void __launch_bounds__(kThreads, 1) k_ptc_wgrad(PtcArgs a, int ntiles
       }
       __syncthreads();
       {
-        const int j = tid % kTileSites, half = tid / kTileSites;
+        constexpr int NPART = kThreads / kTileSites;
+        const int j = tid % kTileSites, part = tid / kTileSites;
         const int id = s_site[j], nid = s_nbr[j];
         float2 u[9];
         if (id >= 0 && p > 0) path_link(a, id, nid, p, u);
-        for (int q = half; q < PAIRS; q += kThreads / kTileSites) {
-          const int ch = q >> 2, s = q & 3;
-          float2 y[3];
-          if (id < 0) y[0] = y[1] = y[2] = make_float2(0.f, 0.f);
-          else if (p == 0) transport3<true>(a.in, a.V, ch, s, nid, u, y);
-          else transport3<false>(a.in, a.V, ch, s, nid, u, y);
+        constexpr int NCH = CI >= NPART ? CI / NPART : 1;
+        constexpr int CB = NCH < 4 ? NCH : 4;
+#pragma unroll 1
+        for (int c0 = 0; c0 < NCH; c0 += CB) {
+          Block f[CB];
 #pragma unroll
-          for (int c = 0; c < 3; c++) {
-            const int n = c * kTileSites + j;
-            put_bf16(sA, kmajor_off(q, n, KW), y[c].x);
-            put_bf16(sA, kmajor_off(q, kN + n, KW), y[c].y);
+          for (int q = 0; q < CB; q++) {
+            const int ch = CI >= NPART ? part + NPART * (c0 + q) : 0;
+            if (id >= 0) load_block(f[q], a.in, (long)ch * a.V + nid);
+            else
+#pragma unroll
+              for (int i = 0; i < 6; i++) f[q].w[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+#pragma unroll
+          for (int q = 0; q < CB; q++) {
+            const int ch = CI >= NPART ? part + NPART * (c0 + q) : 0;
+            if (CI < NPART && part != 0) continue;
+            float2 y[4][3];
+            if (p == 0) transport_block<true>(y, f[q], u);
+            else transport_block<false>(y, f[q], u);
+#pragma unroll
+            for (int sp = 0; sp < 4; sp++)
+#pragma unroll
+              for (int c = 0; c < 3; c++) {
+                const int n = c * kTileSites + j, row = ch * 4 + sp;
+                put_bf16(sA, kmajor_off(row, n, KW), y[sp][c].x);
+                put_bf16(sA, kmajor_off(row, kN + n, KW), y[sp][c].y);
+              }
           }
         }
       }
@@ -430,29 +513,30 @@ __global__ void __launch_bounds__(kThreads, 1) k_ptc_wgrad(PtcArgs a, int ntiles
 }
 
 // even sites of an FP64 engine field (F[k * Vh + h], complex word k = spin * 3 + colour)
-// -> channel 0 of the activation planes, scaled; odd sites and the other planes zero
+// -> channel 0 of the activations (site blocks), scaled; odd sites zero
 __global__ void k_ptc_from_field(float *act, const double2 *f, int V, int Vh, double scale) {
   const int id = blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= V) return;
+  float *dst = act + (long)id * 24;
 #pragma unroll
   for (int k = 0; k < 12; k++) {
-    double2 v = id < Vh ? f[(long)k * Vh + id] : make_double2(0.0, 0.0);
-    act[(long)(2 * k) * V + id] = (float)(v.x * scale);
-    act[(long)(2 * k + 1) * V + id] = (float)(v.y * scale);
+    const double2 v = id < Vh ? f[(long)k * Vh + id] : make_double2(0.0, 0.0);
+    dst[2 * k] = (float)(v.x * scale);
+    dst[2 * k + 1] = (float)(v.y * scale);
   }
 }
 
-// channel 0 of the activation planes on the even sites -> FP64 engine field, scaled
+// channel 0 of the activations on the even sites -> FP64 engine field, scaled
 __global__ void k_ptc_to_field(double2 *f, const float *act, int V, int Vh, double scale) {
   const int h = blockIdx.x * blockDim.x + threadIdx.x;
   if (h >= Vh) return;
+  const float *src = act + (long)h * 24;
 #pragma unroll
-  for (int k = 0; k < 12; k++)
-    f[(long)k * Vh + h] = make_double2(act[(long)(2 * k) * V + h] * scale, act[(long)(2 * k + 1) * V + h] * scale);
+  for (int k = 0; k < 12; k++) f[(long)k * Vh + h] = make_double2(src[2 * k] * scale, src[2 * k + 1] * scale);
 }
 
 // output gradient of the loss term |y - e|^2 / |e|^2 on channel 0's even sites:
-// g = (y - e) / |e|^2 (odd sites and other planes zero); partials of |y - e|^2 per block
+// g = (y - e) / |e|^2 (odd sites zero); partials of |y - e|^2 per block
 __global__ void k_ptc_loss_grad(float *g, double *part, const float *y, const double2 *e, int V, int Vh, double inv_ne,
                                 double escale) {
   const int id = blockIdx.x * blockDim.x + threadIdx.x;
@@ -463,12 +547,12 @@ __global__ void k_ptc_loss_grad(float *g, double *part, const float *y, const do
       double dr = 0.0, di = 0.0;
       if (id < Vh) {
         const double2 ev = e[(long)k * Vh + id];
-        dr = (double)y[(long)(2 * k) * V + id] - ev.x * escale;
-        di = (double)y[(long)(2 * k + 1) * V + id] - ev.y * escale;
+        dr = (double)y[(long)id * 24 + 2 * k] - ev.x * escale;
+        di = (double)y[(long)id * 24 + 2 * k + 1] - ev.y * escale;
         acc += dr * dr + di * di;
       }
-      g[(long)(2 * k) * V + id] = (float)(dr * inv_ne);
-      g[(long)(2 * k + 1) * V + id] = (float)(di * inv_ne);
+      g[(long)id * 24 + 2 * k] = (float)(dr * inv_ne);
+      g[(long)id * 24 + 2 * k + 1] = (float)(di * inv_ne);
     }
   }
   __shared__ double sh[256];
@@ -479,6 +563,15 @@ __global__ void k_ptc_loss_grad(float *g, double *part, const float *y, const do
     __syncthreads();
   }
   if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+// sum of the per-CTA weight-gradient partials in CTA order (FP64): out[e] = sum_b part[b * n + e]
+__global__ void k_ptc_sum_parts(double *out, const float *part, int nparts, long n) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  double acc = 0.0;
+  for (int b = 0; b < nparts; b++) acc += (double)part[(long)b * n + e];
+  out[e] = acc;
 }
 
 }  // namespace
@@ -492,7 +585,7 @@ struct Ptc {
   DevBuf Af[kPtcMaxLayers], Aa[kPtcMaxLayers];
   DevBuf act[kPtcMaxLayers + 1];        // forward activations
   DevBuf g[2];                          // gradient ping-pong
-  DevBuf part, err, dpart;
+  DevBuf part, err, dpart, wsum;
   int maxc = 1;
 };
 
@@ -543,9 +636,10 @@ std::vector<double> adjoint_weights(const std::vector<double> &w, int ci, int co
   return a;
 }
 
-// at least 96 KiB of shared memory per CTA keeps two CTAs per SM at most, so their tensor
-// memory (256 columns each) always fits the SM's 512 columns and no allocation has to wait
-constexpr size_t kMinSmem = 96 * 1024;
+// at least 100 KiB of shared memory per CTA (the epilogue's staging tile needs 96.5 KiB) keeps
+// two CTAs per SM at most, so their tensor memory (256 columns each) always fits the SM's 512
+// columns and no allocation has to wait
+constexpr size_t kMinSmem = 100 * 1024;
 template <int CI, int CO>
 size_t layer_smem() { return std::max(kMinSmem, (size_t)kM * kp_of(CI) * 2 + (size_t)kN * kp_of(CI) * 2 + 16); }
 template <int CI, int CO>
@@ -646,6 +740,7 @@ void ptc_destroy(Ptc *n) {
   for (auto &b : n->act) b.release();
   for (auto &b : n->g) b.release();
   n->part.release();
+  n->wsum.release();
   n->err.release();
   n->dpart.release();
   delete n;
@@ -722,26 +817,62 @@ static void wgrad(Ptc &n, int l, const float *gin, std::vector<double> &grads) {
   a.part = n.part.as<float>();
   int gx = 0;
   YG_PTC_DISPATCH(ci, co, gx = run_wgrad<CI, CO>(L, a, sms));
-  std::vector<float> part((size_t)gx * kPaths * kM * nb);
-  YG_CUDA(cudaMemcpyAsync(part.data(), n.part.p, part.size() * sizeof(float), cudaMemcpyDeviceToHost, L.stream));
+  // C[(i, s'), (o, s)] summed over the CTAs in order on the device; dW[p][o][i][s][s'] = conj(C)
+  const long per = (long)kPaths * kM * nb;
+  if (n.wsum.bytes < sizeof(double) * per) {
+    n.wsum.release();
+    n.wsum.alloc(sizeof(double) * per);
+  }
+  k_ptc_sum_parts<<<nblk(per, 256), 256, 0, L.stream>>>(n.wsum.as<double>(), n.part.as<float>(), gx, per);
+  YG_LAUNCHED();
+  std::vector<double> sum(per);
+  YG_CUDA(cudaMemcpyAsync(sum.data(), n.wsum.p, sizeof(double) * per, cudaMemcpyDeviceToHost, L.stream));
   check_err(n);
-  // C[(i, s'), (o, s)] summed over the CTAs in order; dW[p][o][i][s][s'] = conj(C)
   for (int p = 0; p < kPaths; p++)
     for (int i = 0; i < ci; i++)
       for (int t = 0; t < 4; t++)
         for (int o = 0; o < co; o++)
           for (int s = 0; s < 4; s++) {
             const int m = i * 4 + t, j = o * 4 + s;
-            double re = 0.0, im = 0.0;
-            for (int b = 0; b < gx; b++) {
-              const float *c = part.data() + ((size_t)b * kPaths + p) * kM * nb + (size_t)m * nb;
-              re += c[j];
-              im += c[4 * co + j];
-            }
+            const double *c = sum.data() + ((size_t)p * kM + m) * nb;
             const size_t idx = ((((size_t)p * co + o) * ci + i) * 4 + s) * 4 + t;
-            grads[2 * idx] += re;
-            grads[2 * idx + 1] -= im;
+            grads[2 * idx] += c[j];
+            grads[2 * idx + 1] -= c[4 * co + j];
           }
+}
+
+// weight gradients for a loss whose derivative with respect to conj(N(src)) on the even sites
+// is gout (an FP64 even-site field): the network runs forward on src / |src| (it is linear,
+// N(src) = |src| N(src / |src|)), and the backward pass starts from |src| gout
+void ptc_backward(Ptc &n, const double *src, const double *gout, double *grads_out) {
+  Lattice &L = *n.L;
+  long lo, cnt;
+  L.view_range(YG_VIEW_EVEN, lo, cnt);
+  const double nr = std::sqrt(blas_sqnorm(L, src, lo, cnt));
+  if (!(nr > 0.0)) throw Error(YG_ERR_ARG, "ptc_backward: zero input");
+  k_ptc_from_field<<<nblk(L.V, 256), 256, 0, L.stream>>>(n.act[0].as<float>(), (const double2 *)src, (int)L.V,
+                                                          (int)L.Vh, 1.0 / nr);
+  YG_LAUNCHED();
+  forward(n);
+  float *gcur = n.g[0].as<float>(), *gnext = n.g[1].as<float>();
+  YG_CUDA(cudaMemsetAsync(gcur, 0, planes_bytes(L, n.maxc), L.stream));
+  k_ptc_from_field<<<nblk(L.V, 256), 256, 0, L.stream>>>(gcur, (const double2 *)gout, (int)L.V, (int)L.Vh, nr);
+  YG_LAUNCHED();
+  std::vector<std::vector<double>> grads(n.nl);
+  for (int l = 0; l < n.nl; l++) grads[l].assign(n.W[l].size(), 0.0);
+  for (int l = n.nl - 1; l >= 0; l--) {
+    wgrad(n, l, gcur, grads[l]);
+    if (l > 0) {
+      ptc_layer(n, l, 1, gcur, gnext);
+      std::swap(gcur, gnext);
+    }
+  }
+  check_err(n);
+  size_t off = 0;
+  for (int l = 0; l < n.nl; l++) {
+    std::memcpy(grads_out + off, grads[l].data(), sizeof(double) * grads[l].size());
+    off += grads[l].size();
+  }
 }
 
 double ptc_gradient(Ptc &n, int npairs, double *const *r, double *const *e, double *grads_out) {

@@ -20,6 +20,43 @@ import numpy as np
 from . import fields
 
 
+# the reference's chiral gamma matrices (spinor.cpp:191-264), acting on the spin index
+_I = 1j
+GAMMA = np.array([
+    [[0, 0, -1, 0], [0, 0, 0, -1], [-1, 0, 0, 0], [0, -1, 0, 0]],
+    [[0, 0, 0, -_I], [0, 0, -_I, 0], [0, _I, 0, 0], [_I, 0, 0, 0]],
+    [[0, 0, 0, -1], [0, 0, 1, 0], [0, 1, 0, 0], [-1, 0, 0, 0]],
+    [[0, 0, -_I, 0], [0, 0, 0, _I], [_I, 0, 0, 0], [0, -_I, 0, 0]],
+], dtype=complex)
+
+
+def hopping_start(shapes, mass, rng, noise=0.0):
+    """Weights of the first-order hopping expansion of the Schur inverse, an exact network of
+    three layers: with the Wilson hop H = -1/2 sum_mu [(1 - g_mu) U_mu(x) T+ + (1 + g_mu) U_mu(x-mu)^dag T-]
+    (dirac.cpp:258-697) and D-hat = A_ee - H A_oo^-1 H ~ (4+m) (1 - H^2 / (4+m)^2),
+        D-hat^-1 ~ (1 / (4+m)) (1 + H_eo H_oe / (4+m)^2):
+    layer 1 puts H psi in channel 0 and psi in channel 1, layer 2 applies H to channel 0 and
+    passes channel 1, the last layer adds them with the weights above.  Other weights start at
+    `noise` times Gaussian numbers."""
+    if len(shapes) != 3:
+        raise ValueError("the hopping start is a three-layer network")
+    k = 4.0 + mass
+    Ws = []
+    for shp in shapes:
+        W = noise * (rng.standard_normal(shp) + 1j * rng.standard_normal(shp)) / np.sqrt(2 * 9 * 4 * shp[2])
+        Ws.append(W)
+    one = np.eye(4, dtype=complex)
+    for l in (0, 1):
+        for mu in range(4):
+            Ws[l][1 + mu, 0, 0] = -0.5 * (one - GAMMA[mu])
+            Ws[l][5 + mu, 0, 0] = -0.5 * (one + GAMMA[mu])
+    Ws[0][0, 1, 0] = one
+    Ws[1][0, 1, 1] = one
+    Ws[2][0, 0, 1] = one / k
+    Ws[2][0, 0, 0] = one / k ** 3
+    return Ws
+
+
 def near_identity(shapes, rng, noise=0.02):
     Ws = []
     for shp in shapes:
@@ -80,6 +117,52 @@ class Adam:
             vh = v / (1 - self.b2 ** self.t)
             out.append(W - self.lr * mh / (np.sqrt(vh) + self.eps))
         return out
+
+
+class ResidualLoss:
+    """L(v) = |D-hat N(v) - v|^2 / |v|^2: the network as a right preconditioner, D-hat N close to
+    the identity.  Its gradient with respect to conj(N(v)) is D-hat^dag (D-hat N(v) - v) / |v|^2
+    with D-hat^dag = gamma5 D-hat gamma5 (Hphi = gamma5 D-hat is Hermitian)."""
+
+    def __init__(self, lat, mass):
+        self.lat, self.mass = lat, mass
+        self.y, self.s, self.w, self.t = lat.field(), lat.field(), lat.field(), lat.field()
+
+    def __call__(self, net, v):
+        lat, m = self.lat, self.mass
+        net.apply(self.y, v)
+        lat.spinor_copy(self.s, self.y)
+        lat.Dphi(m, self.w, self.s)
+        lat.spinor_sub_assign(self.w, v)                 # d = D N v - v
+        nv = lat.spinor_sqnorm(v)
+        loss = lat.spinor_sqnorm(self.w) / nv
+        lat.spinor_g5(self.w)
+        lat.Dphi(m, self.t, self.w)
+        lat.spinor_g5(self.t)
+        lat.spinor_mulr_assign(self.t, 1.0 / nv)        # gout = D^dag d / |v|^2
+        return loss, net.backward(v, self.t)
+
+
+def train_residual(net, lat, mass, vectors, steps=200, lr=5e-3, batch=4, rng=None, log=None):
+    """Adam on the right-preconditioner loss over mini-batches of source vectors."""
+    rng = rng or np.random.default_rng(0)
+    lossf = ResidualLoss(lat, mass)
+    Ws = net.get_weights()
+    opt = Adam(Ws, lr=lr)
+    hist = []
+    for s in range(steps):
+        idx = rng.choice(len(vectors), size=min(batch, len(vectors)), replace=False)
+        tot, gsum = 0.0, None
+        for i in idx:
+            l, g = lossf(net, vectors[i])
+            tot += l
+            gsum = g if gsum is None else [a + b for a, b in zip(gsum, g)]
+        Ws = opt.step(Ws, gsum)
+        net.set_weights(Ws)
+        hist.append(tot / len(idx))
+        if log is not None and (s % max(1, steps // 10) == 0 or s == steps - 1):
+            log(f"step {s}: loss {hist[-1]:.4f}")
+    return hist
 
 
 def train(net, pairs, steps=100, lr=2e-3, batch=4, rng=None, log=None):
