@@ -84,6 +84,13 @@ def parse():
                     help="configuration 2: Nf=2 HMC + Hasenbusch trajectories on 16^3x32 through YaHMC's own hmc "
                          "program built on the engine, FP64 and mixed-precision solvers (not the bench line)")
     ap.add_argument("--hmc-trajectories", type=int, default=4)
+    ap.add_argument("--rhmc", action="store_true",
+                    help="configuration 4(i): order-12 rational approximation via one multishift solve and the "
+                         "batched pole force, SU(2) adjoint 48x24^3 (not the bench line)")
+    ap.add_argument("--learned", action="store_true",
+                    help="configuration 5: learned preconditioner trained on 48x24^3, deployed on 64x32^3 "
+                         "(not the bench line)")
+    ap.add_argument("--train-steps", type=int, default=100)
     ap.add_argument("--contract-only", action="store_true",
                     help="with --mesons: only the contraction, on random propagators (for profiling)")
     return ap.parse_args()
@@ -602,6 +609,186 @@ def run_hmc(a):
     print(json.dumps(res))
 
 
+def run_rhmc(a):
+    """Configuration 4(i): the RHMC force and action pieces for Nf = 1 in the SU(2) adjoint
+    representation on 24^3x48 (even-odd clover, m = -0.2): the order-12 rational approximation
+    of x^(-1/2) from the reference's table, rescaled to the spectral bound 8
+    (yahmc_b200/data/rational_order12.json).  Timed with CUDA events: rational_calc (one 12-shift
+    cg_mshift, rational.cpp:134-166) against the 12 shifted systems solved one at a time, and
+    the pole loop of MonomialRHMC::update (rhmc.cpp:100-103) as one batched force against 12
+    separate wilson_fermion_force_q calls.  The field: 40 pure-gauge HMC trajectories of SU(2)
+    at beta 2.2 on 24^3x48 (the engine's molecular-dynamics kernels)."""
+    import torch
+    import yahmc_b200 as yg
+    from yahmc_b200 import fields
+    from yahmc_b200 import thermalize as th
+    torch.cuda.set_device(0)
+    yg.set_device(0)
+    with open(os.path.join(ROOT, "yahmc_b200", "data", "rational_order12.json")) as f:
+        ra = json.load(f)
+    dims = (48, 24, 24, 24)
+    mass, prec = -0.2, 1e-20
+    lat = yg.Lattice(dims, nc=2, repr="adjoint", bc="antiperiodic", clover=True, eo=True, csw=CSW)
+    gl = yg.Lattice(dims, nc=2, repr="fundamental", bc="periodic", clover=False, eo=True)
+    gl.set_links(np.broadcast_to(np.eye(2, dtype=complex), (gl.V, 4, 2, 2)).copy())
+    hist = th.thermalize(gl, 2.2, 40, steps=40, length=1.0, c0=1.0, seed=a.seed, integrator="o2mn", n_warm=10)
+    lat.set_links(gl.get_links())
+    plaq = float(hist[-1][2])
+    del gl
+    rng = np.random.default_rng(a.seed)
+    b = lat.field(fields.gaussian_spinor(lat.V, lat.d, rng))
+    poles, res = ra["poles"], ra["residues"]
+    n = len(poles)
+
+    def ev(fn, k=1):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = [fn() for _ in range(k)]
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k, out[-1]
+
+    x = lat.field()
+    calc = lambda: lat.rational_calc("Hphi_sq", mass, prec, ra["a0"], poles, res, x, b)
+    calc()
+    ms_calc, it_calc = ev(calc, 2)
+    xs = [lat.field() for _ in range(n)]
+
+    def one_by_one():
+        its = 0
+        for p_, xi in zip(poles, xs):
+            its += lat.cg_mshift("Hphi_sq", mass, prec, [p_], [xi], b)
+        return its
+
+    one_by_one()
+    ms_sep, it_sep = ev(one_by_one, 1)
+    # the same combination from the separate solves: a0 b + sum r_i x_i
+    xc = lat.field()
+    lat.spinor_mulr(xc, ra["a0"], b)
+    for r_, xi in zip(res, xs):
+        lat.spinor_mulr_add_assign(xc, r_, xi)
+    lat.spinor_sub_assign(xc, x)
+    diff = (lat.spinor_sqnorm(xc) / lat.spinor_sqnorm(x)) ** 0.5
+    # the force of all poles: batched against one pole at a time, from the same solutions
+    ms_xs = lat.cg_mshift("Hphi_sq", mass, prec, poles, xs, b)
+    srcs = [lat.download(xi) for xi in xs]
+    fields_b = [lat.field(s_) for s_ in srcs]
+    lat.zero_momenta()
+    lat.begin_fermion_force()
+
+    # the force writes the odd half of each field from its even half and reads only the even
+    # half otherwise, so repeated calls on the same fields give the same force
+    def batched():
+        lat.wilson_fermion_force_q_multi(0.1, mass, res, fields_b)
+
+    def separate():
+        for r_, f_ in zip(res, fields_b):
+            lat.wilson_fermion_force_q(0.1, mass, r_, f_)
+
+    batched()
+    lat.zero_momenta()
+    ms_fb, _ = ev(batched, 3)
+    mom_b = lat.momenta()
+    lat.zero_momenta()
+    lat.begin_fermion_force()
+    separate()
+    lat.zero_momenta()
+    ms_fs, _ = ev(separate, 3)
+    mom_s = lat.momenta()
+    print(json.dumps({
+        "workload": "RHMC Nf=1 pieces, SU(2) adjoint 48x24x24x24 even-odd clover, m = -0.2, order-12 x^(-1/2) "
+                    "rational approximation from the reference's table (valid on "
+                    f"[{ra['valid_interval'][0]:.3g}, {ra['valid_interval'][1]:.3g}])",
+        "links": f"40 pure-gauge HMC trajectories at beta 2.2, plaquette {plaq:.5f}",
+        "rational_calc": {"one_mshift_ms": ms_calc, "iterations": it_calc, "shifts_one_at_a_time_ms": ms_sep,
+                          "iterations_one_at_a_time": it_sep, "speedup": ms_sep / ms_calc,
+                          "rel_diff_of_results": diff, "prec_squared": prec},
+        "pole_force": {"batched_ms": ms_fb, "one_at_a_time_ms": ms_fs, "speedup": ms_fs / ms_fb,
+                       "max_rel_diff_momenta": float(np.abs(mom_b - mom_s).max() / np.abs(mom_s).max()),
+                       "poles": n, "mshift_iterations": ms_xs}}))
+
+
+def run_learned(a):
+    """Configuration 5: the learned preconditioner.  Trained on a 24^3x48 SU(3) field (beta 5.6
+    heatbath field tiled from 8^4, m = -0.78): the network starts from the first-order hopping
+    expansion of the Schur inverse and is trained on CG errors of that lattice's own solves;
+    deployed on 32^3x64 (another heatbath field, same beta and mass).  Hphi_sq x = b to true
+    relative residual 1e-12 three ways: the plain even-odd CG (FP64), the learned solve (two
+    flexible-GCR Dphi solves with the network as right preconditioner, the FP64 CG finishing
+    if needed), and the same without the network (plain GCR) for the ablation."""
+    import torch
+    import yahmc_b200 as yg
+    from yahmc_b200 import Ptc, fields, learned
+    torch.cuda.set_device(0)
+    yg.set_device(0)
+    mass, prec, C = -0.78, PREC, 8
+    out = {"workload": "learned preconditioner: train 48x24x24x24, deploy 64x32x32x32, SU(3) fund even-odd "
+                       "Wilson-clover, m = -0.78, Hphi_sq to true rel. residual 1e-12", "channels": [1, C, C, 1]}
+    tdims, ddims = (48, 24, 24, 24), (64, 32, 32, 32)
+    U, plaq = bench_field(tdims, a.seed + 5)
+    lt = yg.Lattice(tdims, nc=3, repr="fundamental", bc="antiperiodic", clover=True, eo=True, csw=CSW)
+    lt.set_links(U)
+    del U
+    rng = np.random.default_rng(a.seed)
+    net = Ptc(lt, (1, C, C, 1))
+    net.set_weights(learned.hopping_start(net.shapes(), mass, rng))
+    t0 = time.perf_counter()
+    pairs = learned.training_pairs(lt, mass, 2, rng, stops=(25, 50, 100, 200), prec=1e-16, random_pairs=2)
+    t1 = time.perf_counter()
+    hist = learned.train(net, pairs, steps=a.train_steps, lr=1e-4, batch=4, rng=rng)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    out["training"] = {"pairs": len(pairs), "pair_generation_s": t1 - t0, "steps": a.train_steps, "train_s": t2 - t1,
+                       "loss_first10": float(np.mean(hist[:10])), "loss_last10": float(np.mean(hist[-10:])),
+                       "train_links_plaquette": plaq}
+    Ws = net.get_weights()
+    del net, pairs, lt
+    U, plaq2 = bench_field(ddims, a.seed + 6)
+    ld = yg.Lattice(ddims, nc=3, repr="fundamental", bc="antiperiodic", clover=True, eo=True, csw=CSW)
+    ld.set_links(U)
+    del U
+    dnet = Ptc(ld, (1, C, C, 1))
+    dnet.set_weights(Ws)
+    b = ld.field(fields.gaussian_spinor(ld.V, 3, rng))
+
+    def ev(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), r
+
+    def true_res(x):
+        xc, r = ld.field(), ld.field()
+        ld.spinor_copy(xc, x)
+        ld.Hphi_sq(mass, r, xc)
+        ld.spinor_sub_assign(r, b)
+        return ld.spinor_sqnorm(r) / ld.spinor_sqnorm(b)
+
+    x = ld.field()
+    ms, it = ev(lambda: ld.cg_inverter("Hphi_sq", mass, prec, x, b))
+    out["plain_eo_cg_fp64"] = {"ms": ms, "iterations": it, "true_residual": true_res(x)}
+    x = ld.field()
+    ms, st = ev(lambda: ld.solve_learned(mass, prec, x, b, net=dnet))
+    out["learned_fgcr"] = {"ms": ms, "gcr_iterations": st["iterations"], "fallback": st["fallback"],
+                           "true_residual": true_res(x)}
+    x = ld.field()
+    ms, st = ev(lambda: ld.solve_learned(mass, prec, x, b, net=None))
+    out["plain_gcr_no_network"] = {"ms": ms, "gcr_iterations": st["iterations"], "fallback": st["fallback"],
+                                   "true_residual": true_res(x)}
+    x = ld.field()
+    ms, st = ev(lambda: ld.cg_mixed("Hphi_sq", mass, prec, x, b))
+    out["mixed_cg"] = {"ms": ms, "iterations": st["iterations"], "true_residual": true_res(x)}
+    out["deploy_links_plaquette"] = plaq2
+    y = ld.field()
+    ms, _ = ev(lambda: [dnet.apply(y, b) for _ in range(10)])
+    out["network_apply_ms"] = ms / 10
+    print(json.dumps(out))
+
+
 def run_lattices(a):
     """FP64 CG (Hphi_sq, m = -0.6, prec 1e-20) on SU(3) fundamental 8^4, 12^4 and 16^4 lattices
     with thermalised-like fields from the engine's own HMC (20 trajectories each): the three
@@ -889,6 +1076,10 @@ def main():
             run_lattices(a)
         elif a.hmc:
             run_hmc(a)
+        elif a.rhmc:
+            run_rhmc(a)
+        elif a.learned:
+            run_learned(a)
         elif a.mshift:
             run_mshift(a)
         elif a.impl == "reference":

@@ -55,6 +55,10 @@ double hamiltonian();
 void reunitarize();
 void reset_variables();
 #include <integrator.h>
+#include <approx.h>
+/* defined in library/rational.cpp without a header declaration */
+double residue(rational_app &data, int n);
+void rescale(rational_app &data, double max);
 
 static int harness_ready = 0;
 
@@ -513,5 +517,65 @@ void yref_hmc_update(double length) { update(length); }
 void yref_hmc_counters(int *out) { out[0] = num_cnfg; out[1] = num_accept; }
 void yref_gauge_backup(void) { gauge_field_backup(); }
 void yref_gauge_restore(void) { gauge_field_restore(); }
+
+/* A rational approximation of a chosen order from the reference's table (include/approx.h):
+ * among the entries for x^(|n|/|d|) of that order, the one with the widest interval; then the
+ * steps of rational_find after its choice (rational.cpp:101-131): roots and poles swapped for
+ * a positive power, rescale(max), the partial-fraction residues.  out: order, a0, prec, min,
+ * max, then order poles and order residues.  Returns -1 if the table has no such entry. */
+int yref_rational_order(int n, int d, int order, double max, double *out)
+{
+	int sz = sizeof(appdb)/sizeof(double);
+	int bi = -1, to = 0;
+	double best = 0;
+	for(int i = 0; i < sz; i += 7+2*to)
+	{
+		int tn = appdb[i+0], td = appdb[i+1];
+		to = appdb[i+2];
+		double ratio = appdb[i+4] / appdb[i+5];
+		if(tn == abs(n) && td == abs(d) && to == order && (bi < 0 || ratio < best))
+		{
+			bi = i;
+			best = ratio;
+		}
+	}
+	if(bi < 0) return -1;
+	rational_app data;
+	data.n = n;
+	data.d = d;
+	data.order = order;
+	data.prec = appdb[bi+3];
+	data.min = appdb[bi+4];
+	data.max = appdb[bi+5];
+	data.a0 = appdb[bi+6];
+	for(int i = 0; i < order; i++)
+	{
+		data.root[i] = appdb[7+bi+i];
+		data.pole[i] = appdb[7+bi+order+i];
+	}
+	if(d*n > 0)
+	{
+		for(int i = 0; i < order; i++)
+		{
+			double r = data.root[i];
+			data.root[i] = data.pole[i];
+			data.pole[i] = r;
+		}
+		data.a0 = 1.0 / data.a0;
+	}
+	rescale(data, max);
+	for(int i = 0; i < order; i++) data.residue[i] = residue(data, i);
+	out[0] = order;
+	out[1] = data.a0;
+	out[2] = data.prec;
+	out[3] = data.min;
+	out[4] = data.max;
+	for(int i = 0; i < order; i++)
+	{
+		out[5+i] = data.pole[i];
+		out[5+order+i] = data.residue[i];
+	}
+	return 0;
+}
 
 }

@@ -107,7 +107,7 @@ struct Lattice {
   int mr_cap = 0;
   DevBuf mr_scal, mr_part;
   double *mr_hist = nullptr;
-  int mr_tile[17] = {};   // measured systems-per-thread tile of the inner operator, per system count
+  int mr_tile[17] = {};   // measured inner-operator variant (tile, threads per site) + 1, per system count
 
   long field_doubles() const { return 8L * d * V; }
   size_t field_bytes() const { return sizeof(double) * field_doubles(); }

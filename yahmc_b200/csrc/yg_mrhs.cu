@@ -21,6 +21,7 @@
 #include <cuda_fp16.h>
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -35,7 +36,6 @@ namespace yg {
 namespace {
 
 constexpr int kMR = 16;       // systems per call (kMaxRhs of the batched solvers)
-constexpr int kTiles[3] = {1, 2, 4};   // systems per thread in the inner operator (autotuned)
 constexpr int kHopThreads = 128;
 constexpr int kVecThreads = 256;
 
@@ -164,40 +164,63 @@ __device__ __forceinline__ void herm_block(float2 (&y)[6], const float4 *C, int 
 // resident blocks per SM the register budget is cut for: 6 (R = 1), 4 (R = 2), 3 (R = 4)
 template <int R> struct MinBlocks { static constexpr int value = R == 1 ? 6 : R == 2 ? 4 : 3; };
 
-template <int K, int R, int STEP, int NRM>
+// SPLIT = 2: two neighbouring threads share a site, one taking the directions mu = 0, 1 and the
+// other mu = 2, 3; their accumulators are added with one shuffle per word and each then finishes
+// half of the tile's systems.  Twice the threads per site hide the latency of the gathers of a
+// register-heavy tile.
+template <int K, int R, int STEP, int NRM, int SPLIT>
 __global__ void __launch_bounds__(kHopThreads, MinBlocks<R>::value) k_mhop(MHopArgs a) {
+  constexpr int SITES = kHopThreads / SPLIT;              // sites per block
   const int tile = blockIdx.x % a.ntile, sb = blockIdx.x / a.ntile;
   const int s0 = tile * R;
   const int rc = min(R, a.nsys - s0);
-  const int t = sb * kHopThreads + threadIdx.x;
+  const int part = SPLIT == 2 ? (threadIdx.x & 1) : 0;
+  const int t = sb * SITES + threadIdx.x / SPLIT;
   const Geom &g = a.g;
   float n2[R];
 #pragma unroll
   for (int r = 0; r < R; r++) n2[r] = 0.f;
-  if (t < a.n) {
-    const int id = a.lo + t;
-    SiteNbr nb;
-    site_nbr(nb, g, id);
-    const int T = g.dim[0], t0 = nb.c[0];
-    float2 acc[R][12];
+  const bool live = t < a.n;
+  const int id = a.lo + (live ? t : 0);
+  SiteNbr nb;
+  site_nbr(nb, g, id);
+  const int T = g.dim[0], t0 = nb.c[0];
+  float2 acc[R][12];
+#pragma unroll
+  for (int r = 0; r < R; r++)
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc[r][k] = make_float2(0.f, 0.f);
+  if (live) {
+    if (SPLIT == 1 || part == 0) {
+      mhop_dir<K, R, 0, -1>(acc, a, s0, rc, nb.f[0], id, t0);
+      mhop_dir<K, R, 0, +1>(acc, a, s0, rc, nb.b[0], nb.b[0], t0 == 0 ? T - 1 : t0 - 1);
+      mhop_dir<K, R, 1, -1>(acc, a, s0, rc, nb.f[1], id, t0);
+      mhop_dir<K, R, 1, +1>(acc, a, s0, rc, nb.b[1], nb.b[1], t0);
+    }
+    if (SPLIT == 1 || part == 1) {
+      mhop_dir<K, R, 2, -1>(acc, a, s0, rc, nb.f[2], id, t0);
+      mhop_dir<K, R, 2, +1>(acc, a, s0, rc, nb.b[2], nb.b[2], t0);
+      mhop_dir<K, R, 3, -1>(acc, a, s0, rc, nb.f[3], id, t0);
+      mhop_dir<K, R, 3, +1>(acc, a, s0, rc, nb.b[3], nb.b[3], t0);
+    }
+  }
+  if (SPLIT == 2) {
+    // every lane takes part (the pair of a dead site holds zeros)
 #pragma unroll
     for (int r = 0; r < R; r++)
 #pragma unroll
-      for (int k = 0; k < 12; k++) acc[r][k] = make_float2(0.f, 0.f);
-    mhop_dir<K, R, 0, -1>(acc, a, s0, rc, nb.f[0], id, t0);
-    mhop_dir<K, R, 0, +1>(acc, a, s0, rc, nb.b[0], nb.b[0], t0 == 0 ? T - 1 : t0 - 1);
-    mhop_dir<K, R, 1, -1>(acc, a, s0, rc, nb.f[1], id, t0);
-    mhop_dir<K, R, 1, +1>(acc, a, s0, rc, nb.b[1], nb.b[1], t0);
-    mhop_dir<K, R, 2, -1>(acc, a, s0, rc, nb.f[2], id, t0);
-    mhop_dir<K, R, 2, +1>(acc, a, s0, rc, nb.b[2], nb.b[2], t0);
-    mhop_dir<K, R, 3, -1>(acc, a, s0, rc, nb.f[3], id, t0);
-    mhop_dir<K, R, 3, +1>(acc, a, s0, rc, nb.b[3], nb.b[3], t0);
+      for (int k = 0; k < 12; k++) {
+        acc[r][k].x += __shfl_xor_sync(0xffffffffu, acc[r][k].x, 1);
+        acc[r][k].y += __shfl_xor_sync(0xffffffffu, acc[r][k].y, 1);
+      }
+  }
+  if (live) {
     const int blk = id >= g.Vh, h = id - blk * g.Vh;
     const bool bnd = spinor_zeroed(g, t0);
     const float4 *C = reinterpret_cast<const float4 *>(a.C);
 #pragma unroll
     for (int r = 0; r < R; r++) {
-      if (r < rc) {
+      if (r < rc && (SPLIT == 1 || (r & 1) == part)) {
         float2 in[12], out[12];
         if (STEP == 1) {
 #pragma unroll
@@ -220,7 +243,7 @@ __global__ void __launch_bounds__(kHopThreads, MinBlocks<R>::value) k_mhop(MHopA
             out[(2 * b + 1) * 3 + i] = y[i + 3];
           }
         }
-        float s = 0.f;
+        float sq = 0.f;
 #pragma unroll
         for (int k = 0; k < 12; k++) {
           if (STEP == 2) {
@@ -228,9 +251,9 @@ __global__ void __launch_bounds__(kHopThreads, MinBlocks<R>::value) k_mhop(MHopA
             if (k >= 6) out[k] = cscale(out[k], -1.f);      // gamma5
           }
           if (bnd) out[k] = make_float2(0.f, 0.f);
-          s = fmaf(out[k].x, out[k].x, fmaf(out[k].y, out[k].y, s));
+          sq = fmaf(out[k].x, out[k].x, fmaf(out[k].y, out[k].y, sq));
         }
-        n2[r] = s;
+        n2[r] = sq;
         sstore<16>(a.dst.d[s0 + r], a.dst.n[s0 + r], out, blk, h, g.Vh);
       }
     }
@@ -396,27 +419,37 @@ SysBufs sys_bufs(Lattice &L, int i) {
 
 int vec_grid(int sms) { return sms * 4; }
 
-// the two Schur steps of the inner operator for a launch's systems, R systems per thread
-template <int K, int R>
-void launch_mhop_r(Lattice &L, const MHopArgs &a, const MHopArgs &b, bool nrm, int nsb) {
-  const int grid = a.ntile * nsb;
-  k_mhop<K, R, 1, 0><<<grid, kHopThreads, 0, L.stream>>>(a);
+// the two Schur steps of the inner operator for a launch's systems, R systems per thread,
+// SPLIT threads per site
+template <int K, int R, int SPLIT>
+void launch_mhop_r(Lattice &L, const MHopArgs &a0, const MHopArgs &b0, bool nrm) {
+  MHopArgs a = a0, b = b0;
+  a.nsb = b.nsb = nblk(a.n, kHopThreads / SPLIT);
+  const int grid = a.ntile * a.nsb;
+  k_mhop<K, R, 1, 0, SPLIT><<<grid, kHopThreads, 0, L.stream>>>(a);
   YG_LAUNCHED();
-  if (nrm) k_mhop<K, R, 2, 1><<<grid, kHopThreads, 0, L.stream>>>(b);
-  else k_mhop<K, R, 2, 0><<<grid, kHopThreads, 0, L.stream>>>(b);
+  if (nrm) k_mhop<K, R, 2, 1, SPLIT><<<grid, kHopThreads, 0, L.stream>>>(b);
+  else k_mhop<K, R, 2, 0, SPLIT><<<grid, kHopThreads, 0, L.stream>>>(b);
   YG_LAUNCHED();
 }
 
-void launch_mhop(Lattice &L, int reals, int tile, const MHopArgs &a, const MHopArgs &b, bool nrm, int nsb) {
-  if (reals == 12) {
-    if (tile == 1) launch_mhop_r<6, 1>(L, a, b, nrm, nsb);
-    else if (tile == 2) launch_mhop_r<6, 2>(L, a, b, nrm, nsb);
-    else launch_mhop_r<6, 4>(L, a, b, nrm, nsb);
-  } else {
-    if (tile == 1) launch_mhop_r<9, 1>(L, a, b, nrm, nsb);
-    else if (tile == 2) launch_mhop_r<9, 2>(L, a, b, nrm, nsb);
-    else launch_mhop_r<9, 4>(L, a, b, nrm, nsb);
+// the inner-operator variants the tuner chooses among: (systems per thread, threads per site)
+constexpr int kVariants[5][2] = {{1, 1}, {2, 1}, {4, 1}, {2, 2}, {4, 2}};
+
+template <int K>
+void launch_mhop_k(Lattice &L, int var, const MHopArgs &a, const MHopArgs &b, bool nrm) {
+  switch (var) {
+    case 0: launch_mhop_r<K, 1, 1>(L, a, b, nrm); break;
+    case 1: launch_mhop_r<K, 2, 1>(L, a, b, nrm); break;
+    case 2: launch_mhop_r<K, 4, 1>(L, a, b, nrm); break;
+    case 3: launch_mhop_r<K, 2, 2>(L, a, b, nrm); break;
+    default: launch_mhop_r<K, 4, 2>(L, a, b, nrm); break;
   }
+}
+
+void launch_mhop(Lattice &L, int reals, int var, const MHopArgs &a, const MHopArgs &b, bool nrm) {
+  if (reals == 12) launch_mhop_k<6>(L, var, a, b, nrm);
+  else launch_mhop_k<9>(L, var, a, b, nrm);
 }
 
 }  // namespace
@@ -445,7 +478,7 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
   YG_CUDA(cudaGetDevice(&dev));
   YG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const int Vh = (int)L.Vh;
-  const int nsb = nblk(Vh, kHopThreads);
+  const int nsb_max = nblk(Vh, kHopThreads / 2);  // partials per system, most for two threads a site
   const int gv = std::min(vec_grid(sms), nblk(Vh, kVecThreads));
   if (L.mr_cap < nb) {
     L.mr_work.release();
@@ -458,7 +491,7 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
     L.mr_scal.alloc(sizeof(double) * kMR * kW);
     YG_CUDA(cudaMemsetAsync(L.mr_scal.p, 0, sizeof(double) * kMR * kW, L.stream));
   }
-  const size_t part_words = (size_t)kMR * std::max(nsb, gv);
+  const size_t part_words = (size_t)kMR * std::max(nsb_max, gv);
   if (L.mr_part.bytes < 2 * part_words * sizeof(double)) {
     L.mr_part.release();
     L.mr_part.alloc(2 * part_words * sizeof(double));
@@ -517,15 +550,15 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
       v.sys[j] = act[j];
     }
   };
-  int tile = 4;
+  int var = 2;                                // index into kVariants
   auto hphi = [&](bool nrm, bool second) {   // t = Hphi p (first) or q = Hphi t (second), o the odd sites
     MHopArgs a{};
     a.g = L.g;
     a.U = L.sl_links.p;
     a.C = L.sl_clover.p;
     a.nsys = (int)act.size();
+    const int tile = kVariants[var][0];
     a.ntile = (a.nsys + tile - 1) / tile;
-    a.nsb = nsb;
     a.part = part_pq;
     MHopArgs b = a;
     for (int j = 0; j < a.nsys; j++) {
@@ -539,7 +572,7 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
     }
     a.coeff = 0.5f; a.lo = Vh; a.n = Vh;
     b.coeff = -0.5f; b.lo = 0; b.n = Vh;
-    launch_mhop(L, reals, tile, a, b, nrm, nsb);
+    launch_mhop(L, reals, var, a, b, nrm);
     L.mvm += 2 * a.nsys;
   };
   auto wait_iteration = [&](unsigned long long k) {
@@ -572,10 +605,11 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
       YG_CUDA(cudaEventCreate(&e0));
       YG_CUDA(cudaEventCreate(&e1));
       float best_ms = 0.f;
-      int best_tile = 4, calls = 0;
-      for (int cand : kTiles) {
-        if (cand > 1 && cand >= 2 * ns) continue;
-        tile = cand;
+      int best = 2, calls = 0;
+      for (int cand = 0; cand < 5; cand++) {
+        const int r = kVariants[cand][0];
+        if (r > 1 && r >= 2 * ns) continue;
+        var = cand;
         calls += 4;
         hphi(false, false);                      // warm-up; t only (p untouched)
         YG_CUDA(cudaEventRecord(e0, L.stream));
@@ -584,14 +618,17 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
         YG_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
         YG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        if (best_ms == 0.f || ms < best_ms) { best_ms = ms; best_tile = cand; }
+        if (best_ms == 0.f || ms < best_ms) { best_ms = ms; best = cand; }
+        if (std::getenv("YG_TUNE_LOG"))
+          std::fprintf(stderr, "yg tune cg_mixed_multi: %d systems, %d per thread, %d-way direction split: %.3f ms/Hphi\n",
+                       ns, r, kVariants[cand][1], ms / 3.f);
       }
       YG_CUDA(cudaEventDestroy(e0));
       YG_CUDA(cudaEventDestroy(e1));
       L.mvm -= 2 * ns * calls;                   // the timing launches are not MVMs of the solve
-      L.mr_tile[ns] = best_tile;
+      L.mr_tile[ns] = best + 1;
     }
-    tile = L.mr_tile[ns];
+    var = L.mr_tile[ns] - 1;
   }
   const double d2 = delta * delta;
   constexpr int kStagnate = 100;   // as the single-system solver: force an update after 100 flat iterations
@@ -607,7 +644,7 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
     MVec v{};
     fill(v);
     hphi(true, false);
-    k_m_alpha<<<1, 32 * v.nsys, 0, L.stream>>>(scal, part_pq, nsb, v, parity);
+    k_m_alpha<<<1, 32 * v.nsys, 0, L.stream>>>(scal, part_pq, nblk(Vh, kHopThreads / kVariants[var][1]), v, parity);
     YG_LAUNCHED();
     hphi(false, true);
     k_m_update<<<dim3(gv, v.nsys), kVecThreads, 0, L.stream>>>(scal, part_r, v, Vh);
