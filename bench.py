@@ -91,6 +91,10 @@ def parse():
                     help="configuration 5: learned preconditioner trained on 48x24^3, deployed on 64x32^3 "
                          "(not the bench line)")
     ap.add_argument("--train-steps", type=int, default=100)
+    ap.add_argument("--train-dims", type=int, nargs=4, default=[48, 24, 24, 24],
+                    help="lattice of the learned preconditioner's training (T X Y Z)")
+    ap.add_argument("--deploy-dims", type=int, nargs=4, default=[64, 32, 32, 32],
+                    help="lattice the trained preconditioner is deployed on (T X Y Z)")
     ap.add_argument("--contract-only", action="store_true",
                     help="with --mesons: only the contraction, on random propagators (for profiling)")
     return ap.parse_args()
@@ -594,14 +598,19 @@ def run_hmc(a):
                        "on the engine", "start": f"20 pure-gauge trajectories from the random start, plaquette "
                        f"{therm['plaquette'][-1]:.6f}", "thermalisation_s": therm["wall_s"]}
     for solver, env in (("fp64", None), ("mixed", {"YAHMC_GPU_SOLVER": "mixed"})):
-        r = run(exe, HMC_CFG.format(seed=seed + 1, prefix="nf2", start=start, last=n, freq=0, **dims) + NF2,
+        # the program counts configurations from the start file's number (hmc.cpp:148): last is absolute
+        r = run(exe, HMC_CFG.format(seed=seed + 1, prefix="nf2", start=start, last=20 + n, freq=0, **dims) + NF2,
                 f"nf2_{solver}", env)
+        if len(r["seconds"]) != n:
+            raise RuntimeError(f"nf2_{solver}: {len(r['seconds'])} trajectories in the log, expected {n}")
         dh = np.array(r["dH"])
         res[solver] = {"trajectory_s": r["seconds"], "mean_trajectory_s": float(np.mean(r["seconds"])),
                        "mvm": r["mvm"], "dH": r["dH"], "exp_minus_dH_mean": float(np.mean(np.exp(-dh))),
                        "acceptance": float(np.mean(r["accepted"])), "plaquette": r["plaquette"]}
     if os.path.exists(cpu_exe) and not a.no_cpu_baseline:
-        r = run(cpu_exe, HMC_CFG.format(seed=seed + 1, prefix="cpu", start=start, last=1, freq=0, **dims) + NF2, "cpu")
+        r = run(cpu_exe, HMC_CFG.format(seed=seed + 1, prefix="cpu", start=start, last=21, freq=0, **dims) + NF2, "cpu")
+        if len(r["seconds"]) != 1:
+            raise RuntimeError("cpu: no trajectory in the log")
         res["cpu_reference"] = {"trajectory_s": r["seconds"], "mvm": r["mvm"], "dH": r["dH"],
                                 "threads": os.cpu_count(), "plaquette": r["plaquette"]}
         res["speedup_fp64_vs_cpu"] = r["seconds"][0] / res["fp64"]["trajectory_s"][0]
@@ -723,9 +732,10 @@ def run_learned(a):
     torch.cuda.set_device(0)
     yg.set_device(0)
     mass, prec, C = -0.78, PREC, 8
-    out = {"workload": "learned preconditioner: train 48x24x24x24, deploy 64x32x32x32, SU(3) fund even-odd "
-                       "Wilson-clover, m = -0.78, Hphi_sq to true rel. residual 1e-12", "channels": [1, C, C, 1]}
-    tdims, ddims = (48, 24, 24, 24), (64, 32, 32, 32)
+    tdims, ddims = tuple(a.train_dims), tuple(a.deploy_dims)
+    out = {"workload": f"learned preconditioner: train {'x'.join(map(str, tdims))}, deploy "
+                       f"{'x'.join(map(str, ddims))}, SU(3) fund even-odd Wilson-clover, m = -0.78, Hphi_sq to "
+                       "true rel. residual 1e-12", "channels": [1, C, C, 1]}
     U, plaq = bench_field(tdims, a.seed + 5)
     lt = yg.Lattice(tdims, nc=3, repr="fundamental", bc="antiperiodic", clover=True, eo=True, csw=CSW)
     lt.set_links(U)
@@ -814,10 +824,16 @@ def run_lattices(a):
             its.append(lat.cg_inverter("Hphi_sq", m, pr, x, b))
         return its
 
+    path = []
+
     def concurrent():
         for lat, m, pr, x, b in solves:
             lat.spinor_zero(x)
-        return yg.cg_inverter_lattices(solves)[0]
+        its, rc, p = yg.cg_inverter_lattices(solves, with_path=True)
+        if rc != 0:
+            raise RuntimeError(f"cg_inverter_lattices status {rc}")
+        path.append(p)
+        return its
 
     def timed(fn):
         fn()
@@ -833,6 +849,7 @@ def run_lattices(a):
     print(json.dumps({"workload": "FP64 CG on Hphi_sq, SU(3) fund even-odd Wilson-clover 8^4 + 12^4 + 16^4",
                       "sequential_ms": t_seq, "concurrent_ms": t_con, "speedup": t_seq / t_con,
                       "iterations": it_seq, "iterations_concurrent": it_con,
+                      "concurrent_path": "one persistent kernel" if path and path[-1] == 1 else "host threads",
                       "timing": "host wall clock around the solves, synchronised, mean of --steps"}))
 
 
@@ -883,13 +900,15 @@ def run_ours(a, rank, world, dist):
         def multi_only():
             for f in bx:
                 lat.spinor_zero(f)
-            return lat.cg_inverter_multi("Hphi_sq", MASS, PREC, bx, bsrc)
+            return lat.cg_mixed_multi("Hphi_sq", MASS, PREC, bx, bsrc, delta=0.1)
 
         for _ in range(max(1, a.warmup)):
             multi_only()
-        ms_b, its_b = timed(multi_only, a.steps)
+        ms_b, sts_b = timed(multi_only, a.steps)
         if rank == 0:
-            print(json.dumps({"batched_ms": ms_b, "nrhs": a.nrhs, "iterations": its_b[-1]}))
+            print(json.dumps({"batched_mixed_ms": ms_b, "nrhs": a.nrhs,
+                              "iterations": [st["iterations"] for st in sts_b[-1]],
+                              "worst_true_residual": max(st["true_residual"] for st in sts_b[-1])}))
         return
 
     # warm-up (W >= 3 solves), then the timed mixed-precision solves with clocks sampled
@@ -973,17 +992,44 @@ def run_ours(a, rank, world, dist):
         multi_mixed()
         ms_mm, sts_mm = timed(multi_mixed, 2)
         worst = max(st["true_residual"] for st in sts_mm[-1])
+
+        # the Hasenbusch pair: the Hphi_sq solves of the HMC monomial (m + dm) and of the
+        # Hasenbusch monomial (m) of one force evaluation, separately and in one call
+        pair = (MASS + 0.2, MASS)
+
+        def pair_separate():
+            out = []
+            for k, m in enumerate(pair):
+                lat.spinor_zero(bx[k])
+                out.append(lat.cg_mixed_multi("Hphi_sq", m, PREC, [bx[k]], [bsrc[k]], delta=0.1)[0])
+            return out
+
+        def pair_joint():
+            for k in range(2):
+                lat.spinor_zero(bx[k])
+            return lat.cg_mixed_multi("Hphi_sq", MASS, PREC, bx[:2], bsrc[:2], delta=0.1, masses=list(pair))
+
+        pair_separate()
+        ms_ps, sts_ps = timed(pair_separate, 2)
+        pair_joint()
+        ms_pj, sts_pj = timed(pair_joint, 2)
         batched = {"nrhs": a.nrhs,
                    "fp64": {"solver": "FP64 CG, all systems per operator launch", "ms_total": ms_multi,
                             "ms_per_rhs": ms_multi / a.nrhs, "iterations": its_multi[-1],
                             "speedup_per_rhs_vs_fp64_cg": ms_fp64 / (ms_multi / a.nrhs)},
-                   "mixed": {"solver": "FP32 inner (FP32 12-real links and clover) / FP64 reliable updates, all "
-                                       "systems per operator launch, true residual per system",
+                   "mixed": {"solver": "inner CG on FP16 spinors with per-site norms, FP32 12-real links and "
+                                       "packed clover, FP64 reliable updates; all systems per operator launch, "
+                                       "systems per thread chosen by the tuner; true residual per system",
                              "ms_total": ms_mm, "ms_per_rhs": ms_mm / a.nrhs,
                              "iterations": [st["iterations"] for st in sts_mm[-1]],
                              "reliable_updates": sts_mm[-1][0]["reliable_updates"],
                              "fallbacks": sum(st["fallback"] for st in sts_mm[-1]), "worst_true_residual": worst,
-                             "speedup_per_rhs_vs_fp64_cg": ms_fp64 / (ms_mm / a.nrhs)}}
+                             "speedup_per_rhs_vs_fp64_cg": ms_fp64 / (ms_mm / a.nrhs)},
+                   "hasenbusch_pair": {"masses": list(pair), "separate_ms": ms_ps, "one_call_ms": ms_pj,
+                                       "speedup": ms_ps / ms_pj,
+                                       "iterations": [st["iterations"] for st in sts_pj[-1]],
+                                       "true_residuals": [st["true_residual"] for st in sts_pj[-1]],
+                                       "fallbacks": sum(st["fallback"] for st in sts_pj[-1] + sts_ps[-1])}}
         del bsrc, bx
 
     variants = None

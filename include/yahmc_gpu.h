@@ -206,25 +206,42 @@ int yg_cg_mixed(yg_lattice *lat, const yg_inv_par *par, double *x, double *b, yg
 int yg_cg_inverter_multi(yg_lattice *lat, const yg_inv_par *par, int nrhs, double *const *xs, double *const *bs,
                          int *iters);
 /* No reference counterpart: n <= 64 independent cg_inverter solves, one per lattice (lattices of
- * any sizes and configurations, each at most once), run concurrently: a host thread and the
- * lattice's own stream per solve, so small lattices that leave the GPU mostly idle overlap.
- * Results and iteration counts are those of separate yg_cg_inverter calls; returns the worst
- * status.  The calling thread's current device is used for all of them. */
+ * any sizes and configurations, each at most once), run concurrently.  Hphi_sq solves on
+ * even-odd lattices of one representation dimension d (2, 3, 4 or 6), all with or all without
+ * a clover term and without open/SF boundaries, run as ONE persistent cooperative kernel: a
+ * group of blocks per lattice, sized by its volume, runs the lattice's whole CG loop on the
+ * device with bounded barriers.  Other mixes run a host thread and the lattice's own stream
+ * per solve.  Results and iteration counts are those of separate yg_cg_inverter calls (to
+ * rounding); returns the worst status.  The calling thread's current device is used for all
+ * of them. */
 int yg_cg_inverter_lattices(int n, yg_lattice *const *lats, const yg_inv_par *pars, double *const *xs,
                             double *const *bs, int *iters);
+/* As yg_cg_inverter_lattices, with the persistent kernel's barrier wait limit in GPU clock
+ * cycles (<= 0: the default, about 10 s): a wait that runs out ends the launch and the call
+ * returns YG_TIMEOUT (the fields then hold a partial solve; the context stays usable).
+ * *persistent (may be NULL) is set to 1 when the persistent kernel ran, 0 for the threads. */
+int yg_cg_inverter_lattices_ex(int n, yg_lattice *const *lats, const yg_inv_par *pars, double *const *xs,
+                               double *const *bs, int *iters, long long wait_cycles, int *persistent);
 /* No reference counterpart: nrhs <= 16 bicgstab_inverter solves on Dphi (bicgstab.cpp:9-97,
  * each system with its own scalars, stopping test and iteration count) sharing every operator
  * application; even-odd lattices with d = 3 */
 int yg_bicgstab_inverter_multi(yg_lattice *lat, const yg_inv_par *par, int nrhs, double *const *xs,
                                double *const *bs, int *iters);
 
-/* No reference counterpart: nrhs solves of Hphi_sq with FP32 inner iterations (the compressed
- * operator with FP32 links and clover blocks) and FP64 reliable updates, advanced together;
- * every system stops on its own TRUE FP64 residual |b_i - A x_i|^2 < prec |b_i|^2 (a
- * system that stalls continues with the batched FP64 CG).  stats[i] per system.
- * 1 <= nrhs <= 16, d = 3, even-odd; xs[i] on entry is the initial guess. */
+/* No reference counterpart: nrhs solves of Hphi_sq with low-precision inner iterations (the
+ * compressed operator: FP16 spinors with per-site norms, FP32 links and clover blocks, one
+ * launch per Schur step for all systems, the CG update fused into the last step) and FP64
+ * reliable updates, advanced together; every system stops on its own TRUE FP64 residual
+ * |b_i - A x_i|^2 < prec |b_i|^2 (a system that stalls continues with the FP64 CG).
+ * stats[i] per system.  1 <= nrhs <= 16, d = 3, even-odd; xs[i] on entry is the initial guess. */
 int yg_cg_mixed_multi(yg_lattice *lat, const yg_inv_par *par, int nrhs, double *const *xs, double *const *bs,
                       double delta, yg_solve_stats *stats);
+/* As yg_cg_mixed_multi with a mass per system (masses[i] replaces par->mass; at most 4
+ * distinct values): the solves of several monomials at once, e.g. the Hphi_sq solves of the
+ * HMC monomial (mass m + dm) and of the Hasenbusch monomial (mass m) of one force evaluation
+ * (hmc.cpp:68-94, hasenbusch.cpp:67-96) in the same operator launches. */
+int yg_cg_mixed_multi_masses(yg_lattice *lat, const yg_inv_par *par, int nrhs, const double *masses,
+                             double *const *xs, double *const *bs, double delta, yg_solve_stats *stats);
 
 /* No reference counterpart (measurement support): mean time per launch of `reps` launches of
  * step 1 of yg_cg_mixed's inner operator (its dominant kernel), timed with CUDA events on the

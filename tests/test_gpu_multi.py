@@ -109,6 +109,34 @@ def test_mixed_multi_true_residuals(name):
             assert sts[0]["iterations"] <= 1.5 * it64 + 10, (sts[0], it64)
 
 
+@pytest.mark.parametrize("name", ["su3_fund_ap", "su3_fund_ap_nocl", "su2_adj_ap"])
+def test_mixed_multi_masses(name):
+    """A mass per system (yg_cg_mixed_multi_masses), as the HMC (m + dm) and Hasenbusch (m)
+    monomials' solves of one force evaluation: every system meets its true FP64 residual with
+    its own mass, and matches a single-mass solve of the same system."""
+    dims = (8, 8, 8, 8) if name.startswith("su3") else (4, 6, 4, 8)
+    lat, O, rng = make_pair(name, dims, seed=56)
+    masses = [-0.4, -0.2, -0.4, -0.3, -0.2]
+    prec = 1e-24
+    bs = [lat.field(source(O, rng)) for _ in masses]
+    xs = [lat.field() for _ in masses]
+    sts = lat.cg_mixed_multi("Hphi_sq", 0.0, prec, xs, bs, delta=0.1, masses=masses)
+    assert lat.last_status == 0
+    for i, m in enumerate(masses):
+        assert sts[i]["fallback"] == 0, sts[i]
+        assert sts[i]["true_residual"] < prec
+        assert _true_residual(lat, "Hphi_sq", m, xs[i], bs[i]) < prec
+    lo, hi = O.default_range()
+    for i in (1, 3):
+        x1 = lat.field()
+        st = lat.cg_mixed_multi("Hphi_sq", masses[i], prec, [x1], [bs[i]], delta=0.1)
+        assert st[0]["true_residual"] < prec
+        a, c = lat.download(xs[i])[lo:hi], lat.download(x1)[lo:hi]
+        assert np.abs(a - c).max() <= 1e-7 * np.abs(c).max()      # both at |r|^2 < 1e-24 |b|^2
+    with pytest.raises(Exception):
+        lat.cg_mixed_multi("Hphi_sq", 0.0, prec, xs, bs, masses=[-0.1, -0.2, -0.3, -0.4, -0.5])
+
+
 @pytest.mark.parametrize("name", ["su3_fund_ap", "su3_fund_open", "su3_fund_ap_nocl", "su2_adj_ap"])
 def test_bicgstab_multi_matches_single(name):
     """Batched bicgstab_inverter on Dphi (yg_bicgstab_inverter_multi): each system reproduces

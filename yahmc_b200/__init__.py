@@ -105,6 +105,7 @@ _SIGNATURES = {
     "yg_cg_mixed_opts": [_P, ctypes.POINTER(InvPar), ctypes.POINTER(MixedOpts), _P, _P, ctypes.POINTER(SolveStats)],
     "yg_cg_inverter_multi": [_P, _P, _I, _P, _P, _P], "yg_bicgstab_inverter_multi": [_P, _P, _I, _P, _P, _P],
     "yg_cg_mixed_multi": [_P, _P, _I, _P, _P, _D, _P],
+    "yg_cg_mixed_multi_masses": [_P, _P, _I, _P, _P, _P, _D, _P],
     "yg_inner_hop_profile": [_P, _D, _I, _P, _P],
     "yg_mre_init": [_P, _I, _I, _D, _P], "yg_mre_store": [_P, _P], "yg_mre_guess": [_P, _P, _P],
     "yg_mre_reset": [_P], "yg_mre_free": [_P],
@@ -112,6 +113,7 @@ _SIGNATURES = {
     "yg_calc_propagator": [_P, _D, _D, _P, _P, _P], "yg_calc_propagator_multi": [_P, _D, _D, _I, _P, _P, _I, _P],
     "yg_meson_contract": [_P, _I, _I, _P, _I, _P],
     "yg_tune_inner_links": [_P, _D, _P, _P], "yg_cg_inverter_lattices": [_I, _P, _P, _P, _P, _P],
+    "yg_cg_inverter_lattices_ex": [_I, _P, _P, _P, _P, _P, ctypes.c_longlong, _P],
     "yg_wf_init": [_P], "yg_wf_zeta": [_P, _D], "yg_wf_update": [_P, _D], "yg_wf_iterate": [_P, _D],
     "yg_wf_observables": [_P, _P, _P, _P], "yg_wf_fermion_init": [_P, _I], "yg_wf_fermion_iterate": [_P, _D, _P, _I],
     "yg_gauge_save_cfg": [_P, ctypes.c_char_p, _I, _I], "yg_gauge_load_cfg": [_P, ctypes.c_char_p, _P, _P, _P],
@@ -257,20 +259,24 @@ def set_device(device: int) -> None:
         raise YGError(1, lib.yg_last_error().decode())
 
 
-def cg_inverter_lattices(solves, op="Hphi_sq"):
-    """Independent cg_inverter solves on several lattices at once (yg_cg_inverter_lattices):
-    `solves` is a list of (lattice, mass, prec, x, b); returns (iteration counts, status)."""
+def cg_inverter_lattices(solves, op="Hphi_sq", wait_cycles=0, with_path=False):
+    """Independent cg_inverter solves on several lattices at once (yg_cg_inverter_lattices_ex):
+    `solves` is a list of (lattice, mass, prec, x, b) or (lattice, mass, prec, x, b, maxiter);
+    returns (iteration counts, status), plus 1 / 0 for the persistent kernel / the host
+    threads when with_path.  wait_cycles bounds each barrier wait of the persistent kernel
+    (0: the default); a wait that runs out gives status 7 (YG_TIMEOUT)."""
     lib = load_library()
     n = len(solves)
     lats = (ctypes.c_void_p * n)(*[s[0].h for s in solves])
-    pars = (InvPar * n)(*[Lattice._par(op, s[1], s[2]) for s in solves])
+    pars = (InvPar * n)(*[Lattice._par(op, s[1], s[2], 0, s[5] if len(s) > 5 else 0) for s in solves])
     xs = (ctypes.c_void_p * n)(*[s[3].ptr for s in solves])
     bs = (ctypes.c_void_p * n)(*[s[4].ptr for s in solves])
     its = (ctypes.c_int * n)()
-    rc = lib.yg_cg_inverter_lattices(n, lats, pars, xs, bs, its)
-    if rc not in (0, 4):
+    path = ctypes.c_int(-1)
+    rc = lib.yg_cg_inverter_lattices_ex(n, lats, pars, xs, bs, its, int(wait_cycles), ctypes.byref(path))
+    if rc not in (0, 4, 7):
         raise YGError(rc, lib.yg_last_error().decode())
-    return list(its), rc
+    return (list(its), rc, path.value) if with_path else (list(its), rc)
 
 
 def launch_count() -> int:
@@ -644,8 +650,9 @@ class Lattice:
         self._check(self.lib.yg_inner_hop_profile(self.h, mass, int(reps), ctypes.byref(ms), ctypes.byref(by)))
         return ms.value, by.value
 
-    def cg_mixed_multi(self, op, mass, prec, xs, bs, delta=0.1, log=0, maxiter=0):
-        """len(xs) mixed-precision solves advanced together; one stats dict per system"""
+    def cg_mixed_multi(self, op, mass, prec, xs, bs, delta=0.1, log=0, maxiter=0, masses=None):
+        """len(xs) mixed-precision solves advanced together; one stats dict per system.
+        masses (a mass per system, at most 4 distinct) replaces mass."""
         n = len(xs)
         if n != len(bs):
             raise ValueError("xs and bs differ in length")
@@ -653,7 +660,13 @@ class Lattice:
         px = (ctypes.c_void_p * n)(*[x.ptr for x in xs])
         pb = (ctypes.c_void_p * n)(*[b.ptr for b in bs])
         sts = (SolveStats * n)()
-        rc = self.lib.yg_cg_mixed_multi(self.h, ctypes.byref(par), n, px, pb, float(delta), sts)
+        if masses is None:
+            rc = self.lib.yg_cg_mixed_multi(self.h, ctypes.byref(par), n, px, pb, float(delta), sts)
+        else:
+            if len(masses) != n:
+                raise ValueError("one mass per system")
+            pm = (ctypes.c_double * n)(*[float(m) for m in masses])
+            rc = self.lib.yg_cg_mixed_multi_masses(self.h, ctypes.byref(par), n, pm, px, pb, float(delta), sts)
         self.last_status = rc
         if rc not in (0, 4, 5):
             self._check(rc)

@@ -289,6 +289,19 @@ int yg_cg_inverter_lattices(int n, yg_lattice *const *lats, const yg_inv_par *pa
     return yg::cg_lattices(n, L.data(), pars, xs, bs, iters);
   });
 }
+int yg_cg_inverter_lattices_ex(int n, yg_lattice *const *lats, const yg_inv_par *pars, double *const *xs,
+                               double *const *bs, int *iters, long long wait_cycles, int *persistent) {
+  return guard_status([&] {
+    need(lats, "lats"); need(pars, "pars"); need(xs, "xs"); need(bs, "bs"); need(iters, "iters");
+    if (n < 1 || n > 64) throw yg::Error(YG_ERR_ARG, "1..64 lattices");
+    std::vector<yg::Lattice *> L(n);
+    for (int i = 0; i < n; i++) {
+      check_par(&pars[i]); need(xs[i], "xs[i]"); need(bs[i], "bs[i]");
+      L[i] = &lat(lats[i]);
+    }
+    return yg::cg_lattices(n, L.data(), pars, xs, bs, iters, wait_cycles, persistent);
+  });
+}
 int yg_bicgstab_inverter_multi(yg_lattice *l, const yg_inv_par *p, int nrhs, double *const *xs, double *const *bs,
                                int *iters) {
   return guard_status([&] {
@@ -303,6 +316,14 @@ int yg_cg_mixed_multi(yg_lattice *l, const yg_inv_par *p, int nrhs, double *cons
     check_par(p); need(xs, "xs"); need(bs, "bs"); need(stats, "stats");
     for (int i = 0; i < nrhs; i++) { need(xs[i], "xs[i]"); need(bs[i], "bs[i]"); }
     return yg::cg_mixed_mrhs(lat(l), *p, nrhs, xs, bs, delta, stats);
+  });
+}
+int yg_cg_mixed_multi_masses(yg_lattice *l, const yg_inv_par *p, int nrhs, const double *masses,
+                             double *const *xs, double *const *bs, double delta, yg_solve_stats *stats) {
+  return guard_status([&] {
+    check_par(p); need(masses, "masses"); need(xs, "xs"); need(bs, "bs"); need(stats, "stats");
+    for (int i = 0; i < nrhs; i++) { need(xs[i], "xs[i]"); need(bs[i], "bs[i]"); }
+    return yg::cg_mixed_mrhs(lat(l), *p, nrhs, xs, bs, delta, stats, masses);
   });
 }
 int yg_inner_hop_profile(yg_lattice *l, double mass, int reps, double *ms, double *bytes) {

@@ -97,6 +97,7 @@ struct Lattice {
   DevBuf sl_part;      // per-block partial sums of the device-scalar reductions
   int sl_grid_nrm = 0; // blocks of the hop that forms <p, A p> (resident-grid size)
   int sl_grid_vec = 0; // blocks of the inner vector kernels
+  int sl_grid_cg = 0;  // blocks of the last Schur step with the fused CG update (resident grid)
   DevBuf sl_scal;      // device scalars of the inner CG (rr, alpha, beta, ...) + completion counter
   double *sl_hist = nullptr;          // mapped pinned host ring of inner |r|^2 (written by the GPU)
   cudaEvent_t sl_ev[2] = {nullptr, nullptr};
@@ -106,6 +107,7 @@ struct Lattice {
   DevBuf mr_work;
   int mr_cap = 0;
   DevBuf mr_scal, mr_part;
+  DevBuf mr_clov;      // packed FP32 clover blocks of the further masses of a multi-mass call
   double *mr_hist = nullptr;
   int mr_tile[17] = {};   // measured inner-operator variant (tile, threads per site) + 1, per system count
 
@@ -182,7 +184,11 @@ void f_xpay(Lattice &L, float *p, float b, const float *r, long cnt);
 // ---- yg_solvers.cu
 int cg(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
 // cg on several lattices at once, one host thread and the lattice's own stream each (yg_solvers.cu)
-int cg_lattices(int n, Lattice *const *L, const yg_inv_par *par, double *const *xs, double *const *bs, int *iters);
+int cg_lattices(int n, Lattice *const *L, const yg_inv_par *par, double *const *xs, double *const *bs, int *iters,
+                long long wait_cycles = 0, int *persistent = nullptr);
+bool batch_eligible(int n, Lattice *const *L, const yg_inv_par *par);
+int cg_lattices_persistent(int n, Lattice *const *L, const yg_inv_par *par, double *const *xs, double *const *bs,
+                           int *iters, long long wait_cycles);
 int cg_mshift(Lattice &L, const yg_inv_par &par, int num, const double *shift, double *const *xs, double *b, int *iters);
 int bicgstab(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
 int minres(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
@@ -253,7 +259,8 @@ int cg_mixed_multi(Lattice &L, const yg_inv_par &par, int nrhs, double *const *x
 // the same with the compressed FP16/FP32 inner operator applied to a tile of systems per
 // thread, device-side scalars and one-iteration-late host reads (yg_mrhs.cu)
 int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, double *const *bs, double delta,
-                  yg_solve_stats *stats);
+                  yg_solve_stats *stats, const double *masses = nullptr);
+void pack_clover_f32(Lattice &L, double mass, void *dst, float *cn);
 // the compressed inner operator's matrices (yg_sloppy.cu); formats 32 / 16 / 15, 0 = as prec
 void ensure_sloppy(Lattice &L, double mass, int prec, int reals, int lfmt, int cfmt);
 void inner_hop_profile(Lattice &L, double mass, int reps, double *ms, double *bytes);

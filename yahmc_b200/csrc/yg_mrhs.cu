@@ -11,7 +11,9 @@
 // the other tiles find the links in L2.
 //
 // Every system keeps its own fields in the single-system formats (FP16 spinors with per-site
-// norms for p, A p and the intermediates; FP32 x and r), its own device scalars (|r|^2 in
+// norms for p, Hphi p and the intermediates; FP32 x and r; A p = Hphi Hphi p is never stored:
+// x += alpha p, r -= alpha A p and the |r|^2 partials are the epilogue of the operator's
+// last step), its own device scalars (|r|^2 in
 // two alternating slots, alpha, beta), and the single-system rules: reliable updates with
 // the FP64 operator when |r| has fallen by delta or stagnates, a stop on the TRUE FP64
 // residual |b - A x|^2 < prec |b|^2, and a fall-back to the FP64 CG on a stall.  All
@@ -36,6 +38,7 @@ namespace yg {
 namespace {
 
 constexpr int kMR = 16;       // systems per call (kMaxRhs of the batched solvers)
+constexpr int kMaxMasses = 4; // distinct masses per call
 constexpr int kHopThreads = 128;
 constexpr int kVecThreads = 256;
 
@@ -49,13 +52,23 @@ struct MHopArgs {
   Geom g;
   MSpin src, src2, dst;
   const void *U;            // FP32 links, K complex words each
-  const void *C;            // FP32 packed clover blocks (M_e even, M_o^-1 odd), 18 float4 per site
+  const void *C[kMR];       // FP32 packed clover blocks (M_e even, M_o^-1 odd) of slot j's mass, 18 float4 per site
   float coeff;
   int lo, n;                // output sites [lo, lo + n)
   int nsys, ntile;
-  double *part;             // NRM: part[j * nsb + site block] = sum of |dst_j|^2 over the block
-  int nsb;
+  double *part;             // NRM: part[j * nsb + site block] = sum of |dst_j|^2 (NRM 1) or of the new
+  int nsb;                  //   |r_j|^2 (NRM 2) over the block
+  // NRM = 2, the last step of the iteration's second Hphi: the CG update of launch slot j
+  // (x_j += alpha p_j, r_j -= alpha q_j with q_j = the step's output, never stored)
+  float2 *x[kMR], *r[kMR];  // FP32 even-site words
+  MSpin p;
+  const double *scal;
+  int sys[kMR];             // global system index of launch slot j (its scalars)
 };
+
+// Device scalars of system i: scal[i * kW + M_*] (M_RR0/M_RR1 alternate with the iteration
+// parity, as in the single-system solver), plus the next beta.
+enum { M_RR0 = 0, M_RR1 = 1, M_ALPHA = 2, M_PQ = 3, M_BETA = 4, kW = 8 };
 
 template <int MU, int SIG>
 __device__ __forceinline__ void project(float2 (&hh)[2][3], const float2 (&p)[12]) {
@@ -217,10 +230,10 @@ __global__ void __launch_bounds__(kHopThreads, MinBlocks<R>::value) k_mhop(MHopA
   if (live) {
     const int blk = id >= g.Vh, h = id - blk * g.Vh;
     const bool bnd = spinor_zeroed(g, t0);
-    const float4 *C = reinterpret_cast<const float4 *>(a.C);
 #pragma unroll
     for (int r = 0; r < R; r++) {
       if (r < rc && (SPLIT == 1 || (r & 1) == part)) {
+        const float4 *C = reinterpret_cast<const float4 *>(a.C[s0 + r]);
         float2 in[12], out[12];
         if (STEP == 1) {
 #pragma unroll
@@ -251,10 +264,30 @@ __global__ void __launch_bounds__(kHopThreads, MinBlocks<R>::value) k_mhop(MHopA
             if (k >= 6) out[k] = cscale(out[k], -1.f);      // gamma5
           }
           if (bnd) out[k] = make_float2(0.f, 0.f);
-          sq = fmaf(out[k].x, out[k].x, fmaf(out[k].y, out[k].y, sq));
+          if (NRM != 2) sq = fmaf(out[k].x, out[k].x, fmaf(out[k].y, out[k].y, sq));
+        }
+        if constexpr (NRM == 2) {
+          // x += alpha p ; r -= alpha q on the (even) site, |r|^2 of the site
+          const float al = (float)a.scal[a.sys[s0 + r] * kW + M_ALPHA];
+          float2 pp[12];
+          sload<16>(pp, a.p.d[s0 + r], a.p.n[s0 + r], 0, h, g.Vh);
+          float2 *xs = a.x[s0 + r], *rs = a.r[s0 + r];
+#pragma unroll
+          for (int k = 0; k < 12; k++) {
+            const long i = (long)k * g.Vh + h;
+            float2 xi = xs[i], ri = rs[i];
+            xi.x = fmaf(al, pp[k].x, xi.x);
+            xi.y = fmaf(al, pp[k].y, xi.y);
+            ri.x = fmaf(-al, out[k].x, ri.x);
+            ri.y = fmaf(-al, out[k].y, ri.y);
+            xs[i] = xi;
+            rs[i] = ri;
+            sq = fmaf(ri.x, ri.x, fmaf(ri.y, ri.y, sq));
+          }
+        } else {
+          sstore<16>(a.dst.d[s0 + r], a.dst.n[s0 + r], out, blk, h, g.Vh);
         }
         n2[r] = sq;
-        sstore<16>(a.dst.d[s0 + r], a.dst.n[s0 + r], out, blk, h, g.Vh);
       }
     }
   }
@@ -268,14 +301,11 @@ __global__ void __launch_bounds__(kHopThreads, MinBlocks<R>::value) k_mhop(MHopA
 }
 
 // ---- per-system vectors and scalars
-// Device scalars of system i: scal[i * kW + S_*] (S_RR0/S_RR1 alternate with the iteration
-// parity, as in the single-system solver), plus the next beta.
-enum { M_RR0 = 0, M_RR1 = 1, M_ALPHA = 2, M_PQ = 3, M_BETA = 4, kW = 8 };
 
 struct MVec {
   float2 *x[kMR];           // FP32 inner solution increments
   float2 *r[kMR];           // FP32 iterated residuals
-  MSpin p, q;
+  MSpin p;
   int sys[kMR];             // global system index of launch slot j
   int nsys;
 };
@@ -300,35 +330,6 @@ __global__ void k_m_alpha(double *scal, const double *part, int nsb, MVec v, int
     s[M_PQ] = pq;
     s[M_ALPHA] = s[M_RR0 + par] / pq;
   }
-}
-
-// x_i += alpha_i p_i ; r_i -= alpha_i q_i ; per-block partials of |r_i|^2
-__global__ void __launch_bounds__(kVecThreads) k_m_update(const double *scal, double *part, MVec v, int Vh) {
-  const int j = blockIdx.y;
-  const float al = (float)scal[v.sys[j] * kW + M_ALPHA];
-  float2 *x = v.x[j], *r = v.r[j];
-  double acc = 0.0;
-  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += gridDim.x * blockDim.x) {
-    float2 pp[12], qq[12];
-    sload<16>(pp, v.p.d[j], v.p.n[j], 0, h, Vh);
-    sload<16>(qq, v.q.d[j], v.q.n[j], 0, h, Vh);
-    float s = 0.f;
-#pragma unroll
-    for (int k = 0; k < 12; k++) {
-      const long i = (long)k * Vh + h;
-      float2 xi = x[i], ri = r[i];
-      xi.x = fmaf(al, pp[k].x, xi.x);
-      xi.y = fmaf(al, pp[k].y, xi.y);
-      ri.x = fmaf(-al, qq[k].x, ri.x);
-      ri.y = fmaf(-al, qq[k].y, ri.y);
-      x[i] = xi;
-      r[i] = ri;
-      s = fmaf(ri.x, ri.x, fmaf(ri.y, ri.y, s));
-    }
-    acc += s;
-  }
-  acc = block_total(acc);
-  if (threadIdx.x == 0) part[(long)j * gridDim.x + blockIdx.x] = acc;
 }
 
 // |r_i|^2 from the update's partials, beta_i = |r_i|^2 / |r_i,old|^2; the values go to the
@@ -392,7 +393,7 @@ struct HField {
 // per-system working storage, carved from one allocation kept on the lattice
 struct SysBufs {
   float2 *fx, *fr;          // FP32 even-site words (12 complex per site)
-  HField p, q, t, o;        // FP16 fields of the whole lattice (p, q, t on even sites, o odd)
+  HField p, t, o;           // FP16 fields of the whole lattice (p, t = Hphi p on even sites, o odd)
   double *xbest;            // FP64 copy of the best iterate (whole field)
 };
 
@@ -400,7 +401,7 @@ size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
 size_t sys_bytes(const Lattice &L) {
   const size_t vh = (size_t)L.Vh;
-  return 2 * align256(96 * vh) + 4 * (align256(96 * vh) + align256(8 * vh)) + align256(L.field_bytes());
+  return 2 * align256(96 * vh) + 3 * (align256(96 * vh) + align256(8 * vh)) + align256(L.field_bytes());
 }
 
 SysBufs sys_bufs(Lattice &L, int i) {
@@ -409,7 +410,7 @@ SysBufs sys_bufs(Lattice &L, int i) {
   SysBufs b;
   b.fx = reinterpret_cast<float2 *>(p); p += align256(96 * vh);
   b.fr = reinterpret_cast<float2 *>(p); p += align256(96 * vh);
-  for (HField *f : {&b.p, &b.q, &b.t, &b.o}) {
+  for (HField *f : {&b.p, &b.t, &b.o}) {
     f->d = p; p += align256(96 * vh);
     f->n = reinterpret_cast<float *>(p); p += align256(8 * vh);
   }
@@ -421,14 +422,16 @@ int vec_grid(int sms) { return sms * 4; }
 
 // the two Schur steps of the inner operator for a launch's systems, R systems per thread,
 // SPLIT threads per site
+// mode of the second step: 0 plain, 1 with the |dst|^2 partials, 2 with the CG update
 template <int K, int R, int SPLIT>
-void launch_mhop_r(Lattice &L, const MHopArgs &a0, const MHopArgs &b0, bool nrm) {
+void launch_mhop_r(Lattice &L, const MHopArgs &a0, const MHopArgs &b0, int mode) {
   MHopArgs a = a0, b = b0;
   a.nsb = b.nsb = nblk(a.n, kHopThreads / SPLIT);
   const int grid = a.ntile * a.nsb;
   k_mhop<K, R, 1, 0, SPLIT><<<grid, kHopThreads, 0, L.stream>>>(a);
   YG_LAUNCHED();
-  if (nrm) k_mhop<K, R, 2, 1, SPLIT><<<grid, kHopThreads, 0, L.stream>>>(b);
+  if (mode == 1) k_mhop<K, R, 2, 1, SPLIT><<<grid, kHopThreads, 0, L.stream>>>(b);
+  else if (mode == 2) k_mhop<K, R, 2, 2, SPLIT><<<grid, kHopThreads, 0, L.stream>>>(b);
   else k_mhop<K, R, 2, 0, SPLIT><<<grid, kHopThreads, 0, L.stream>>>(b);
   YG_LAUNCHED();
 }
@@ -437,19 +440,19 @@ void launch_mhop_r(Lattice &L, const MHopArgs &a0, const MHopArgs &b0, bool nrm)
 constexpr int kVariants[5][2] = {{1, 1}, {2, 1}, {4, 1}, {2, 2}, {4, 2}};
 
 template <int K>
-void launch_mhop_k(Lattice &L, int var, const MHopArgs &a, const MHopArgs &b, bool nrm) {
+void launch_mhop_k(Lattice &L, int var, const MHopArgs &a, const MHopArgs &b, int mode) {
   switch (var) {
-    case 0: launch_mhop_r<K, 1, 1>(L, a, b, nrm); break;
-    case 1: launch_mhop_r<K, 2, 1>(L, a, b, nrm); break;
-    case 2: launch_mhop_r<K, 4, 1>(L, a, b, nrm); break;
-    case 3: launch_mhop_r<K, 2, 2>(L, a, b, nrm); break;
-    default: launch_mhop_r<K, 4, 2>(L, a, b, nrm); break;
+    case 0: launch_mhop_r<K, 1, 1>(L, a, b, mode); break;
+    case 1: launch_mhop_r<K, 2, 1>(L, a, b, mode); break;
+    case 2: launch_mhop_r<K, 4, 1>(L, a, b, mode); break;
+    case 3: launch_mhop_r<K, 2, 2>(L, a, b, mode); break;
+    default: launch_mhop_r<K, 4, 2>(L, a, b, mode); break;
   }
 }
 
-void launch_mhop(Lattice &L, int reals, int var, const MHopArgs &a, const MHopArgs &b, bool nrm) {
-  if (reals == 12) launch_mhop_k<6>(L, var, a, b, nrm);
-  else launch_mhop_k<9>(L, var, a, b, nrm);
+void launch_mhop(Lattice &L, int reals, int var, const MHopArgs &a, const MHopArgs &b, int mode) {
+  if (reals == 12) launch_mhop_k<6>(L, var, a, b, mode);
+  else launch_mhop_k<9>(L, var, a, b, mode);
 }
 
 }  // namespace
@@ -457,7 +460,7 @@ void launch_mhop(Lattice &L, int reals, int var, const MHopArgs &a, const MHopAr
 int cg(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
 
 int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs, double *const *bs, double delta,
-                  yg_solve_stats *stats) {
+                  yg_solve_stats *stats, const double *masses) {
   auto t0 = std::chrono::steady_clock::now();
   if (par.op != YG_OP_HPHI_SQ) throw Error(YG_ERR_ARG, "the multi-system mixed CG solves Hphi_sq systems");
   if (nrhs < 1 || nrhs > kMR) throw Error(YG_ERR_ARG, "1..16 right-hand sides");
@@ -472,7 +475,32 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
   }
   const int nb = nrhs;
   const int reals = (L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL) ? 12 : 18;
-  ensure_sloppy(L, par.mass, 16, reals, 32, 32);
+  // the mass of each system (masses == nullptr: par.mass for all); the first one's clover
+  // blocks are the lattice's own inner-operator copy, every other distinct mass gets a
+  // packed set of its own, rebuilt on each call (a few hop times)
+  std::vector<double> mass(nb, par.mass);
+  if (masses)
+    for (int i = 0; i < nb; i++) {
+      if (!std::isfinite(masses[i])) throw Error(YG_ERR_ARG, "masses must be finite");
+      mass[i] = masses[i];
+    }
+  std::vector<double> dist;
+  for (double mv : mass)
+    if (std::find(dist.begin(), dist.end(), mv) == dist.end()) dist.push_back(mv);
+  if ((int)dist.size() > kMaxMasses) throw Error(YG_ERR_ARG, "at most 4 distinct masses per call");
+  const size_t clov_bytes = sizeof(float) * 72 * (size_t)L.V;
+  if (dist.size() > 1) {
+    L.mr_clov.alloc(clov_bytes * (dist.size() - 1) + sizeof(float) * (size_t)L.V);
+    for (size_t k = 1; k < dist.size(); k++)
+      pack_clover_f32(L, dist[k], L.mr_clov.as<char>() + clov_bytes * (k - 1),
+                      reinterpret_cast<float *>(L.mr_clov.as<char>() + clov_bytes * (dist.size() - 1)));
+  }
+  ensure_sloppy(L, dist[0], 16, reals, 32, 32);
+  std::vector<const void *> clov(nb);
+  for (int i = 0; i < nb; i++) {
+    const size_t k = std::find(dist.begin(), dist.end(), mass[i]) - dist.begin();
+    clov[i] = k == 0 ? L.sl_clover.p : L.mr_clov.as<char>() + clov_bytes * (k - 1);
+  }
 
   int dev = 0, sms = 0;
   YG_CUDA(cudaGetDevice(&dev));
@@ -511,7 +539,7 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
 
   auto residual = [&](int i) {      // r64 = b_i - A x_i in FP64, returns |r|^2
     blas_copy(L, xd, xs[i]);
-    apply_op(L, YG_OP_HPHI_SQ, par.mass, Ax, xd);
+    apply_op(L, YG_OP_HPHI_SQ, mass[i], Ax, xd);
     blas_copy(L, r64, bs[i]);
     blas_axpby(L, r64, make_double2(1, 0), make_double2(-1, 0), Ax, lo, n);
     return blas_sqnorm(L, r64, lo, n);
@@ -546,33 +574,40 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
       v.x[j] = b.fx;
       v.r[j] = b.fr;
       v.p.d[j] = b.p.d; v.p.n[j] = b.p.n;
-      v.q.d[j] = b.q.d; v.q.n[j] = b.q.n;
       v.sys[j] = act[j];
     }
   };
   int var = 2;                                // index into kVariants
-  auto hphi = [&](bool nrm, bool second) {   // t = Hphi p (first) or q = Hphi t (second), o the odd sites
+  // t = Hphi p (first; mode 1 adds the <p, A p> partials) or Hphi t (second; mode 2 fuses the
+  // CG update, x += alpha p, r -= alpha Hphi t, with the |r|^2 partials), o the odd sites
+  auto hphi = [&](int mode, bool second) {
     MHopArgs a{};
     a.g = L.g;
     a.U = L.sl_links.p;
-    a.C = L.sl_clover.p;
     a.nsys = (int)act.size();
     const int tile = kVariants[var][0];
     a.ntile = (a.nsys + tile - 1) / tile;
-    a.part = part_pq;
+    a.part = mode == 2 ? part_r : part_pq;
+    a.scal = scal;
     MHopArgs b = a;
     for (int j = 0; j < a.nsys; j++) {
       const SysBufs &s = sb[act[j]];
-      const HField in = second ? s.t : s.p, out = second ? s.q : s.t;
+      const HField in = second ? s.t : s.p;
       a.src.d[j] = in.d; a.src.n[j] = in.n;
       a.dst.d[j] = s.o.d; a.dst.n[j] = s.o.n;
       b.src.d[j] = s.o.d; b.src.n[j] = s.o.n;
       b.src2.d[j] = in.d; b.src2.n[j] = in.n;
-      b.dst.d[j] = out.d; b.dst.n[j] = out.n;
+      b.dst.d[j] = second ? nullptr : s.t.d;         // the second Hphi stores no output
+      b.dst.n[j] = second ? nullptr : s.t.n;
+      a.C[j] = clov[act[j]];
+      b.C[j] = clov[act[j]];
+      b.x[j] = s.fx; b.r[j] = s.fr;
+      b.p.d[j] = s.p.d; b.p.n[j] = s.p.n;
+      b.sys[j] = act[j];
     }
     a.coeff = 0.5f; a.lo = Vh; a.n = Vh;
     b.coeff = -0.5f; b.lo = 0; b.n = Vh;
-    launch_mhop(L, reals, var, a, b, nrm);
+    launch_mhop(L, reals, var, a, b, mode);
     L.mvm += 2 * a.nsys;
   };
   auto wait_iteration = [&](unsigned long long k) {
@@ -611,9 +646,9 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
         if (r > 1 && r >= 2 * ns) continue;
         var = cand;
         calls += 4;
-        hphi(false, false);                      // warm-up; t only (p untouched)
+        hphi(0, false);                          // warm-up; t only (p untouched)
         YG_CUDA(cudaEventRecord(e0, L.stream));
-        for (int rep = 0; rep < 3; rep++) hphi(false, false);
+        for (int rep = 0; rep < 3; rep++) hphi(0, false);
         YG_CUDA(cudaEventRecord(e1, L.stream));
         YG_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
@@ -643,13 +678,12 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
     const int parity = it & 1;
     MVec v{};
     fill(v);
-    hphi(true, false);
-    k_m_alpha<<<1, 32 * v.nsys, 0, L.stream>>>(scal, part_pq, nblk(Vh, kHopThreads / kVariants[var][1]), v, parity);
+    const int nsb = nblk(Vh, kHopThreads / kVariants[var][1]);     // site blocks of an operator launch
+    hphi(1, false);
+    k_m_alpha<<<1, 32 * v.nsys, 0, L.stream>>>(scal, part_pq, nsb, v, parity);
     YG_LAUNCHED();
-    hphi(false, true);
-    k_m_update<<<dim3(gv, v.nsys), kVecThreads, 0, L.stream>>>(scal, part_r, v, Vh);
-    YG_LAUNCHED();
-    k_m_beta<<<1, 32 * v.nsys, 0, L.stream>>>(scal, part_r, gv, v, parity, const_cast<double *>(hist), seq,
+    hphi(2, true);
+    k_m_beta<<<1, 32 * v.nsys, 0, L.stream>>>(scal, part_r, nsb, v, parity, const_cast<double *>(hist), seq,
                                               (unsigned long long)it + 1);
     YG_LAUNCHED();
     k_m_xpay<<<dim3(gv, v.nsys), kVecThreads, 0, L.stream>>>(scal, v, Vh);
@@ -703,6 +737,7 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
     blas_copy(L, xs[i], sb[i].xbest);
     yg_inv_par p64 = par;
     p64.log = 0;
+    p64.mass = mass[i];
     int st = YG_OK;
     for (int attempt = 0; attempt < 3; attempt++) {
       int it64 = 0;

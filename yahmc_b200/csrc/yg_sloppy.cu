@@ -18,6 +18,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <thread>
 #include "yg_lattice.h"
 #include "yg_kernels.h"
@@ -88,11 +89,11 @@ __device__ __forceinline__ void shop_dir(float2 (&acc)[12], const SHopArgs &a, i
   }
 }
 
-// STEP 1 (odd output):  dst = M_o^-1 (coeff * hop(src))
-// STEP 2 (even output): dst = gamma5 (M_e src2 + coeff * hop(src))
-// returns |dst|^2 of the site (before FP16 rounding)
+// STEP 1 (odd output):  out = M_o^-1 (coeff * hop(src))
+// STEP 2 (even output): out = gamma5 (M_e src2 + coeff * hop(src))
+// (zero on the sites a boundary condition zeroes)
 template <int P, int LP, int CP, int K, int STEP>
-__device__ __forceinline__ float shop_site(const SHopArgs &a, int id, const SiteNbr &n) {
+__device__ __forceinline__ void shop_out(float2 (&out)[12], const SHopArgs &a, int id, const SiteNbr &n) {
   const Geom &g = a.g;
   const int T = g.dim[0], t0 = n.c[0];
   float2 acc[12];
@@ -107,7 +108,6 @@ __device__ __forceinline__ float shop_site(const SHopArgs &a, int id, const Site
   shop_dir<P, LP, K, 3, -1>(acc, a, n.f[3], id, t0);
   shop_dir<P, LP, K, 3, +1>(acc, a, n.b[3], n.b[3], t0);
   int blk = id >= g.Vh, h = id - blk * g.Vh;
-  float2 out[12];
   bool bnd = spinor_zeroed(g, t0);
   float cl[72];
   cload<CP>(cl, a.C, a.Cn, blk, h, g.Vh);
@@ -125,13 +125,22 @@ __device__ __forceinline__ float shop_site(const SHopArgs &a, int id, const Site
       if (k >= 6) out[k] = cscale(out[k], -1.f);            // gamma5
     }
   }
+  if (bnd) {
+#pragma unroll
+    for (int k = 0; k < 12; k++) out[k] = make_float2(0.f, 0.f);
+  }
+}
+
+// dst = out of the site; returns |dst|^2 (before FP16 rounding)
+template <int P, int LP, int CP, int K, int STEP>
+__device__ __forceinline__ float shop_site(const SHopArgs &a, int id, const SiteNbr &n) {
+  float2 out[12];
+  shop_out<P, LP, CP, K, STEP>(out, a, id, n);
   float n2 = 0.f;
 #pragma unroll
-  for (int k = 0; k < 12; k++) {
-    if (bnd) out[k] = make_float2(0.f, 0.f);
-    n2 = fmaf(out[k].x, out[k].x, fmaf(out[k].y, out[k].y, n2));
-  }
-  sstore<P>(a.dst, a.dst_norm, out, blk, h, g.Vh);
+  for (int k = 0; k < 12; k++) n2 = fmaf(out[k].x, out[k].x, fmaf(out[k].y, out[k].y, n2));
+  const int blk = id >= a.g.Vh;
+  sstore<P>(a.dst, a.dst_norm, out, blk, id - blk * a.g.Vh, a.g.Vh);
   return n2;
 }
 
@@ -158,6 +167,59 @@ __global__ void __launch_bounds__(128) k_shop(SHopArgs a) {
   }
   n2 = block_total(n2);
   if (threadIdx.x == 0) a.part[blockIdx.x] = n2;
+  griddep_launch();
+}
+
+// The last Schur step of the iteration's second Hphi with the CG update as its epilogue:
+// q = Hphi t stays in registers, alpha = |r|^2 / <p, A p> (every block sums the partials of
+// the NRM hop in the same order), x += alpha p, r -= alpha q on the site, and the per-block
+// partials of the new |r|^2 go to part_r.  q is never stored.  Resident grid, grid-stride.
+struct SCgArgs {
+  float2 *x, *r;                  // FP32 even-site words
+  const void *p;                  // search direction in the spinor format
+  const float *pn;
+  double *scal;
+  const double *part_pq;
+  int n_pq;
+  double *part_r;
+  int par;
+};
+
+template <int P, int LP, int CP, int K>
+__global__ void __launch_bounds__(128) k_shop_cg(SHopArgs a, SCgArgs c) {
+  griddep_wait();
+  const double pq = sum_partials(c.part_pq, c.n_pq);
+  const double alpha = c.scal[S_RR0 + c.par] / pq;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    c.scal[S_PQ] = pq;
+    c.scal[S_ALPHA] = alpha;
+  }
+  const float al = (float)alpha;
+  const int Vh = a.g.Vh;
+  double acc = 0.0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < a.n; t += gridDim.x * blockDim.x) {
+    SiteNbr n;
+    site_nbr(n, a.g, a.lo + t);
+    float2 q[12], pp[12];
+    shop_out<P, LP, CP, K, 2>(q, a, a.lo + t, n);
+    sload<P>(pp, c.p, c.pn, 0, t, Vh);
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+      const long i = (long)k * Vh + t;
+      float2 xi = c.x[i], ri = c.r[i];
+      xi.x = fmaf(al, pp[k].x, xi.x);
+      xi.y = fmaf(al, pp[k].y, xi.y);
+      ri.x = fmaf(-al, q[k].x, ri.x);
+      ri.y = fmaf(-al, q[k].y, ri.y);
+      c.x[i] = xi;
+      c.r[i] = ri;
+      s = fmaf(ri.x, ri.x, fmaf(ri.y, ri.y, s));
+    }
+    acc += s;
+  }
+  acc = block_total(acc);
+  if (threadIdx.x == 0) c.part_r[blockIdx.x] = acc;
   griddep_launch();
 }
 
@@ -343,61 +405,25 @@ __global__ void __launch_bounds__(256) k_s_from_d(void *dst, float *dn, const do
   }
 }
 
-// alpha = |r|^2 / <p, A p> from the partials of the NRM hop; x += alpha p ; r -= alpha q ;
-// per-block partials of the new |r|^2 into part_r
-template <int P>
-__global__ void __launch_bounds__(256) k_s_cg_update(float2 *x, float2 *r, const void *p, const float *pn,
-                                                     const void *q, const float *qn, double *scal,
-                                                     const double *part_pq, int n_pq, double *part_r, int par,
-                                                     int Vh) {
-  griddep_wait();
-  const double pq = sum_partials(part_pq, n_pq);
-  const double alpha = scal[S_RR0 + par] / pq;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    scal[S_PQ] = pq;
-    scal[S_ALPHA] = alpha;
-  }
-  const float a = (float)alpha;
-  double acc = 0.0;
-  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += gridDim.x * blockDim.x) {
-    float2 pp[12], qq[12];
-    sload<P>(pp, p, pn, 0, h, Vh);
-    sload<P>(qq, q, qn, 0, h, Vh);
-    float s = 0.f;
-#pragma unroll
-    for (int k = 0; k < 12; k++) {
-      long i = (long)k * Vh + h;
-      float2 xi = x[i], ri = r[i];
-      xi.x = fmaf(a, pp[k].x, xi.x);
-      xi.y = fmaf(a, pp[k].y, xi.y);
-      ri.x = fmaf(-a, qq[k].x, ri.x);
-      ri.y = fmaf(-a, qq[k].y, ri.y);
-      x[i] = xi;
-      r[i] = ri;
-      s = fmaf(ri.x, ri.x, fmaf(ri.y, ri.y, s));
-    }
-    acc += s;
-  }
-  acc = block_total(acc);
-  if (threadIdx.x == 0) part_r[blockIdx.x] = acc;
-  griddep_launch();
-}
-
 // |r|^2 from the update's partials, beta = |r|^2 / |r_old|^2, p = r + beta p; block 0
-// stores |r|^2 for the next iteration and into *hist, then the iteration number into *seq
-// (both mapped host memory, which the host polls one iteration later)
+// stores |r|^2 for the next iteration and into *hist, then counts the iteration (S_ITER)
+// and stores the count into *seq (hist and seq are mapped host memory, which the host polls
+// one iteration later).  Nothing in the arguments changes between iterations of the same
+// parity, so an iteration can be replayed as a CUDA graph.
 template <int P>
 __global__ void __launch_bounds__(256) k_s_xpay(void *p, float *pn, double *scal, const double *part_r, int n_r,
-                                                int par, double *hist, unsigned long long *seq,
-                                                unsigned long long iter, const float2 *r, int Vh) {
+                                                int par, double *hist, unsigned long long *seq, const float2 *r,
+                                                int Vh) {
   griddep_wait();
   const double rr = sum_partials(part_r, n_r);
   const float b = (float)(rr / scal[S_RR0 + par]);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     scal[S_RR0 + (par ^ 1)] = rr;
+    const double done = scal[S_ITER] + 1.0;
+    scal[S_ITER] = done;
     *reinterpret_cast<volatile double *>(hist) = rr;
     __threadfence_system();
-    *reinterpret_cast<volatile unsigned long long *>(seq) = iter;
+    *reinterpret_cast<volatile unsigned long long *>(seq) = (unsigned long long)done;
   }
   for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += gridDim.x * blockDim.x) {
     float2 pp[12];
@@ -500,16 +526,18 @@ void ensure_sloppy(Lattice &L, double mass, int prec, int reals, int lfmt, int c
     return;
   {
     // resident-grid sizes of the reduction kernels, and room for their partials
-    int dev = 0, sms = 0, per_nrm = 0, per_vec = 0;
+    int dev = 0, sms = 0, per_nrm = 0, per_vec = 0, per_cg = 0;
     YG_CUDA(cudaGetDevice(&dev));
     YG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     YG_SLOPPY_DISPATCH(prec, lfmt, cfmt, reals, {
       YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_nrm, k_shop<SP, SL, SC, SK, 2, 1>, 128, 0));
-      YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_vec, k_s_cg_update<SP>, 256, 0));
+      YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_cg, k_shop_cg<SP, SL, SC, SK>, 128, 0));
+      YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_vec, k_s_xpay<SP>, 256, 0));
     });
     L.sl_grid_nrm = (int)std::min<long>((long)sms * std::max(per_nrm, 1), nblk(L.Vh, 128));
+    L.sl_grid_cg = (int)std::min<long>((long)sms * std::max(per_cg, 1), nblk(L.Vh, 128));
     L.sl_grid_vec = (int)std::min<long>((long)sms * std::max(per_vec, 1), nblk(L.Vh, 256));
-    L.sl_part.alloc(sizeof(double) * (size_t)(L.sl_grid_nrm + L.sl_grid_vec));
+    L.sl_part.alloc(sizeof(double) * (size_t)(L.sl_grid_nrm + L.sl_grid_cg));
   }
   const int K = reals / 2;
   L.sl_links.alloc((lfmt == ST_F32 ? 8 : 4) * (size_t)K * 4 * L.V);
@@ -535,6 +563,20 @@ void ensure_sloppy(Lattice &L, double mass, int prec, int reals, int lfmt, int c
   L.sl_cfmt = cfmt;
   L.sl_mass = mass;
   L.sl_valid = true;
+}
+
+// FP32 packed clover blocks of another mass (M_e = (4+m+cf) + A on even sites, M_o^-1 on odd
+// sites; without a clover term 1 and (4+m)^2) into dst, for inner operators that carry one
+// block set per system.  cn receives the per-site norms of the packing (unused for FP32).
+void pack_clover_f32(Lattice &L, double mass, void *dst, float *cn) {
+  if (L.p.clover) ensure_ldl(L, 4.0 + mass);
+  const int clover = L.p.clover ? 1 : 0;
+  const double diag = clover ? 4.0 + mass : (4.0 + mass) * (4.0 + mass);
+  k_pack_clover_even<ST_F32><<<nblk(L.Vh, 64), 64, 0, L.stream>>>(dst, cn, L.clover.as<double2>(), L.g, diag,
+                                                                   L.p.cf - 1.0, clover);
+  YG_LAUNCHED();
+  k_pack_clover_odd<ST_F32><<<nblk(L.Vh, 64), 64, 0, L.stream>>>(dst, cn, L.ldl.as<double2>(), L.g, clover);
+  YG_LAUNCHED();
 }
 
 // launch with programmatic stream serialisation (the kernel waits for its predecessor
@@ -588,19 +630,46 @@ static void sloppy_hphi(Lattice &L, SField dst, SField src, SField tmp, bool nrm
   L.mvm += 2;
 }
 
-// par = iteration parity (selects the |r|^2 slot)
-static void sloppy_cg_update(Lattice &L, float *x, float *r, SField p, SField q, int par) {
-  YG_SPINOR_DISPATCH(L.sl_prec, {
-    launch_pdl(k_s_cg_update<SP>, L.sl_grid_vec, 256, L.stream, (float2 *)x, (float2 *)r, p.data, p.norm, q.data,
-               q.norm, dscal(L), part_pq(L), L.sl_grid_nrm, part_r(L), par, (int)L.Vh);
+// q = Hphi(t) with the CG update fused into its last step: x += alpha p, r -= alpha q and the
+// partials of the new |r|^2 (par = iteration parity, selecting the |r|^2 slot)
+static void sloppy_hphi_cg(Lattice &L, SField t, SField tmp, float *x, float *r, SField p, int par) {
+  SHopArgs a{};
+  a.g = L.g;
+  a.U = L.sl_links.p;
+  a.C = L.sl_clover.p;
+  a.Cn = L.sl_cnorm.as<float>();
+  a.src = t.data; a.src_norm = t.norm;
+  a.dst = tmp.data; a.dst_norm = tmp.norm;
+  a.coeff = 0.5f;
+  a.lo = (int)L.Vh; a.n = (int)L.Vh;
+  SHopArgs b = a;
+  b.src = tmp.data; b.src_norm = tmp.norm;
+  b.src2 = t.data; b.src2_norm = t.norm;
+  b.dst = nullptr; b.dst_norm = nullptr;
+  b.coeff = -0.5f;
+  b.lo = 0;
+  SCgArgs c{};
+  c.x = reinterpret_cast<float2 *>(x);
+  c.r = reinterpret_cast<float2 *>(r);
+  c.p = p.data; c.pn = p.norm;
+  c.scal = dscal(L);
+  c.part_pq = part_pq(L);
+  c.n_pq = L.sl_grid_nrm;
+  c.part_r = part_r(L);
+  c.par = par;
+  YG_SLOPPY_DISPATCH(L.sl_prec, L.sl_lfmt, L.sl_cfmt, L.sl_reals, {
+    launch_pdl(k_shop<SP, SL, SC, SK, 1, 0>, nblk(a.n, 128), 128, L.stream, a);
+    YG_LAUNCHED();
+    launch_pdl(k_shop_cg<SP, SL, SC, SK>, L.sl_grid_cg, 128, L.stream, b, c);
     YG_LAUNCHED();
   });
+  L.mvm += 2;
 }
 
-static void sloppy_xpay(Lattice &L, SField p, const float *r, int par, double *hist, unsigned long long iter) {
+static void sloppy_xpay(Lattice &L, SField p, const float *r, int par, double *hist) {
   YG_SPINOR_DISPATCH(L.sl_prec, {
-    launch_pdl(k_s_xpay<SP>, L.sl_grid_vec, 256, L.stream, p.data, p.norm, dscal(L), part_r(L), L.sl_grid_vec, par,
-               hist, hist_seq(L), iter, (const float2 *)r, (int)L.Vh);
+    launch_pdl(k_s_xpay<SP>, L.sl_grid_vec, 256, L.stream, p.data, p.norm, dscal(L), part_r(L), L.sl_grid_cg, par,
+               hist, hist_seq(L), (const float2 *)r, (int)L.Vh);
     YG_LAUNCHED();
   });
 }
@@ -634,9 +703,66 @@ static void set_scalar(Lattice &L, int i, double v) {
   YG_LAUNCHED();
 }
 
+// CUDA graphs of the inner iteration (YG_CUDA_GRAPH=0 turns them off)
+static bool use_graphs() {
+  const char *e = std::getenv("YG_CUDA_GRAPH");
+  return !(e && e[0] == '0');
+}
+
+// The two parities of the inner iteration as instantiated graphs.  Capture records the
+// launches without running them: the launch counter and the MVM counter are restored after
+// the capture and advanced at every replay instead.  A capture that fails (a driver that
+// cannot record a launch form) is ended and discarded, and the solver issues the launches
+// one by one as without graphs.
+struct IterGraphs {
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  long launches[2] = {0, 0};
+  int mvm[2] = {0, 0};
+  bool failed = false;
+  bool ready() const { return !failed && exec[0] && exec[1]; }
+  template <typename F>
+  void capture(Lattice &L, int par, F &&issue) {
+    if (failed) return;
+    const long n0 = g_launch_count.load();
+    const int m0 = L.mvm;
+    cudaGraph_t g = nullptr;
+    bool ok = cudaStreamBeginCapture(L.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      try {
+        issue();
+      } catch (const Error &) {
+        ok = false;
+      }
+      ok = (cudaStreamEndCapture(L.stream, &g) == cudaSuccess) && ok && g;
+    }
+    launches[par] = g_launch_count.load() - n0;
+    g_launch_count -= launches[par];
+    mvm[par] = L.mvm - m0;
+    L.mvm = m0;
+    if (ok) ok = cudaGraphInstantiate(&exec[par], g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+    if (!ok) {
+      failed = true;
+      (void)cudaGetLastError();              // the failed capture's error is not sticky
+    }
+  }
+  void launch(Lattice &L, int par) {
+    YG_CUDA(cudaGraphLaunch(exec[par], L.stream));
+    g_launch_count += launches[par];
+    L.mvm += mvm[par];
+  }
+  ~IterGraphs() {
+    for (cudaGraphExec_t &e : exec)
+      if (e) cudaGraphExecDestroy(e);
+  }
+};
+
 // Mixed-precision CG on Hphi_sq with the compressed inner operator.  x and r of the inner
-// iterations are FP32, p and A p are in the inner storage format.  alpha and beta live on
-// the device, so an inner iteration is six launches and no host synchronisation; the host
+// iterations are FP32, p and Hphi p are in the inner storage format, A p = Hphi Hphi p stays
+// in registers: the x and r updates are the epilogue of the operator's last step.  alpha
+// and beta live on the device, so an inner iteration is five launches (four operator steps
+// and p = r + beta p), replayed as one CUDA graph per iteration, and no host
+// synchronisation; the host
 // reads each iteration's |r|^2 one iteration late (while the next one runs) and then
 // decides on a reliable update: b - A x is recomputed with the FP64 operator whenever the
 // iterated |r| fell below delta times its value at the last update, r is replaced by it
@@ -663,9 +789,10 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int 
   double *r = L.scratch_field(3), *Ax = L.scratch_field(4), *xd = L.scratch_field(5);
   float *fr = reinterpret_cast<float *>(L.scratch_field(40));
   float *fx = reinterpret_cast<float *>(L.scratch_field(42));
-  SField p = sfield(L, 41), q = sfield(L, 43), t = sfield(L, 44), o = sfield(L, 45);
+  SField p = sfield(L, 41), t = sfield(L, 44), o = sfield(L, 45);
   volatile double *hist = L.sl_hist;
   *hist_seq(L) = 0;                 // no GPU work of this lattice is in flight here
+  set_scalar(L, S_ITER, 0.0);       // the device's count of finished inner iterations
 
   auto residual = [&]() {           // r = b - A x in FP64, returns |r|^2
     blas_copy(L, xd, x);
@@ -700,16 +827,31 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int 
     double min_cycle = rr;
     int since_min = 0;
     stall = 0;
+    // an inner iteration is the same five launches with the same arguments for every
+    // iteration of one parity; with graphs on, each parity is captured once per inner run and
+    // replayed as one CUDA graph launch
+    IterGraphs graphs;
+    if (use_graphs()) {
+      for (int gp = 0; gp < 2; gp++)
+        graphs.capture(L, gp, [&] {
+          sloppy_hphi(L, t, p, o, true);
+          sloppy_hphi_cg(L, t, o, fx, fr, p, gp);
+          sloppy_xpay(L, p, fr, gp, const_cast<double *>(hist) + gp);
+        });
+    }
     while (true) {
       if (par.maxiter > 0 && it >= par.maxiter) {
         d_add_f(L, x, fx, cnt);     // keep the progress of the inner iterations
         return YG_MAXITER;
       }
       int slot = it & 1;
-      sloppy_hphi(L, t, p, o, true);
-      sloppy_hphi(L, q, t, o, false);
-      sloppy_cg_update(L, fx, fr, p, q, slot);
-      sloppy_xpay(L, p, fr, slot, const_cast<double *>(hist) + slot, (unsigned long long)it + 1);
+      if (graphs.ready()) {
+        graphs.launch(L, slot);
+      } else {
+        sloppy_hphi(L, t, p, o, true);
+        sloppy_hphi_cg(L, t, o, fx, fr, p, slot);
+        sloppy_xpay(L, p, fr, slot, const_cast<double *>(hist) + slot);
+      }
       it++;
       if (!pending) { pending = true; continue; }
       // the previous iteration's |r|^2, read while this one runs

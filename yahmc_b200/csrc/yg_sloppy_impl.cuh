@@ -249,11 +249,11 @@ struct SHopArgs {
 // ------------------------------------------------------------------ device-side reductions
 // Device scalars of the inner CG (sl_scal): |r|^2 in two slots that alternate between
 // iterations (iteration k reads slot k&1 and writes slot (k+1)&1, so no block overwrites
-// a value another block of the same launch still reads), and alpha, <p, A p> for
-// inspection.  Grid sums are two-phase: a producer launch stores one partial per block,
+// a value another block of the same launch still reads), alpha, <p, A p> for inspection,
+// and the count of finished inner iterations (S_ITER, the value the host polls).  Grid sums are two-phase: a producer launch stores one partial per block,
 // and every block of the consumer launch adds all of them in index order, so the result
 // is deterministic and no block ever waits for another.
-enum { S_RR0 = 0, S_RR1 = 1, S_ALPHA = 2, S_PQ = 3, S_WORDS = 8 };
+enum { S_RR0 = 0, S_RR1 = 1, S_ALPHA = 2, S_PQ = 3, S_ITER = 4, S_WORDS = 8 };
 
 // block total of v, returned to every thread (blockDim a multiple of 32, at most 1024)
 __device__ __forceinline__ double block_total(double v) {

@@ -87,14 +87,22 @@ int cg(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters) {
 
 // No reference counterpart: independent cg_inverter solves on lattices of any sizes at once.
 // A small lattice's CG is bound by kernel and reduction latency and leaves most of the GPU
-// idle, so each lattice's solve runs in its own host thread on the lattice's own stream and
-// the solves overlap on the device.  Every solve is the single-lattice cg, so results and
-// iteration counts are those of one-at-a-time calls.  Returns the worst status.
-int cg_lattices(int n, Lattice *const *L, const yg_inv_par *par, double *const *xs, double *const *bs, int *iters) {
+// idle.  Hphi_sq solves on even-odd lattices of one representation dimension d (2, 3, 4, 6;
+// all with or all without a clover term; no open/SF boundaries) run as one persistent kernel
+// (yg_batch.cu); any other mix runs each lattice's single-lattice cg in its own host thread
+// on the lattice's own stream, so the solves overlap on the device.  Iteration counts are
+// those of one-at-a-time calls (the persistent kernel's reductions add in another order, so
+// a count can differ by one where |r|^2 lands within rounding of the stopping threshold).
+// Returns the worst status; *persistent (when given) tells which path ran.
+int cg_lattices(int n, Lattice *const *L, const yg_inv_par *par, double *const *xs, double *const *bs, int *iters,
+                long long wait_cycles, int *persistent) {
   if (n < 1 || n > 64) throw Error(YG_ERR_ARG, "1..64 lattices");
   for (int i = 0; i < n; i++)
     for (int j = 0; j < i; j++)
       if (L[i] == L[j]) throw Error(YG_ERR_ARG, "each lattice may appear once (its scratch fields are per solve)");
+  const bool batch = batch_eligible(n, L, par);
+  if (persistent) *persistent = batch ? 1 : 0;
+  if (batch) return cg_lattices_persistent(n, L, par, xs, bs, iters, wait_cycles);
   int dev = 0;
   YG_CUDA(cudaGetDevice(&dev));
   std::vector<int> st(n, YG_OK);
