@@ -13,9 +13,10 @@
 // Every system keeps its own fields in the single-system formats (FP16 spinors with per-site
 // norms for p, Hphi p and the intermediates; FP32 x and r; A p = Hphi Hphi p is never stored:
 // x += alpha p, r -= alpha A p and the |r|^2 partials are the epilogue of the operator's
-// last step), its own device scalars (|r|^2 in
-// two alternating slots, alpha, beta), and the single-system rules: reliable updates with
-// the FP64 operator when |r| has fallen by delta or stagnates, a stop on the TRUE FP64
+// last step), its own device scalars (|r|^2 in two alternating slots, alpha, beta), its own
+// mass (the packed clover blocks are per launch slot, so the HMC and Hasenbusch monomials'
+// solves at m + dm and m share the launches), and the single-system rules: reliable updates
+// with the FP64 operator when |r| has fallen by delta or stagnates, a stop on the TRUE FP64
 // residual |b - A x|^2 < prec |b|^2, and a fall-back to the FP64 CG on a stall.  All
 // reductions are deterministic: per-block partials summed in index order by one warp per
 // system.  The host reads each iteration's |r|^2 values one iteration late from mapped
