@@ -463,12 +463,33 @@ def run_mshift(a):
     def apart():
         return [lat.cg_mshift("Hphi_sq", mass, prec, shifts[k:k + 1], xs[k:k + 1], b) for k in range(len(shifts))]
 
+    def true_residuals():
+        out = []
+        bn = lat.spinor_sqnorm(b)
+        for s_, x in zip(shifts, xs):
+            xc, r = lat.field(), lat.field()
+            lat.spinor_copy(xc, x)
+            lat.Hphi_sq(mass, r, xc)
+            lat.spinor_mulr_add_assign(r, float(s_), x)
+            lat.spinor_sub_assign(r, b)
+            out.append(lat.spinor_sqnorm(r) / bn)
+        return out
+
     t1, it1 = ev_time(together)
+    res1 = true_residuals()
+    x_together = [lat.download(x) for x in xs]
     t2, it2 = ev_time(apart)
+    res2 = true_residuals()
+    diff = max(float(np.abs(lat.download(x) - xt).max() / np.abs(xt).max()) for x, xt in zip(xs, x_together))
+    valid = max(res1 + res2) < 10 * prec
     print(json.dumps({"workload": "12-shift CG on Hphi_sq + s, SU(2) adjoint 48x24x24x24 even-odd Wilson-clover, "
                                   "Haar-random links", "shifts": list(shifts), "mass": mass, "prec_squared": prec,
                       "cg_mshift_ms": t1, "cg_mshift_iterations": it1, "one_shift_at_a_time_ms": t2,
-                      "one_shift_iterations": it2, "speedup": t2 / t1}))
+                      "one_shift_iterations": it2, "speedup": t2 / t1,
+                      "true_residuals_together": res1, "true_residuals_apart": res2,
+                      "max_rel_diff_of_solutions": diff,
+                      "valid": bool(valid), "validity": "every true residual below 10 x prec (the multishift "
+                                                        "stops on recursive residuals)"}))
 
 
 HMC_CFG = """[lattice]

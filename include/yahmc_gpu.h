@@ -212,8 +212,8 @@ int yg_cg_inverter_multi(yg_lattice *lat, const yg_inv_par *par, int nrhs, doubl
  * group of blocks per lattice, sized by its volume, runs the lattice's whole CG loop on the
  * device with bounded barriers.  Other mixes run a host thread and the lattice's own stream
  * per solve.  Results and iteration counts are those of separate yg_cg_inverter calls (to
- * rounding); returns the worst status.  The calling thread's current device is used for all
- * of them. */
+ * rounding); returns the worst status.  Every lattice must have been created on the calling
+ * thread's current device (YG_ERR_ARG otherwise). */
 int yg_cg_inverter_lattices(int n, yg_lattice *const *lats, const yg_inv_par *pars, double *const *xs,
                             double *const *bs, int *iters);
 /* As yg_cg_inverter_lattices, with the persistent kernel's barrier wait limit in GPU clock

@@ -114,9 +114,11 @@ __device__ __noinline__ void step(const HopArgs<double> &a, int t) {
 }
 
 // CLOV = 1: A_oo^-1 from the packed inverse blocks and A_ee from the clover term (d <= 6);
-// CLOV = 0: no clover term, A_oo = 1 and the (4+m)^2 diagonal
+// CLOV = 0: no clover term, A_oo = 1 and the (4+m)^2 diagonal.  Registers are capped for 3
+// resident CTAs per SM, so that a 16^4 lattice's group covers its 32768 even sites in one
+// pass of the grid (one site per thread).
 template <int D, int CLOV>
-__global__ void __launch_bounds__(kThreads) k_cg_batch(const BLat *lats, int n, double *part_pq, double *part_rr,
+__global__ void __launch_bounds__(kThreads, 3) k_cg_batch(const BLat *lats, int n, double *part_pq, double *part_rr,
                                                        unsigned *sync, int *err, BOut *out, long long limit) {
   constexpr int E1 = CLOV ? EPI_CLOVPK : EPI_PLAIN, E2 = CLOV ? EPI_CLOVADD : EPI_AXPY;
   int li = 0;

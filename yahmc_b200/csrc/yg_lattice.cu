@@ -284,6 +284,7 @@ Lattice *lattice_create(const yg_params &p) {
     // the lattice's own stream; a blocking stream, so work on the legacy default stream
     // (and events recorded there) still orders with it
     YG_CUDA(cudaStreamCreateWithFlags(&L->stream, cudaStreamDefault));
+    YG_CUDA(cudaGetDevice(&L->device));
     L->p = p;
     L->d = d;
     L->nc = p.nc;

@@ -54,6 +54,7 @@ struct Lattice {
   long V = 0, Vh = 0;
   cudaStream_t stream = 0;
   int mvm = 0;
+  int device = 0;          // the CUDA device the lattice was created on
 
   DevBuf fund;      // fundamental links, 4 x N x N per site        (gfield_fund)
   DevBuf fund_backup;  // gauge_field_backup copy of fund
@@ -94,6 +95,7 @@ struct Lattice {
   double sl_mass = 0;
   bool sl_valid = false;
   int sl_tuned_reals = 0;  // link format of the default mixed solve (tune_inner_links), 0 = not yet
+  int sl_shape = 0;        // block shape of the inner step-1 hop (tune_inner_links), 0 = the default
   DevBuf sl_part;      // per-block partial sums of the device-scalar reductions
   int sl_grid_nrm = 0; // blocks of the hop that forms <p, A p> (resident-grid size)
   int sl_grid_vec = 0; // blocks of the inner vector kernels

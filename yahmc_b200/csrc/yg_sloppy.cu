@@ -147,8 +147,10 @@ __device__ __forceinline__ float shop_site(const SHopArgs &a, int id, const Site
 // NRM = 1 (first Hphi of a CG iteration, t = Hphi p): also the per-block partials of
 // <p, A p> = |t|^2 (Hphi is Hermitian and A = Hphi^2); a grid-stride loop over a grid of
 // resident blocks keeps the number of partials small
-template <int P, int LP, int CP, int K, int STEP, int NRM>
-__global__ void __launch_bounds__(128) k_shop(SHopArgs a) {
+// TPB x MINB: the block shape (threads per block, resident blocks per SM the register
+// allocation is cut for) that the tuner chooses for the plain step-1 launches
+template <int P, int LP, int CP, int K, int STEP, int NRM, int TPB = 128, int MINB = 1>
+__global__ void __launch_bounds__(TPB, MINB) k_shop(SHopArgs a) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (!NRM) {
     SiteNbr n;
@@ -596,6 +598,25 @@ static void launch_pdl(void (*kern)(KArgs...), int grid, int block, cudaStream_t
   YG_CUDA(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
 }
 
+// Block shapes of the step-1 hop the tuner chooses among (threads per block, minimum resident
+// blocks per SM): the default, a register cap for 6 blocks of 128, 256-thread blocks capped
+// for 3 per SM, 64-thread blocks.  Only the default storage (FP16 spinors, FP32 matrices) has
+// the variants; other formats always use the first.
+constexpr int kShapes[4][2] = {{128, 1}, {128, 6}, {256, 3}, {64, 1}};
+
+template <int SP, int SL, int SC, int SK>
+static void launch_step1(int shape, cudaStream_t s, const SHopArgs &a) {
+  if constexpr (SP == 16 && SL == 32 && SC == 32) {
+    switch (shape) {
+      case 1: launch_pdl(k_shop<SP, SL, SC, SK, 1, 0, 128, 6>, nblk(a.n, 128), 128, s, a); return;
+      case 2: launch_pdl(k_shop<SP, SL, SC, SK, 1, 0, 256, 3>, nblk(a.n, 256), 256, s, a); return;
+      case 3: launch_pdl(k_shop<SP, SL, SC, SK, 1, 0, 64, 1>, nblk(a.n, 64), 64, s, a); return;
+      default: break;
+    }
+  }
+  launch_pdl(k_shop<SP, SL, SC, SK, 1, 0>, nblk(a.n, 128), 128, s, a);
+}
+
 static double *dscal(Lattice &L) { return L.sl_scal.as<double>(); }
 static unsigned long long *hist_seq(Lattice &L) { return reinterpret_cast<unsigned long long *>(L.sl_hist + 4); }
 static double *part_pq(Lattice &L) { return L.sl_part.as<double>(); }
@@ -621,7 +642,7 @@ static void sloppy_hphi(Lattice &L, SField dst, SField src, SField tmp, bool nrm
   b.lo = 0;
   b.part = part_pq(L);
   YG_SLOPPY_DISPATCH(L.sl_prec, L.sl_lfmt, L.sl_cfmt, L.sl_reals, {
-    launch_pdl(k_shop<SP, SL, SC, SK, 1, 0>, nblk(a.n, 128), 128, L.stream, a);
+    launch_step1<SP, SL, SC, SK>(L.sl_shape, L.stream, a);
     YG_LAUNCHED();
     if (nrm) launch_pdl(k_shop<SP, SL, SC, SK, 2, 1>, L.sl_grid_nrm, 128, L.stream, b);
     else launch_pdl(k_shop<SP, SL, SC, SK, 2, 0>, nblk(b.n, 128), 128, L.stream, b);
@@ -658,7 +679,7 @@ static void sloppy_hphi_cg(Lattice &L, SField t, SField tmp, float *x, float *r,
   c.part_r = part_r(L);
   c.par = par;
   YG_SLOPPY_DISPATCH(L.sl_prec, L.sl_lfmt, L.sl_cfmt, L.sl_reals, {
-    launch_pdl(k_shop<SP, SL, SC, SK, 1, 0>, nblk(a.n, 128), 128, L.stream, a);
+    launch_step1<SP, SL, SC, SK>(L.sl_shape, L.stream, a);
     YG_LAUNCHED();
     launch_pdl(k_shop_cg<SP, SL, SC, SK>, L.sl_grid_cg, 128, L.stream, b, c);
     YG_LAUNCHED();
@@ -932,7 +953,8 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int 
 // with CUDA events on the lattice's stream, and the compulsory bytes one launch moves
 // (neighbour spinors read once, links, clover blocks, output spinor).
 // mean time of the inner operator's step-1 hop (FP16 spinors, FP32 matrices, `reals` per link)
-static void hop_time(Lattice &L, double mass, int reals, int reps, double *ms, double *bytes) {
+// in block shape `shape`
+static void hop_time(Lattice &L, double mass, int reals, int reps, double *ms, double *bytes, int shape) {
   if (reps < 1) throw Error(YG_ERR_ARG, "reps must be >= 1");
   ensure_sloppy(L, mass, 16, reals, 32, 32);
   SField src = sfield(L, 41), dst = sfield(L, 44);
@@ -950,9 +972,9 @@ static void hop_time(Lattice &L, double mass, int reals, int reps, double *ms, d
   YG_CUDA(cudaEventCreate(&e0));
   YG_CUDA(cudaEventCreate(&e1));
   YG_SLOPPY_DISPATCH(L.sl_prec, L.sl_lfmt, L.sl_cfmt, L.sl_reals, {
-    for (int w = 0; w < 3; w++) launch_pdl(k_shop<SP, SL, SC, SK, 1, 0>, nblk(a.n, 128), 128, L.stream, a);
+    for (int w = 0; w < 3; w++) launch_step1<SP, SL, SC, SK>(shape, L.stream, a);
     YG_CUDA(cudaEventRecord(e0, L.stream));
-    for (int r = 0; r < reps; r++) launch_pdl(k_shop<SP, SL, SC, SK, 1, 0>, nblk(a.n, 128), 128, L.stream, a);
+    for (int r = 0; r < reps; r++) launch_step1<SP, SL, SC, SK>(shape, L.stream, a);
     YG_CUDA(cudaEventRecord(e1, L.stream));
     for (int r = 0; r < reps + 3; r++) YG_LAUNCHED();
   });
@@ -968,15 +990,19 @@ static void hop_time(Lattice &L, double mass, int reals, int reps, double *ms, d
   *bytes = (double)L.Vh * (spinor + 8.0 * link + clov + spinor);
 }
 
+// the step-1 hop of the default solve in the lattice's tuned block shape
 void inner_hop_profile(Lattice &L, double mass, int reps, double *ms, double *bytes) {
-  hop_time(L, mass, (L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL) ? 12 : 18, reps, ms, bytes);
+  const int reals = L.sl_tuned_reals ? L.sl_tuned_reals : (L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL) ? 12 : 18;
+  hop_time(L, mass, reals, reps, ms, bytes, L.sl_shape);
 }
 
-// No reference counterpart: the link format of the default mixed solve chosen by measurement.
-// The candidates carry FP32 matrices (the formats whose rounding leaves the operator accurate
-// enough on rough fields): 18 reals always, 12 for SU(3) fundamental links, 8 in addition on
-// periodic / antiperiodic lattices.  Each is timed over 20 step-1 hops on this lattice; the
-// fastest is kept for the lattice (ms[0..2] = 18, 12, 8 real, 0 where not a candidate).
+// No reference counterpart: the link format and block shape of the default mixed solve chosen
+// by measurement.  The link candidates carry FP32 matrices (the formats whose rounding leaves
+// the operator accurate enough on rough fields): 18 reals always, 12 for SU(3) fundamental
+// links, 8 in addition on periodic / antiperiodic lattices.  Each is timed over 20 step-1 hops
+// on this lattice in the default block shape; then the fastest format is timed in every block
+// shape of kShapes.  Both choices are kept for the lattice (ms[0..2] = 18, 12, 8 real, 0 where
+// not a candidate).  YG_TUNE_LOG prints the block-shape timings.
 int tune_inner_links(Lattice &L, double mass, double *ms) {
   const bool su3 = L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL;
   const bool pbc = L.p.bc == YG_BC_PERIODIC || L.p.bc == YG_BC_ANTIPERIODIC;
@@ -987,12 +1013,23 @@ int tune_inner_links(Lattice &L, double mass, double *ms) {
   for (int k = 0; k < 3; k++) {
     double t = 0.0, bytes = 0.0;
     if (ok[k]) {
-      hop_time(L, mass, cand[k], 20, &t, &bytes);
+      hop_time(L, mass, cand[k], 20, &t, &bytes, 0);
       if (best_ms == 0.0 || t < best_ms) { best_ms = t; best = cand[k]; }
     }
     if (ms) ms[k] = t;
   }
+  int shape = 0;
+  double shape_ms = best_ms;
+  for (int v = 1; v < 4; v++) {
+    double t = 0.0, bytes = 0.0;
+    hop_time(L, mass, best, 20, &t, &bytes, v);
+    if (t < shape_ms) { shape_ms = t; shape = v; }
+    if (std::getenv("YG_TUNE_LOG"))
+      fprintf(stderr, "yg tune inner hop: %d-real links, %d threads x %d blocks/SM: %.4f ms (default %.4f)\n",
+              best, kShapes[v][0], kShapes[v][1], t, best_ms);
+  }
   L.sl_tuned_reals = best;
+  L.sl_shape = shape;
   return best;
 }
 

@@ -100,6 +100,11 @@ int cg_lattices(int n, Lattice *const *L, const yg_inv_par *par, double *const *
   for (int i = 0; i < n; i++)
     for (int j = 0; j < i; j++)
       if (L[i] == L[j]) throw Error(YG_ERR_ARG, "each lattice may appear once (its scratch fields are per solve)");
+  int cur = 0;
+  YG_CUDA(cudaGetDevice(&cur));
+  for (int i = 0; i < n; i++)
+    if (L[i]->device != cur)
+      throw Error(YG_ERR_ARG, "every lattice must belong to the calling thread's current device");
   const bool batch = batch_eligible(n, L, par);
   if (persistent) *persistent = batch ? 1 : 0;
   if (batch) return cg_lattices_persistent(n, L, par, xs, bs, iters, wait_cycles);
