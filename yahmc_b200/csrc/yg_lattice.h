@@ -95,7 +95,8 @@ struct Lattice {
   double sl_mass = 0;
   bool sl_valid = false;
   int sl_tuned_reals = 0;  // link format of the default mixed solve (tune_inner_links), 0 = not yet
-  int sl_shape = 0;        // block shape of the inner step-1 hop (tune_inner_links), 0 = the default
+  int sl_shape = 0;        // block shape of the inner step-1 hop (tune_shape), 0 = the default
+  int sl_shape_reals = 0;  // link reals sl_shape was tuned for, 0 = not yet
   DevBuf sl_part;      // per-block partial sums of the device-scalar reductions
   int sl_grid_nrm = 0; // blocks of the hop that forms <p, A p> (resident-grid size)
   int sl_grid_vec = 0; // blocks of the inner vector kernels

@@ -147,10 +147,8 @@ __device__ __forceinline__ float shop_site(const SHopArgs &a, int id, const Site
 // NRM = 1 (first Hphi of a CG iteration, t = Hphi p): also the per-block partials of
 // <p, A p> = |t|^2 (Hphi is Hermitian and A = Hphi^2); a grid-stride loop over a grid of
 // resident blocks keeps the number of partials small
-// TPB x MINB: the block shape (threads per block, resident blocks per SM the register
-// allocation is cut for) that the tuner chooses for the plain step-1 launches
-template <int P, int LP, int CP, int K, int STEP, int NRM, int TPB = 128, int MINB = 1>
-__global__ void __launch_bounds__(TPB, MINB) k_shop(SHopArgs a) {
+template <int P, int LP, int CP, int K, int STEP, int NRM>
+__global__ void __launch_bounds__(128) k_shop(SHopArgs a) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (!NRM) {
     SiteNbr n;
@@ -169,6 +167,18 @@ __global__ void __launch_bounds__(TPB, MINB) k_shop(SHopArgs a) {
   }
   n2 = block_total(n2);
   if (threadIdx.x == 0) a.part[blockIdx.x] = n2;
+  griddep_launch();
+}
+
+// The plain step 1 in another block shape (TPB threads per block, registers cut for MINB
+// resident blocks per SM), for the tuner to choose; one site per thread as k_shop.
+template <int P, int LP, int CP, int K, int TPB, int MINB>
+__global__ void __launch_bounds__(TPB, MINB) k_shop_shaped(SHopArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  SiteNbr n;
+  if (t < a.n) site_nbr(n, a.g, a.lo + t);
+  griddep_wait();
+  if (t < a.n) shop_site<P, LP, CP, K, 1>(a, a.lo + t, n);
   griddep_launch();
 }
 
@@ -598,19 +608,20 @@ static void launch_pdl(void (*kern)(KArgs...), int grid, int block, cudaStream_t
   YG_CUDA(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
 }
 
-// Block shapes of the step-1 hop the tuner chooses among (threads per block, minimum resident
-// blocks per SM): the default, a register cap for 6 blocks of 128, 256-thread blocks capped
-// for 3 per SM, 64-thread blocks.  Only the default storage (FP16 spinors, FP32 matrices) has
-// the variants; other formats always use the first.
-constexpr int kShapes[4][2] = {{128, 1}, {128, 6}, {256, 3}, {64, 1}};
+// Block shapes of the step-1 hop the tuner chooses among (threads per block, resident blocks
+// per SM the registers are cut for; 0 = the compiler's own choice): the default, 128-thread
+// blocks cut for 6 per SM, 256-thread blocks cut for 3, 64-thread blocks cut for 10.  Only the
+// default storage (FP16 spinors, FP32 matrices) has the variants; other formats always use
+// the first.
+constexpr int kShapes[4][2] = {{128, 0}, {128, 6}, {256, 3}, {64, 10}};
 
 template <int SP, int SL, int SC, int SK>
 static void launch_step1(int shape, cudaStream_t s, const SHopArgs &a) {
   if constexpr (SP == 16 && SL == 32 && SC == 32) {
     switch (shape) {
-      case 1: launch_pdl(k_shop<SP, SL, SC, SK, 1, 0, 128, 6>, nblk(a.n, 128), 128, s, a); return;
-      case 2: launch_pdl(k_shop<SP, SL, SC, SK, 1, 0, 256, 3>, nblk(a.n, 256), 256, s, a); return;
-      case 3: launch_pdl(k_shop<SP, SL, SC, SK, 1, 0, 64, 1>, nblk(a.n, 64), 64, s, a); return;
+      case 1: launch_pdl(k_shop_shaped<SP, SL, SC, SK, 128, 6>, nblk(a.n, 128), 128, s, a); return;
+      case 2: launch_pdl(k_shop_shaped<SP, SL, SC, SK, 256, 3>, nblk(a.n, 256), 256, s, a); return;
+      case 3: launch_pdl(k_shop_shaped<SP, SL, SC, SK, 64, 10>, nblk(a.n, 64), 64, s, a); return;
       default: break;
     }
   }
@@ -798,11 +809,15 @@ namespace yg {
 
 int cg(Lattice &L, const yg_inv_par &par, double *x, double *b, int *iters);
 
+static void tune_shape(Lattice &L, double mass, int reals);
+
 int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int lfmt, int cfmt, double delta,
                     double *x, double *b, yg_solve_stats *st, bool escalate) {
   auto t0 = std::chrono::steady_clock::now();
   if (par.op != YG_OP_HPHI_SQ) throw Error(YG_ERR_ARG, "cg_mixed solves Hphi_sq systems");
   if (!(delta > 0.0 && delta < 1.0)) throw Error(YG_ERR_ARG, "reliable-update delta must lie in (0,1)");
+  if (prec == 16 && matrix_format(lfmt, prec) == ST_F32 && matrix_format(cfmt, prec) == ST_F32 && reals != 8)
+    tune_shape(L, par.mass, reals);         // the block shape of the step-1 hop, once per lattice
   ensure_sloppy(L, par.mass, prec, reals, lfmt, cfmt);
   long lo, n;
   L.view_range(YG_VIEW_DEFAULT, lo, n);
@@ -990,6 +1005,25 @@ static void hop_time(Lattice &L, double mass, int reals, int reps, double *ms, d
   *bytes = (double)L.Vh * (spinor + 8.0 * link + clov + spinor);
 }
 
+// The block shape of the step-1 hop for FP16 spinors, FP32 matrices and `reals` link reals:
+// each shape of kShapes timed over 20 hops on this lattice, the fastest kept (once per
+// lattice and link format).  YG_TUNE_LOG prints the timings.
+static void tune_shape(Lattice &L, double mass, int reals) {
+  if (L.sl_shape_reals == reals) return;
+  int shape = 0;
+  double best_ms = 0.0;
+  for (int v = 0; v < 4; v++) {
+    double t = 0.0, bytes = 0.0;
+    hop_time(L, mass, reals, 20, &t, &bytes, v);
+    if (v == 0 || t < best_ms) { best_ms = t; shape = v; }
+    if (std::getenv("YG_TUNE_LOG"))
+      fprintf(stderr, "yg tune inner hop: %d-real links, %d threads/block, %d blocks/SM: %.4f ms\n", reals,
+              kShapes[v][0], kShapes[v][1], t);
+  }
+  L.sl_shape = shape;
+  L.sl_shape_reals = reals;
+}
+
 // the step-1 hop of the default solve in the lattice's tuned block shape
 void inner_hop_profile(Lattice &L, double mass, int reps, double *ms, double *bytes) {
   const int reals = L.sl_tuned_reals ? L.sl_tuned_reals : (L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL) ? 12 : 18;
@@ -1018,18 +1052,8 @@ int tune_inner_links(Lattice &L, double mass, double *ms) {
     }
     if (ms) ms[k] = t;
   }
-  int shape = 0;
-  double shape_ms = best_ms;
-  for (int v = 1; v < 4; v++) {
-    double t = 0.0, bytes = 0.0;
-    hop_time(L, mass, best, 20, &t, &bytes, v);
-    if (t < shape_ms) { shape_ms = t; shape = v; }
-    if (std::getenv("YG_TUNE_LOG"))
-      fprintf(stderr, "yg tune inner hop: %d-real links, %d threads x %d blocks/SM: %.4f ms (default %.4f)\n",
-              best, kShapes[v][0], kShapes[v][1], t, best_ms);
-  }
   L.sl_tuned_reals = best;
-  L.sl_shape = shape;
+  tune_shape(L, mass, best);
   return best;
 }
 
