@@ -47,6 +47,8 @@ struct ReprTables {
   double2 *itfund;   // NG x N x N generators of the fundamental representation
 };
 
+constexpr int kStep2Shapes = 3;   // register variants of the inner operator's step-2 kernels
+
 struct Lattice {
   yg_params p{};
   Geom g{};
@@ -98,9 +100,13 @@ struct Lattice {
   int sl_shape = 0;        // block shape of the inner step-1 hop (tune_shape), 0 = the default
   int sl_shape_reals = 0;  // link reals sl_shape was tuned for, 0 = not yet
   DevBuf sl_part;      // per-block partial sums of the device-scalar reductions
-  int sl_grid_nrm = 0; // blocks of the hop that forms <p, A p> (resident-grid size)
   int sl_grid_vec = 0; // blocks of the inner vector kernels
-  int sl_grid_cg = 0;  // blocks of the last Schur step with the fused CG update (resident grid)
+  // resident-grid sizes of the two step-2 kernels of an inner iteration (the hop forming
+  // <p, A p>, and the last Schur step with the fused CG update) for each register variant,
+  // the variants in use (tuned), and where the |r|^2 partials start in sl_part
+  int sl_gnrm[kStep2Shapes] = {0, 0, 0}, sl_gcg[kStep2Shapes] = {0, 0, 0};
+  int sl_shape_n = 0, sl_shape_c = 0;
+  int sl_part_off = 0;
   DevBuf sl_scal;      // device scalars of the inner CG (rr, alpha, beta, ...) + completion counter
   double *sl_hist = nullptr;          // mapped pinned host ring of inner |r|^2 (written by the GPU)
   cudaEvent_t sl_ev[2] = {nullptr, nullptr};

@@ -148,7 +148,7 @@ __device__ __forceinline__ float shop_site(const SHopArgs &a, int id, const Site
 // <p, A p> = |t|^2 (Hphi is Hermitian and A = Hphi^2); a grid-stride loop over a grid of
 // resident blocks keeps the number of partials small
 template <int P, int LP, int CP, int K, int STEP, int NRM>
-__global__ void __launch_bounds__(128) k_shop(SHopArgs a) {
+__device__ __forceinline__ void shop_body(const SHopArgs &a) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (!NRM) {
     SiteNbr n;
@@ -168,6 +168,18 @@ __global__ void __launch_bounds__(128) k_shop(SHopArgs a) {
   n2 = block_total(n2);
   if (threadIdx.x == 0) a.part[blockIdx.x] = n2;
   griddep_launch();
+}
+
+template <int P, int LP, int CP, int K, int STEP, int NRM>
+__global__ void __launch_bounds__(128) k_shop(SHopArgs a) {
+  shop_body<P, LP, CP, K, STEP, NRM>(a);
+}
+
+// step 2 with the <p, A p> partials, registers cut for MINB resident blocks per SM (the tuner
+// chooses between this and the compiler's own register count)
+template <int P, int LP, int CP, int K, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_shop_nrm_min(SHopArgs a) {
+  shop_body<P, LP, CP, K, 2, 1>(a);
 }
 
 // The plain step 1 in another block shape (TPB threads per block, registers cut for MINB
@@ -198,7 +210,7 @@ struct SCgArgs {
 };
 
 template <int P, int LP, int CP, int K>
-__global__ void __launch_bounds__(128) k_shop_cg(SHopArgs a, SCgArgs c) {
+__device__ __forceinline__ void shop_cg_body(const SHopArgs &a, const SCgArgs &c) {
   griddep_wait();
   const double pq = sum_partials(c.part_pq, c.n_pq);
   const double alpha = c.scal[S_RR0 + c.par] / pq;
@@ -233,6 +245,16 @@ __global__ void __launch_bounds__(128) k_shop_cg(SHopArgs a, SCgArgs c) {
   acc = block_total(acc);
   if (threadIdx.x == 0) c.part_r[blockIdx.x] = acc;
   griddep_launch();
+}
+
+template <int P, int LP, int CP, int K>
+__global__ void __launch_bounds__(128) k_shop_cg(SHopArgs a, SCgArgs c) {
+  shop_cg_body<P, LP, CP, K>(a, c);
+}
+
+template <int P, int LP, int CP, int K, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_shop_cg_min(SHopArgs a, SCgArgs c) {
+  shop_cg_body<P, LP, CP, K>(a, c);
 }
 
 // ------------------------------------------------------------------ builds (once per gauge field / mass)
@@ -538,18 +560,30 @@ void ensure_sloppy(Lattice &L, double mass, int prec, int reals, int lfmt, int c
     return;
   {
     // resident-grid sizes of the reduction kernels, and room for their partials
-    int dev = 0, sms = 0, per_nrm = 0, per_vec = 0, per_cg = 0;
+    int dev = 0, sms = 0, per_vec = 0;
+    int per_nrm[kStep2Shapes] = {0, 0, 0}, per_cg[kStep2Shapes] = {0, 0, 0};
     YG_CUDA(cudaGetDevice(&dev));
     YG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     YG_SLOPPY_DISPATCH(prec, lfmt, cfmt, reals, {
-      YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_nrm, k_shop<SP, SL, SC, SK, 2, 1>, 128, 0));
-      YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_cg, k_shop_cg<SP, SL, SC, SK>, 128, 0));
+      YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_nrm[0], k_shop<SP, SL, SC, SK, 2, 1>, 128, 0));
+      YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_cg[0], k_shop_cg<SP, SL, SC, SK>, 128, 0));
+      if constexpr (SP == 16 && SL == 32 && SC == 32) {
+        YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_nrm[1], k_shop_nrm_min<SP, SL, SC, SK, 5>, 128, 0));
+        YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_nrm[2], k_shop_nrm_min<SP, SL, SC, SK, 6>, 128, 0));
+        YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_cg[1], k_shop_cg_min<SP, SL, SC, SK, 5>, 128, 0));
+        YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_cg[2], k_shop_cg_min<SP, SL, SC, SK, 6>, 128, 0));
+      }
       YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_vec, k_s_xpay<SP>, 256, 0));
     });
-    L.sl_grid_nrm = (int)std::min<long>((long)sms * std::max(per_nrm, 1), nblk(L.Vh, 128));
-    L.sl_grid_cg = (int)std::min<long>((long)sms * std::max(per_cg, 1), nblk(L.Vh, 128));
+    int gmax = 0;
+    for (int v = 0; v < kStep2Shapes; v++) {
+      L.sl_gnrm[v] = (int)std::min<long>((long)sms * std::max(per_nrm[v], 1), nblk(L.Vh, 128));
+      L.sl_gcg[v] = (int)std::min<long>((long)sms * std::max(per_cg[v], 1), nblk(L.Vh, 128));
+      gmax = std::max({gmax, L.sl_gnrm[v], L.sl_gcg[v]});
+    }
     L.sl_grid_vec = (int)std::min<long>((long)sms * std::max(per_vec, 1), nblk(L.Vh, 256));
-    L.sl_part.alloc(sizeof(double) * (size_t)(L.sl_grid_nrm + L.sl_grid_cg));
+    L.sl_part_off = gmax;
+    L.sl_part.alloc(sizeof(double) * (size_t)(2 * gmax));
   }
   const int K = reals / 2;
   L.sl_links.alloc((lfmt == ST_F32 ? 8 : 4) * (size_t)K * 4 * L.V);
@@ -614,6 +648,9 @@ static void launch_pdl(void (*kern)(KArgs...), int grid, int block, cudaStream_t
 // default storage (FP16 spinors, FP32 matrices) has the variants; other formats always use
 // the first.
 constexpr int kShapes[4][2] = {{128, 0}, {128, 6}, {256, 3}, {64, 10}};
+// the step-2 kernels (resident grids) tried with the compiler's registers, and cut for 5 and 6
+// resident blocks per SM
+constexpr int kStep2Min[kStep2Shapes] = {0, 5, 6};
 
 template <int SP, int SL, int SC, int SK>
 static void launch_step1(int shape, cudaStream_t s, const SHopArgs &a) {
@@ -631,7 +668,12 @@ static void launch_step1(int shape, cudaStream_t s, const SHopArgs &a) {
 static double *dscal(Lattice &L) { return L.sl_scal.as<double>(); }
 static unsigned long long *hist_seq(Lattice &L) { return reinterpret_cast<unsigned long long *>(L.sl_hist + 4); }
 static double *part_pq(Lattice &L) { return L.sl_part.as<double>(); }
-static double *part_r(Lattice &L) { return L.sl_part.as<double>() + L.sl_grid_nrm; }
+static double *part_r(Lattice &L) { return L.sl_part.as<double>() + L.sl_part_off; }
+
+// the step-2 shapes in use: the tuned ones for the default storage, the compiler's otherwise
+static bool default_storage(const Lattice &L) { return L.sl_prec == 16 && L.sl_lfmt == ST_F32 && L.sl_cfmt == ST_F32; }
+static int shape_nrm(const Lattice &L) { return default_storage(L) ? L.sl_shape_n : 0; }
+static int shape_cg(const Lattice &L) { return default_storage(L) ? L.sl_shape_c : 0; }
 
 // dst = Hphi(src) with the compressed operator; tmp receives the odd-site intermediate.
 // nrm: also the partials of |dst|^2 = <p, A p> (the first Hphi of a CG iteration)
@@ -655,8 +697,19 @@ static void sloppy_hphi(Lattice &L, SField dst, SField src, SField tmp, bool nrm
   YG_SLOPPY_DISPATCH(L.sl_prec, L.sl_lfmt, L.sl_cfmt, L.sl_reals, {
     launch_step1<SP, SL, SC, SK>(L.sl_shape, L.stream, a);
     YG_LAUNCHED();
-    if (nrm) launch_pdl(k_shop<SP, SL, SC, SK, 2, 1>, L.sl_grid_nrm, 128, L.stream, b);
-    else launch_pdl(k_shop<SP, SL, SC, SK, 2, 0>, nblk(b.n, 128), 128, L.stream, b);
+    if (nrm) {
+      const int v = shape_nrm(L);
+      const int grid = L.sl_gnrm[v];
+      if constexpr (SP == 16 && SL == 32 && SC == 32) {
+        if (v == 1) launch_pdl(k_shop_nrm_min<SP, SL, SC, SK, 5>, grid, 128, L.stream, b);
+        else if (v == 2) launch_pdl(k_shop_nrm_min<SP, SL, SC, SK, 6>, grid, 128, L.stream, b);
+        else launch_pdl(k_shop<SP, SL, SC, SK, 2, 1>, grid, 128, L.stream, b);
+      } else {
+        launch_pdl(k_shop<SP, SL, SC, SK, 2, 1>, grid, 128, L.stream, b);
+      }
+    } else {
+      launch_pdl(k_shop<SP, SL, SC, SK, 2, 0>, nblk(b.n, 128), 128, L.stream, b);
+    }
     YG_LAUNCHED();
   });
   L.mvm += 2;
@@ -686,13 +739,21 @@ static void sloppy_hphi_cg(Lattice &L, SField t, SField tmp, float *x, float *r,
   c.p = p.data; c.pn = p.norm;
   c.scal = dscal(L);
   c.part_pq = part_pq(L);
-  c.n_pq = L.sl_grid_nrm;
+  c.n_pq = L.sl_gnrm[shape_nrm(L)];
   c.part_r = part_r(L);
   c.par = par;
   YG_SLOPPY_DISPATCH(L.sl_prec, L.sl_lfmt, L.sl_cfmt, L.sl_reals, {
     launch_step1<SP, SL, SC, SK>(L.sl_shape, L.stream, a);
     YG_LAUNCHED();
-    launch_pdl(k_shop_cg<SP, SL, SC, SK>, L.sl_grid_cg, 128, L.stream, b, c);
+    const int v = shape_cg(L);
+    const int grid = L.sl_gcg[v];
+    if constexpr (SP == 16 && SL == 32 && SC == 32) {
+      if (v == 1) launch_pdl(k_shop_cg_min<SP, SL, SC, SK, 5>, grid, 128, L.stream, b, c);
+      else if (v == 2) launch_pdl(k_shop_cg_min<SP, SL, SC, SK, 6>, grid, 128, L.stream, b, c);
+      else launch_pdl(k_shop_cg<SP, SL, SC, SK>, grid, 128, L.stream, b, c);
+    } else {
+      launch_pdl(k_shop_cg<SP, SL, SC, SK>, grid, 128, L.stream, b, c);
+    }
     YG_LAUNCHED();
   });
   L.mvm += 2;
@@ -700,7 +761,8 @@ static void sloppy_hphi_cg(Lattice &L, SField t, SField tmp, float *x, float *r,
 
 static void sloppy_xpay(Lattice &L, SField p, const float *r, int par, double *hist) {
   YG_SPINOR_DISPATCH(L.sl_prec, {
-    launch_pdl(k_s_xpay<SP>, L.sl_grid_vec, 256, L.stream, p.data, p.norm, dscal(L), part_r(L), L.sl_grid_cg, par,
+    launch_pdl(k_s_xpay<SP>, L.sl_grid_vec, 256, L.stream, p.data, p.norm, dscal(L), part_r(L), L.sl_gcg[shape_cg(L)],
+               par,
                hist, hist_seq(L), (const float2 *)r, (int)L.Vh);
     YG_LAUNCHED();
   });
@@ -1005,11 +1067,13 @@ static void hop_time(Lattice &L, double mass, int reals, int reps, double *ms, d
   *bytes = (double)L.Vh * (spinor + 8.0 * link + clov + spinor);
 }
 
-// The block shape of the step-1 hop for FP16 spinors, FP32 matrices and `reals` link reals:
-// each shape of kShapes timed over 20 hops on this lattice, the fastest kept (once per
-// lattice and link format).  YG_TUNE_LOG prints the timings.
+// The block shapes of the inner operator for FP16 spinors, FP32 matrices and `reals` link
+// reals: each step-1 shape of kShapes timed over 20 hops on this lattice, then each register
+// variant of the two step-2 kernels; the fastest of each kept (once per lattice and link
+// format).  YG_TUNE_LOG prints the timings.
 static void tune_shape(Lattice &L, double mass, int reals) {
   if (L.sl_shape_reals == reals) return;
+  L.sl_shape_n = L.sl_shape_c = 0;
   int shape = 0;
   double best_ms = 0.0;
   for (int v = 0; v < 4; v++) {
@@ -1021,6 +1085,50 @@ static void tune_shape(Lattice &L, double mass, int reals) {
               kShapes[v][0], kShapes[v][1], t);
   }
   L.sl_shape = shape;
+  // the register variants of the two step-2 kernels, each timed over 10 Hphi applications on
+  // the solver's own scratch fields (which the solve rewrites before it reads them)
+  const int mvm0 = L.mvm;
+  SField p = sfield(L, 41), t = sfield(L, 44), o = sfield(L, 45);
+  float *fr = reinterpret_cast<float *>(L.scratch_field(40));
+  float *fx = reinterpret_cast<float *>(L.scratch_field(42));
+  sloppy_from_d(L, p, L.scratch_field(3));
+  set_scalar(L, S_RR0, 1.0);
+  cudaEvent_t e0, e1;
+  YG_CUDA(cudaEventCreate(&e0));
+  YG_CUDA(cudaEventCreate(&e1));
+  auto timed = [&](auto &&fn) {
+    fn();
+    YG_CUDA(cudaEventRecord(e0, L.stream));
+    for (int r = 0; r < 10; r++) fn();
+    YG_CUDA(cudaEventRecord(e1, L.stream));
+    YG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    YG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    return ms / 10.f;
+  };
+  float best_n = 0.f, best_c = 0.f;
+  int vn = 0, vc = 0;
+  for (int v = 0; v < kStep2Shapes; v++) {
+    L.sl_shape_n = v;
+    const float ms = timed([&] { sloppy_hphi(L, t, p, o, true); });
+    if (v == 0 || ms < best_n) { best_n = ms; vn = v; }
+    if (std::getenv("YG_TUNE_LOG"))
+      fprintf(stderr, "yg tune inner Hphi with <p,Ap>: step 2 cut for %d blocks/SM: %.4f ms\n", kStep2Min[v], ms);
+  }
+  L.sl_shape_n = vn;
+  sloppy_hphi(L, t, p, o, true);            // the <p, A p> partials the update kernel reads
+  for (int v = 0; v < kStep2Shapes; v++) {
+    L.sl_shape_c = v;
+    const float ms = timed([&] { sloppy_hphi_cg(L, t, o, fx, fr, p, 0); });
+    if (v == 0 || ms < best_c) { best_c = ms; vc = v; }
+    if (std::getenv("YG_TUNE_LOG"))
+      fprintf(stderr, "yg tune inner Hphi with the CG update: step 2 cut for %d blocks/SM: %.4f ms\n", kStep2Min[v],
+              ms);
+  }
+  L.sl_shape_c = vc;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  L.mvm = mvm0;
   L.sl_shape_reals = reals;
 }
 
