@@ -51,7 +51,7 @@ Lattice::~Lattice() {
   }
   for (DevBuf *b : {&fund, &links, &clover, &ldl, &cl_force, &mom, &tables, &red_partial, &red_result, &links_f,
                     &clover_f, &cinv_f, &sl_links, &sl_clover, &cpk64, &sl_part, &sl_scal, &fund_backup, &sl_cnorm,
-                    &mr_work, &mr_scal, &mr_part, &mr_clov, &sl_tick})
+                    &mr_work, &mr_scal, &mr_part, &mr_clov})
     b->release();
 }
 

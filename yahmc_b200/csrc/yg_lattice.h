@@ -101,10 +101,12 @@ struct Lattice {
   int sl_shape_reals = 0;  // link reals sl_shape was tuned for, 0 = not yet
   DevBuf sl_part;      // per-block partial sums of the device-scalar reductions
   int sl_grid_vec = 0; // blocks of the inner vector kernels
-  // register variants (tuned) of the two step-2 kernels of an inner iteration: the hop
-  // forming <p, A p>, and the last Schur step with the fused CG update
+  // resident-grid sizes of the two step-2 kernels of an inner iteration (the hop forming
+  // <p, A p>, and the last Schur step with the fused CG update) for each register variant,
+  // the variants in use (tuned), and where the |r|^2 partials start in sl_part
+  int sl_gnrm[kStep2Shapes] = {0, 0, 0}, sl_gcg[kStep2Shapes] = {0, 0, 0};
   int sl_shape_n = 0, sl_shape_c = 0;
-  DevBuf sl_tick;      // the ticket counters of their grid-wide sums
+  int sl_part_off = 0;
   DevBuf sl_scal;      // device scalars of the inner CG (rr, alpha, beta, ...) + completion counter
   double *sl_hist = nullptr;          // mapped pinned host ring of inner |r|^2 (written by the GPU)
   cudaEvent_t sl_ev[2] = {nullptr, nullptr};

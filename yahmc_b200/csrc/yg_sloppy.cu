@@ -158,12 +158,15 @@ __device__ __forceinline__ void shop_body(const SHopArgs &a) {
     griddep_launch();
     return;
   }
-  // NRM: one site per thread as well; the grid's sum of |dst|^2 = <p, A p> goes to *a.total
-  SiteNbr n;
-  if (t < a.n) site_nbr(n, a.g, a.lo + t);
   griddep_wait();
-  const double n2 = t < a.n ? (double)shop_site<P, LP, CP, K, STEP>(a, a.lo + t, n) : 0.0;
-  grid_total(n2, a.part, a.ticket, a.total);
+  double n2 = 0.0;
+  for (; t < a.n; t += gridDim.x * blockDim.x) {
+    SiteNbr n;
+    site_nbr(n, a.g, a.lo + t);
+    n2 += (double)shop_site<P, LP, CP, K, STEP>(a, a.lo + t, n);
+  }
+  n2 = block_total(n2);
+  if (threadIdx.x == 0) a.part[blockIdx.x] = n2;
   griddep_launch();
 }
 
@@ -192,31 +195,35 @@ __global__ void __launch_bounds__(TPB, MINB) k_shop_shaped(SHopArgs a) {
 }
 
 // The last Schur step of the iteration's second Hphi with the CG update as its epilogue:
-// q = Hphi t stays in registers, alpha = |r|^2 / <p, A p> (<p, A p> formed by the NRM hop's
-// last block), x += alpha p, r -= alpha q on the site, and the new |r|^2 summed over the grid
-// into scal[S_RRN] by the last block.  q is never stored.  One site per thread.
+// q = Hphi t stays in registers, alpha = |r|^2 / <p, A p> (every block sums the partials of
+// the NRM hop in the same order), x += alpha p, r -= alpha q on the site, and the per-block
+// partials of the new |r|^2 go to part_r.  q is never stored.  Resident grid, grid-stride.
 struct SCgArgs {
   float2 *x, *r;                  // FP32 even-site words
   const void *p;                  // search direction in the spinor format
   const float *pn;
   double *scal;
-  double *part_r;                 // one |r|^2 partial per block
-  unsigned *ticket;
+  const double *part_pq;
+  int n_pq;
+  double *part_r;
   int par;
 };
 
 template <int P, int LP, int CP, int K>
 __device__ __forceinline__ void shop_cg_body(const SHopArgs &a, const SCgArgs &c) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  SiteNbr n;
-  if (t < a.n) site_nbr(n, a.g, a.lo + t);
   griddep_wait();
-  const double alpha = c.scal[S_RR0 + c.par] / c.scal[S_PQ];
-  if (blockIdx.x == 0 && threadIdx.x == 0) c.scal[S_ALPHA] = alpha;
+  const double pq = sum_partials(c.part_pq, c.n_pq);
+  const double alpha = c.scal[S_RR0 + c.par] / pq;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    c.scal[S_PQ] = pq;
+    c.scal[S_ALPHA] = alpha;
+  }
   const float al = (float)alpha;
   const int Vh = a.g.Vh;
   double acc = 0.0;
-  if (t < a.n) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < a.n; t += gridDim.x * blockDim.x) {
+    SiteNbr n;
+    site_nbr(n, a.g, a.lo + t);
     float2 q[12], pp[12];
     shop_out<P, LP, CP, K, 2>(q, a, a.lo + t, n);
     sload<P>(pp, c.p, c.pn, 0, t, Vh);
@@ -233,9 +240,10 @@ __device__ __forceinline__ void shop_cg_body(const SHopArgs &a, const SCgArgs &c
       c.r[i] = ri;
       s = fmaf(ri.x, ri.x, fmaf(ri.y, ri.y, s));
     }
-    acc = s;
+    acc += s;
   }
-  grid_total(acc, c.part_r, c.ticket, c.scal + S_RRN);
+  acc = block_total(acc);
+  if (threadIdx.x == 0) c.part_r[blockIdx.x] = acc;
   griddep_launch();
 }
 
@@ -431,16 +439,17 @@ __global__ void __launch_bounds__(256) k_s_from_d(void *dst, float *dn, const do
   }
 }
 
-// |r|^2 from the update kernel's grid total, beta = |r|^2 / |r_old|^2, p = r + beta p; block 0
+// |r|^2 from the update's partials, beta = |r|^2 / |r_old|^2, p = r + beta p; block 0
 // stores |r|^2 for the next iteration and into *hist, then counts the iteration (S_ITER)
 // and stores the count into *seq (hist and seq are mapped host memory, which the host polls
 // one iteration later).  Nothing in the arguments changes between iterations of the same
 // parity, so an iteration can be replayed as a CUDA graph.
 template <int P>
-__global__ void __launch_bounds__(256) k_s_xpay(void *p, float *pn, double *scal, int par, double *hist,
-                                                unsigned long long *seq, const float2 *r, int Vh) {
+__global__ void __launch_bounds__(256) k_s_xpay(void *p, float *pn, double *scal, const double *part_r, int n_r,
+                                                int par, double *hist, unsigned long long *seq, const float2 *r,
+                                                int Vh) {
   griddep_wait();
-  const double rr = scal[S_RRN];
+  const double rr = sum_partials(part_r, n_r);
   const float b = (float)(rr / scal[S_RR0 + par]);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     scal[S_RR0 + (par ^ 1)] = rr;
@@ -552,18 +561,29 @@ void ensure_sloppy(Lattice &L, double mass, int prec, int reals, int lfmt, int c
   {
     // resident-grid sizes of the reduction kernels, and room for their partials
     int dev = 0, sms = 0, per_vec = 0;
+    int per_nrm[kStep2Shapes] = {0, 0, 0}, per_cg[kStep2Shapes] = {0, 0, 0};
     YG_CUDA(cudaGetDevice(&dev));
     YG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    YG_SPINOR_DISPATCH(prec, {
+    YG_SLOPPY_DISPATCH(prec, lfmt, cfmt, reals, {
+      YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_nrm[0], k_shop<SP, SL, SC, SK, 2, 1>, 128, 0));
+      YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_cg[0], k_shop_cg<SP, SL, SC, SK>, 128, 0));
+      if constexpr (SP == 16 && SL == 32 && SC == 32) {
+        YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_nrm[1], k_shop_nrm_min<SP, SL, SC, SK, 5>, 128, 0));
+        YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_nrm[2], k_shop_nrm_min<SP, SL, SC, SK, 6>, 128, 0));
+        YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_cg[1], k_shop_cg_min<SP, SL, SC, SK, 5>, 128, 0));
+        YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_cg[2], k_shop_cg_min<SP, SL, SC, SK, 6>, 128, 0));
+      }
       YG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_vec, k_s_xpay<SP>, 256, 0));
     });
-    L.sl_grid_vec = (int)std::min<long>((long)sms * std::max(per_vec, 1), nblk(L.Vh, 256));
-    // one partial per block of the two grid-sum kernels (one site per thread), two tickets
-    L.sl_part.alloc(sizeof(double) * 2 * (size_t)nblk(L.Vh, 128));
-    if (!L.sl_tick.p) {
-      L.sl_tick.alloc(2 * sizeof(unsigned));
-      YG_CUDA(cudaMemsetAsync(L.sl_tick.p, 0, 2 * sizeof(unsigned), L.stream));
+    int gmax = 0;
+    for (int v = 0; v < kStep2Shapes; v++) {
+      L.sl_gnrm[v] = (int)std::min<long>((long)sms * std::max(per_nrm[v], 1), nblk(L.Vh, 128));
+      L.sl_gcg[v] = (int)std::min<long>((long)sms * std::max(per_cg[v], 1), nblk(L.Vh, 128));
+      gmax = std::max({gmax, L.sl_gnrm[v], L.sl_gcg[v]});
     }
+    L.sl_grid_vec = (int)std::min<long>((long)sms * std::max(per_vec, 1), nblk(L.Vh, 256));
+    L.sl_part_off = gmax;
+    L.sl_part.alloc(sizeof(double) * (size_t)(2 * gmax));
   }
   const int K = reals / 2;
   L.sl_links.alloc((lfmt == ST_F32 ? 8 : 4) * (size_t)K * 4 * L.V);
@@ -648,8 +668,7 @@ static void launch_step1(int shape, cudaStream_t s, const SHopArgs &a) {
 static double *dscal(Lattice &L) { return L.sl_scal.as<double>(); }
 static unsigned long long *hist_seq(Lattice &L) { return reinterpret_cast<unsigned long long *>(L.sl_hist + 4); }
 static double *part_pq(Lattice &L) { return L.sl_part.as<double>(); }
-static double *part_r(Lattice &L) { return L.sl_part.as<double>() + nblk(L.Vh, 128); }
-static unsigned *tickets(Lattice &L) { return L.sl_tick.as<unsigned>(); }
+static double *part_r(Lattice &L) { return L.sl_part.as<double>() + L.sl_part_off; }
 
 // the step-2 shapes in use: the tuned ones for the default storage, the compiler's otherwise
 static bool default_storage(const Lattice &L) { return L.sl_prec == 16 && L.sl_lfmt == ST_F32 && L.sl_cfmt == ST_F32; }
@@ -675,14 +694,12 @@ static void sloppy_hphi(Lattice &L, SField dst, SField src, SField tmp, bool nrm
   b.coeff = -0.5f;
   b.lo = 0;
   b.part = part_pq(L);
-  b.ticket = tickets(L);
-  b.total = dscal(L) + S_PQ;
   YG_SLOPPY_DISPATCH(L.sl_prec, L.sl_lfmt, L.sl_cfmt, L.sl_reals, {
     launch_step1<SP, SL, SC, SK>(L.sl_shape, L.stream, a);
     YG_LAUNCHED();
     if (nrm) {
       const int v = shape_nrm(L);
-      const int grid = nblk(b.n, 128);
+      const int grid = L.sl_gnrm[v];
       if constexpr (SP == 16 && SL == 32 && SC == 32) {
         if (v == 1) launch_pdl(k_shop_nrm_min<SP, SL, SC, SK, 5>, grid, 128, L.stream, b);
         else if (v == 2) launch_pdl(k_shop_nrm_min<SP, SL, SC, SK, 6>, grid, 128, L.stream, b);
@@ -721,14 +738,15 @@ static void sloppy_hphi_cg(Lattice &L, SField t, SField tmp, float *x, float *r,
   c.r = reinterpret_cast<float2 *>(r);
   c.p = p.data; c.pn = p.norm;
   c.scal = dscal(L);
+  c.part_pq = part_pq(L);
+  c.n_pq = L.sl_gnrm[shape_nrm(L)];
   c.part_r = part_r(L);
-  c.ticket = tickets(L) + 1;
   c.par = par;
   YG_SLOPPY_DISPATCH(L.sl_prec, L.sl_lfmt, L.sl_cfmt, L.sl_reals, {
     launch_step1<SP, SL, SC, SK>(L.sl_shape, L.stream, a);
     YG_LAUNCHED();
     const int v = shape_cg(L);
-    const int grid = nblk(b.n, 128);
+    const int grid = L.sl_gcg[v];
     if constexpr (SP == 16 && SL == 32 && SC == 32) {
       if (v == 1) launch_pdl(k_shop_cg_min<SP, SL, SC, SK, 5>, grid, 128, L.stream, b, c);
       else if (v == 2) launch_pdl(k_shop_cg_min<SP, SL, SC, SK, 6>, grid, 128, L.stream, b, c);
@@ -743,7 +761,8 @@ static void sloppy_hphi_cg(Lattice &L, SField t, SField tmp, float *x, float *r,
 
 static void sloppy_xpay(Lattice &L, SField p, const float *r, int par, double *hist) {
   YG_SPINOR_DISPATCH(L.sl_prec, {
-    launch_pdl(k_s_xpay<SP>, L.sl_grid_vec, 256, L.stream, p.data, p.norm, dscal(L), par,
+    launch_pdl(k_s_xpay<SP>, L.sl_grid_vec, 256, L.stream, p.data, p.norm, dscal(L), part_r(L), L.sl_gcg[shape_cg(L)],
+               par,
                hist, hist_seq(L), (const float2 *)r, (int)L.Vh);
     YG_LAUNCHED();
   });

@@ -244,8 +244,6 @@ struct SHopArgs {
   float coeff;              // +1/2 (step 1) or -1/2 (step 2)
   int lo, n;                // output sites [lo, lo+n): the odd block (step 1) or even (step 2)
   double *part;             // NRM: one partial sum of |dst|^2 per block
-  unsigned *ticket;         // NRM: blocks finished (the last one forms the total, then rearms it)
-  double *total;            // NRM: the sum of the partials
 };
 
 // ------------------------------------------------------------------ device-side reductions
@@ -255,7 +253,7 @@ struct SHopArgs {
 // and the count of finished inner iterations (S_ITER, the value the host polls).  Grid sums are two-phase: a producer launch stores one partial per block,
 // and every block of the consumer launch adds all of them in index order, so the result
 // is deterministic and no block ever waits for another.
-enum { S_RR0 = 0, S_RR1 = 1, S_ALPHA = 2, S_PQ = 3, S_ITER = 4, S_RRN = 5, S_WORDS = 8 };
+enum { S_RR0 = 0, S_RR1 = 1, S_ALPHA = 2, S_PQ = 3, S_ITER = 4, S_WORDS = 8 };
 
 // block total of v, returned to every thread (blockDim a multiple of 32, at most 1024)
 __device__ __forceinline__ double block_total(double v) {
@@ -281,32 +279,6 @@ __device__ __forceinline__ double sum_partials(const double *part, int n) {
   double acc = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) acc += part[i];
   return block_total(acc);
-}
-
-// Grid-wide sum in one launch: every block stores its block total in part[blockIdx.x]; the
-// last block to finish (a ticket counter) adds all partials in block order, stores the sum in
-// *total and rearms the counter for the next launch.  The order of the additions is fixed,
-// so the result does not depend on which block finishes last.  Every thread of the block
-// must call it.
-__device__ __forceinline__ void grid_total(double v, double *part, unsigned *ticket, double *total) {
-  __shared__ int last;
-  v = block_total(v);
-  if (threadIdx.x == 0) {
-    part[blockIdx.x] = v;
-    __threadfence();
-    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (last) {
-    __threadfence();
-    double acc = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) acc += __ldcg(part + i);
-    acc = block_total(acc);
-    if (threadIdx.x == 0) {
-      *total = acc;
-      *ticket = 0u;
-    }
-  }
 }
 
 // Programmatic dependent launch: a kernel launched with programmatic stream serialisation
