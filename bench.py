@@ -1101,8 +1101,9 @@ def run_ours(a, rank, world, dist):
         "fp64_cg": {"ms": ms_fp64, "iterations": it_fp64, "speedup_mixed_vs_fp64": ms_fp64 / ms_mixed},
         "dslash_fp64": {"ms": ms_hop, "GB_s": hop_gbs, "bytes_per_site": bytes_per_site, "sites": V // 2},
         "roofline": {"bound": "hbm",
-                     "kernel": "k_shop<16,32,32,6,1,0> (inner operator step 1: FP16 spinors + norms, FP32 12-real "
-                               "links, FP32 packed clover; 2 of the 6 launches of an inner iteration)",
+                     "kernel": "inner operator step 1 (k_shop<16,32,32,6,1,0>, or k_shop_shaped in the block shape "
+                               "the tuner chose for this lattice: FP16 spinors + norms, FP32 12-real links, FP32 "
+                               "packed clover; 2 of the 5 launches of an inner iteration)",
                      "achieved": inner_gbs, "peak": peak, "unit": "GB/s", "frac": inner_gbs / peak,
                      "peak_kind": peak_kind, "traffic": inner_traffic(a.inner, V // 2),
                      "traffic_source": INNER_NCU.get(a.inner, (0, 0, "no ncu capture of this inner format"))[2],
