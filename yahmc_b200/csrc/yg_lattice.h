@@ -118,7 +118,8 @@ struct Lattice {
   DevBuf mr_scal, mr_part;
   DevBuf mr_clov;      // packed FP32 clover blocks of the further masses of a multi-mass call
   double *mr_hist = nullptr;
-  int mr_tile[17] = {};   // measured inner-operator variant (tile, threads per site) + 1, per system count
+  int mr_tile[17] = {};   // measured inner-operator variant (tile, threads per site) + 1, + 8 for 18-real
+                          // links, per system count
 
   long field_doubles() const { return 8L * d * V; }
   size_t field_bytes() const { return sizeof(double) * field_doubles(); }

@@ -475,7 +475,8 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
         throw Error(YG_ERR_ARG, "solution fields must be distinct from each other and from the sources");
   }
   const int nb = nrhs;
-  const int reals = (L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL) ? 12 : 18;
+  const bool su3 = L.nc == 3 && L.p.repr == YG_REPR_FUNDAMENTAL;
+  int reals = su3 ? 12 : 18;               // link reals of the inner operator (tuned below for SU(3))
   // the mass of each system (masses == nullptr: par.mass for all); the first one's clover
   // blocks are the lattice's own inner-operator copy, every other distinct mass gets a
   // packed set of its own, rebuilt on each call (a few hop times)
@@ -632,8 +633,11 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
     k_m_p_from_r<<<dim3(gv, v.nsys), kVecThreads, 0, L.stream>>>(v, Vh);
     YG_LAUNCHED();
   }
-  // the tile (systems per thread) of the inner operator: measured once per lattice and system
-  // count on the current fields (one Hphi of each candidate, after a warm-up launch)
+  // the tile (systems per thread), the threads per site and, for SU(3) fundamental links, the
+  // link format (12 reals with the third row rebuilt, or all 18: the operator is bound by
+  // instruction issue, so the rebuild can cost more than the bytes it saves): measured once
+  // per lattice and system count on the current fields (one Hphi of each candidate, after a
+  // warm-up launch).  mr_tile[ns] = variant + 1, plus 8 for 18-real links.
   if (!act.empty()) {
     const int ns = (int)act.size();
     if (L.mr_tile[ns] == 0) {
@@ -641,30 +645,39 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
       YG_CUDA(cudaEventCreate(&e0));
       YG_CUDA(cudaEventCreate(&e1));
       float best_ms = 0.f;
-      int best = 2, calls = 0;
-      for (int cand = 0; cand < 5; cand++) {
-        const int r = kVariants[cand][0];
-        if (r > 1 && r >= 2 * ns) continue;
-        var = cand;
-        calls += 4;
-        hphi(0, false);                          // warm-up; t only (p untouched)
-        YG_CUDA(cudaEventRecord(e0, L.stream));
-        for (int rep = 0; rep < 3; rep++) hphi(0, false);
-        YG_CUDA(cudaEventRecord(e1, L.stream));
-        YG_CUDA(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        YG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        if (best_ms == 0.f || ms < best_ms) { best_ms = ms; best = cand; }
-        if (std::getenv("YG_TUNE_LOG"))
-          std::fprintf(stderr, "yg tune cg_mixed_multi: %d systems, %d per thread, %d-way direction split: %.3f ms/Hphi\n",
-                       ns, r, kVariants[cand][1], ms / 3.f);
+      int best = 2, best_reals = reals, calls = 0;
+      for (int lr : {12, 18}) {
+        if (lr == 12 && !su3) continue;
+        reals = lr;
+        ensure_sloppy(L, dist[0], 16, reals, 32, 32);
+        for (int cand = 0; cand < 5; cand++) {
+          const int r = kVariants[cand][0];
+          if (r > 1 && r >= 2 * ns) continue;
+          var = cand;
+          calls += 4;
+          hphi(0, false);                        // warm-up; t only (p untouched)
+          YG_CUDA(cudaEventRecord(e0, L.stream));
+          for (int rep = 0; rep < 3; rep++) hphi(0, false);
+          YG_CUDA(cudaEventRecord(e1, L.stream));
+          YG_CUDA(cudaEventSynchronize(e1));
+          float ms = 0.f;
+          YG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          if (best_ms == 0.f || ms < best_ms) { best_ms = ms; best = cand; best_reals = lr; }
+          if (std::getenv("YG_TUNE_LOG"))
+            std::fprintf(stderr,
+                         "yg tune cg_mixed_multi: %d systems, %d-real links, %d per thread, %d-way direction split: "
+                         "%.3f ms/Hphi\n", ns, lr, r, kVariants[cand][1], ms / 3.f);
+        }
       }
       YG_CUDA(cudaEventDestroy(e0));
       YG_CUDA(cudaEventDestroy(e1));
       L.mvm -= 2 * ns * calls;                   // the timing launches are not MVMs of the solve
-      L.mr_tile[ns] = best + 1;
+      L.mr_tile[ns] = best + 1 + (best_reals == 18 && su3 ? 8 : 0);
     }
-    var = L.mr_tile[ns] - 1;
+    const int code = L.mr_tile[ns] - 1;
+    var = code & 7;
+    reals = (code & 8) || !su3 ? 18 : 12;
+    ensure_sloppy(L, dist[0], 16, reals, 32, 32);
   }
   const double d2 = delta * delta;
   constexpr int kStagnate = 100;   // as the single-system solver: force an update after 100 flat iterations
