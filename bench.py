@@ -83,7 +83,9 @@ def parse():
     ap.add_argument("--hmc", action="store_true",
                     help="configuration 2: Nf=2 HMC + Hasenbusch trajectories on 16^3x32 through YaHMC's own hmc "
                          "program built on the engine, FP64 and mixed-precision solvers (not the bench line)")
-    ap.add_argument("--hmc-trajectories", type=int, default=4)
+    ap.add_argument("--hmc-trajectories", type=int, default=8)
+    ap.add_argument("--hmc-fermion-therm", type=int, default=10,
+                    help="Nf=2 trajectories between the pure-gauge start and the measured ones")
     ap.add_argument("--rhmc", action="store_true",
                     help="configuration 4(i): order-12 rational approximation via one multishift solve and the "
                          "batched pole force, SU(2) adjoint 48x24^3 (not the bench line)")
@@ -581,11 +583,13 @@ def run_hmc(a):
     Wilson gauge action beta 5.6, clover csw 1, an HMC monomial (m = -0.75, dm = 0.2) and a
     Hasenbusch monomial (m = -0.75, dm = 0.2) on level 1 with 10 o2mn steps, the gauge monomial
     on level 0 with 1 step, trajectory length 1, prec 1e-24 (relative residual 1e-12).  The
-    start is 20 pure-gauge trajectories from the reference's random start (seed given).  Then
-    --hmc-trajectories trajectories with the reference's FP64 solvers and the same number with
-    the mixed-precision CG for the Hphi_sq solves (YAHMC_GPU_SOLVER=mixed); the program's own
-    log gives trajectory times, MVM counts, dH and acceptance.  The CPU build of the same
-    program (oracle/_ref) runs one trajectory from the same start for comparison."""
+    start is 20 pure-gauge trajectories from the reference's random start (seed given), then
+    --hmc-fermion-therm trajectories of the full action.  Then --hmc-trajectories trajectories
+    with the reference's FP64 solvers and the same number with the mixed-precision CG for the
+    Hphi_sq solves (YAHMC_GPU_SOLVER=mixed), both from that start with the same seed; the
+    program's own log gives trajectory times, MVM counts, dH, <exp(-dH)> and acceptance.  The
+    CPU build of the same program (oracle/_ref) runs one trajectory from the same start for
+    comparison."""
     exe = os.path.join(ROOT, "integration", "_build", "hmc_su3_fund_ap")
     cpu_exe = os.path.join(ROOT, "oracle", "_ref", "hmc_su3_fund_ap")
     if not os.path.exists(exe):
@@ -613,23 +617,38 @@ def run_hmc(a):
     seed = a.seed % 100000
     therm = run(exe, HMC_CFG.format(seed=seed, prefix="therm", start="random", last=20, freq=20, **dims) + GAUGE_ONLY,
                 "therm")
+    # then --hmc-fermion-therm trajectories with the fermions (the mixed solver), so that the
+    # measured trajectories start near equilibrium of the full action
+    nt = a.hmc_fermion_therm
     start = f"therm_{T}x{X}x{Y}x{Z}_nc3_n0020"
+    ftherm = None
+    if nt > 0:
+        ftherm = run(exe, HMC_CFG.format(seed=seed + 2, prefix="ftherm", start=start, last=20 + nt, freq=nt,
+                                         **dims) + NF2, "ftherm", {"YAHMC_GPU_SOLVER": "mixed"})
+        start = f"ftherm_{T}x{X}x{Y}x{Z}_nc3_n{20 + nt:04d}"
+    n0 = 20 + nt
     n = a.hmc_trajectories
     res = {"workload": "Nf=2 HMC + Hasenbusch trajectory, 16^3x32 SU(3) fund clover even-odd, YaHMC's hmc program "
-                       "on the engine", "start": f"20 pure-gauge trajectories from the random start, plaquette "
-                       f"{therm['plaquette'][-1]:.6f}", "thermalisation_s": therm["wall_s"]}
+                       "on the engine", "start": f"20 pure-gauge trajectories from the random start (plaquette "
+                       f"{therm['plaquette'][-1]:.6f}), then {nt} Nf=2 trajectories"
+                       + (f" (plaquette {ftherm['plaquette'][-1]:.6f}, dH of the last {ftherm['dH'][-1]:.4f})"
+                          if ftherm else ""),
+           "thermalisation_s": therm["wall_s"] + (ftherm["wall_s"] if ftherm else 0.0)}
     for solver, env in (("fp64", None), ("mixed", {"YAHMC_GPU_SOLVER": "mixed"})):
         # the program counts configurations from the start file's number (hmc.cpp:148): last is absolute
-        r = run(exe, HMC_CFG.format(seed=seed + 1, prefix="nf2", start=start, last=20 + n, freq=0, **dims) + NF2,
+        r = run(exe, HMC_CFG.format(seed=seed + 1, prefix="nf2", start=start, last=n0 + n, freq=0, **dims) + NF2,
                 f"nf2_{solver}", env)
         if len(r["seconds"]) != n:
             raise RuntimeError(f"nf2_{solver}: {len(r['seconds'])} trajectories in the log, expected {n}")
         dh = np.array(r["dH"])
+        emdh = np.exp(-dh)
         res[solver] = {"trajectory_s": r["seconds"], "mean_trajectory_s": float(np.mean(r["seconds"])),
-                       "mvm": r["mvm"], "dH": r["dH"], "exp_minus_dH_mean": float(np.mean(np.exp(-dh))),
-                       "acceptance": float(np.mean(r["accepted"])), "plaquette": r["plaquette"]}
+                       "mvm": r["mvm"], "dH": r["dH"], "exp_minus_dH_mean": float(np.mean(emdh)),
+                       "exp_minus_dH_stderr": float(np.std(emdh, ddof=1) / np.sqrt(len(emdh))) if len(emdh) > 1
+                       else None, "acceptance": float(np.mean(r["accepted"])), "plaquette": r["plaquette"]}
     if os.path.exists(cpu_exe) and not a.no_cpu_baseline:
-        r = run(cpu_exe, HMC_CFG.format(seed=seed + 1, prefix="cpu", start=start, last=21, freq=0, **dims) + NF2, "cpu")
+        r = run(cpu_exe, HMC_CFG.format(seed=seed + 1, prefix="cpu", start=start, last=n0 + 1, freq=0, **dims) + NF2,
+                "cpu")
         if len(r["seconds"]) != 1:
             raise RuntimeError("cpu: no trajectory in the log")
         res["cpu_reference"] = {"trajectory_s": r["seconds"], "mvm": r["mvm"], "dH": r["dH"],
