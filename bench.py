@@ -83,8 +83,8 @@ def parse():
     ap.add_argument("--hmc", action="store_true",
                     help="configuration 2: Nf=2 HMC + Hasenbusch trajectories on 16^3x32 through YaHMC's own hmc "
                          "program built on the engine, FP64 and mixed-precision solvers (not the bench line)")
-    ap.add_argument("--hmc-trajectories", type=int, default=8)
-    ap.add_argument("--hmc-fermion-therm", type=int, default=10,
+    ap.add_argument("--hmc-trajectories", type=int, default=4)
+    ap.add_argument("--hmc-fermion-therm", type=int, default=0,
                     help="Nf=2 trajectories between the pure-gauge start and the measured ones")
     ap.add_argument("--rhmc", action="store_true",
                     help="configuration 4(i): order-12 rational approximation via one multishift solve and the "
@@ -612,6 +612,8 @@ def run_hmc(a):
             raise RuntimeError(f"{name}: rc {r.returncode}: {r.stderr[-1000:]}")
         out = _hmc_log(log)
         out["wall_s"] = wall
+        with open(log) as f:
+            out["log_tail"] = f.read()[-1500:]
         return out
 
     seed = a.seed % 100000
@@ -625,6 +627,9 @@ def run_hmc(a):
     if nt > 0:
         ftherm = run(exe, HMC_CFG.format(seed=seed + 2, prefix="ftherm", start=start, last=20 + nt, freq=nt,
                                          **dims) + NF2, "ftherm", {"YAHMC_GPU_SOLVER": "mixed"})
+        if len(ftherm["seconds"]) != nt:
+            raise RuntimeError(f"ftherm: {len(ftherm['seconds'])} trajectories in the log, expected {nt}; log "
+                               f"ends:\n{ftherm['log_tail']}")
         start = f"ftherm_{T}x{X}x{Y}x{Z}_nc3_n{20 + nt:04d}"
     n0 = 20 + nt
     n = a.hmc_trajectories
@@ -639,7 +644,8 @@ def run_hmc(a):
         r = run(exe, HMC_CFG.format(seed=seed + 1, prefix="nf2", start=start, last=n0 + n, freq=0, **dims) + NF2,
                 f"nf2_{solver}", env)
         if len(r["seconds"]) != n:
-            raise RuntimeError(f"nf2_{solver}: {len(r['seconds'])} trajectories in the log, expected {n}")
+            raise RuntimeError(f"nf2_{solver}: {len(r['seconds'])} trajectories in the log, expected {n}; log ends:\n"
+                               f"{r['log_tail']}")
         dh = np.array(r["dH"])
         emdh = np.exp(-dh)
         res[solver] = {"trajectory_s": r["seconds"], "mean_trajectory_s": float(np.mean(r["seconds"])),

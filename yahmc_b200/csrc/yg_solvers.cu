@@ -108,6 +108,10 @@ int cg_lattices(int n, Lattice *const *L, const yg_inv_par *par, double *const *
   const bool batch = batch_eligible(n, L, par);
   if (persistent) *persistent = batch ? 1 : 0;
   if (batch) return cg_lattices_persistent(n, L, par, xs, bs, iters, wait_cycles);
+  // the scratch fields the solves use, allocated here: a cudaMalloc inside the threads would
+  // synchronise the device while the other lattices' solves run
+  for (int i = 0; i < n; i++)
+    for (int k = 1; k <= 5; k++) L[i]->scratch_field(k);
   int dev = 0;
   YG_CUDA(cudaGetDevice(&dev));
   std::vector<int> st(n, YG_OK);
