@@ -300,7 +300,19 @@ int cg_mixed(inv_par &par, SpinorField &x, SpinorField &b, const char *who)
 	yg_solve_stats st;
 	Fields f;
 	double *dx = f(x), *db = f(b);
-	check(yg_cg_mixed(lat(), &p, dx, db, &st), "yg_cg_mixed");
+	const int rc = yg_cg_mixed(lat(), &p, dx, db, &st);
+	if(rc == YG_STALL)
+	{
+		// the true residual could not be brought below prec (an ill-conditioned system whose
+		// FP64 rounding floor lies above it); x is the FP64 CG's solution, which met prec on
+		// its recursive residual, which is all YaHMC's own cg_inverter (cg.cpp:186) asks for
+		lprintf("INVERTER", NOTICE, "%s (mixed CG): true residual %1.4e above prec %1.1e, kept the FP64 CG's solution",
+		        who, st.true_residual, par.prec);
+	}
+	else
+	{
+		check(rc, "yg_cg_mixed");
+	}
 	if(par.log)
 	{
 		lprintf("INVERTER", NOTICE, "%s (mixed CG): iterations = %d, precision = %1.4e, reliable updates = %d%s",

@@ -31,7 +31,13 @@ static int guard(F &&f) {
 template <typename F>
 static int guard_status(F &&f) {
   try {
-    return f();
+    const int rc = f();
+    // a solver status returned rather than thrown: leave a message for yg_last_error()
+    if (rc == YG_MAXITER) g_last_error = "the solver reached maxiter before its stopping criterion";
+    else if (rc == YG_STALL) g_last_error = "the solver stopped making progress above the requested precision";
+    else if (rc == YG_NONFINITE) g_last_error = "a reduction gave a non-finite value";
+    else if (rc == YG_TIMEOUT) g_last_error = "a bounded device-side wait gave up";
+    return rc;
   } catch (const Error &e) {
     g_last_error = e.what();
     return e.code;
