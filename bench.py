@@ -86,6 +86,8 @@ def parse():
     ap.add_argument("--hmc-trajectories", type=int, default=4)
     ap.add_argument("--hmc-fermion-therm", type=int, default=0,
                     help="Nf=2 trajectories between the pure-gauge start and the measured ones")
+    ap.add_argument("--hmc-mass", type=float, default=-0.75,
+                    help="bare mass m of the HMC (m + 0.2) and Hasenbusch (m) monomials")
     ap.add_argument("--rhmc", action="store_true",
                     help="configuration 4(i): order-12 rational approximation via one multishift solve and the "
                          "batched pole force, SU(2) adjoint 48x24^3 (not the bench line)")
@@ -553,14 +555,14 @@ c0 = 1.0
 [monomial]
 level = 1
 type = hmc
-mass = -0.75
+mass = {mass}
 dm = 0.2
 prec = 1e-24
 mre_past = 5
 [monomial]
 level = 1
 type = hasenbusch
-mass = -0.75
+mass = {mass}
 dm = 0.2
 prec = 1e-24
 """
@@ -626,7 +628,7 @@ def run_hmc(a):
     ftherm = None
     if nt > 0:
         ftherm = run(exe, HMC_CFG.format(seed=seed + 2, prefix="ftherm", start=start, last=20 + nt, freq=nt,
-                                         **dims) + NF2, "ftherm", {"YAHMC_GPU_SOLVER": "mixed"})
+                                         **dims) + NF2.format(mass=a.hmc_mass), "ftherm", {"YAHMC_GPU_SOLVER": "mixed"})
         if len(ftherm["seconds"]) != nt:
             raise RuntimeError(f"ftherm: {len(ftherm['seconds'])} trajectories in the log, expected {nt}; log "
                                f"ends:\n{ftherm['log_tail']}")
@@ -634,15 +636,15 @@ def run_hmc(a):
     n0 = 20 + nt
     n = a.hmc_trajectories
     res = {"workload": "Nf=2 HMC + Hasenbusch trajectory, 16^3x32 SU(3) fund clover even-odd, YaHMC's hmc program "
-                       "on the engine", "start": f"20 pure-gauge trajectories from the random start (plaquette "
+                       f"on the engine, m = {a.hmc_mass}", "start": f"20 pure-gauge trajectories from the random start (plaquette "
                        f"{therm['plaquette'][-1]:.6f}), then {nt} Nf=2 trajectories"
                        + (f" (plaquette {ftherm['plaquette'][-1]:.6f}, dH of the last {ftherm['dH'][-1]:.4f})"
                           if ftherm else ""),
            "thermalisation_s": therm["wall_s"] + (ftherm["wall_s"] if ftherm else 0.0)}
     for solver, env in (("fp64", None), ("mixed", {"YAHMC_GPU_SOLVER": "mixed"})):
         # the program counts configurations from the start file's number (hmc.cpp:148): last is absolute
-        r = run(exe, HMC_CFG.format(seed=seed + 1, prefix="nf2", start=start, last=n0 + n, freq=0, **dims) + NF2,
-                f"nf2_{solver}", env)
+        r = run(exe, HMC_CFG.format(seed=seed + 1, prefix="nf2", start=start, last=n0 + n, freq=0, **dims)
+                + NF2.format(mass=a.hmc_mass), f"nf2_{solver}", env)
         if len(r["seconds"]) != n:
             raise RuntimeError(f"nf2_{solver}: {len(r['seconds'])} trajectories in the log, expected {n}; log ends:\n"
                                f"{r['log_tail']}")
@@ -653,8 +655,8 @@ def run_hmc(a):
                        "exp_minus_dH_stderr": float(np.std(emdh, ddof=1) / np.sqrt(len(emdh))) if len(emdh) > 1
                        else None, "acceptance": float(np.mean(r["accepted"])), "plaquette": r["plaquette"]}
     if os.path.exists(cpu_exe) and not a.no_cpu_baseline:
-        r = run(cpu_exe, HMC_CFG.format(seed=seed + 1, prefix="cpu", start=start, last=n0 + 1, freq=0, **dims) + NF2,
-                "cpu")
+        r = run(cpu_exe, HMC_CFG.format(seed=seed + 1, prefix="cpu", start=start, last=n0 + 1, freq=0, **dims)
+                + NF2.format(mass=a.hmc_mass), "cpu")
         if len(r["seconds"]) != 1:
             raise RuntimeError("cpu: no trajectory in the log")
         res["cpu_reference"] = {"trajectory_s": r["seconds"], "mvm": r["mvm"], "dH": r["dH"],
