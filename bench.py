@@ -627,7 +627,8 @@ def run_hmc(a):
     start = f"therm_{T}x{X}x{Y}x{Z}_nc3_n0020"
     ftherm = None
     if nt > 0:
-        ftherm = run(exe, HMC_CFG.format(seed=seed + 2, prefix="ftherm", start=start, last=20 + nt, freq=nt,
+        # the program saves when the configuration number is a multiple of freq: only the last one
+        ftherm = run(exe, HMC_CFG.format(seed=seed + 2, prefix="ftherm", start=start, last=20 + nt, freq=20 + nt,
                                          **dims) + NF2.format(mass=a.hmc_mass), "ftherm", {"YAHMC_GPU_SOLVER": "mixed"})
         if len(ftherm["seconds"]) != nt:
             raise RuntimeError(f"ftherm: {len(ftherm['seconds'])} trajectories in the log, expected {nt}; log "
