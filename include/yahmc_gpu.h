@@ -191,10 +191,12 @@ int yg_rational_calc(yg_lattice *lat, const yg_inv_par *par, double a0, int orde
  * reliable updates; stops on the TRUE FP64 squared residual |b-Ax|^2 < prec*|b|^2.  Uses
  * the compressed inner operator for d = 3 (FP16 spinors with per-site norms, FP32 links in
  * the format yg_tune_inner_links measures fastest on the lattice at the first call, FP32
- * clover blocks, delta 0.1; if that stalls, the inner
- * solve restarts with FP32 spinors from its best iterate) and the generic FP32 operator
- * otherwise.  stats->fallback: bit 0 the FP64 CG finished the solve, bit 1 the inner
- * storage was raised to FP32. */
+ * clover blocks, delta 0.1, the CG update fused into the operator, launch shapes tuned at
+ * the first call; if that stalls, the inner solve restarts with FP32 spinors from its best
+ * iterate) and the generic FP32 operator otherwise.  stats->fallback: bit 0 the FP64 CG
+ * finished the solve, bit 1 the inner storage was raised to FP32.  Returns YG_STALL when even
+ * the FP64 CG cannot bring the true residual below prec (x then holds the FP64 CG's solution,
+ * which met prec on its recursive residual). */
 int yg_cg_mixed(yg_lattice *lat, const yg_inv_par *par, double *x, double *b, yg_solve_stats *stats);
 
 /* No reference counterpart: nrhs cg_inverter solves (cg.cpp:132-202) of the same operator
