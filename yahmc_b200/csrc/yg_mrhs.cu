@@ -12,15 +12,15 @@
 //
 // Every system keeps its own fields in the single-system formats (FP16 spinors with per-site
 // norms for p, Hphi p and the intermediates; FP32 x and r; A p = Hphi Hphi p is never stored:
-// x += alpha p, r -= alpha A p and the |r|^2 partials are the epilogue of the operator's
-// last step), its own device scalars (|r|^2 in two alternating slots, alpha, beta), its own
-// mass (the packed clover blocks are per launch slot, so the HMC and Hasenbusch monomials'
-// solves at m + dm and m share the launches), and the single-system rules: reliable updates
-// with the FP64 operator when |r| has fallen by delta or stagnates, a stop on the TRUE FP64
-// residual |b - A x|^2 < prec |b|^2, and a fall-back to the FP64 CG on a stall.  All
-// reductions are deterministic: per-block partials summed in index order by one warp per
-// system.  The host reads each iteration's |r|^2 values one iteration late from mapped
-// memory while the next iteration runs, as the single-system solver does.
+// r -= alpha A p and the |r|^2 partials are the epilogue of the operator's last step, and
+// x += alpha p rides with p = r + beta p), its own device scalars (|r|^2 in two alternating
+// slots, alpha, beta), its own mass (the packed clover blocks are per launch slot, so the HMC
+// and Hasenbusch monomials' solves at m + dm and m share the launches), and the
+// single-system rules: reliable updates with the FP64 operator when |r| has fallen by delta or
+// stagnates, a stop on the TRUE FP64 residual |b - A x|^2 < prec |b|^2, and a fall-back to the
+// FP64 CG on a stall.  All reductions are deterministic: per-block partials summed in index
+// order by one warp per system.  The host reads each iteration's |r|^2 values one iteration
+// late from mapped memory while the next iteration runs, as the single-system solver does.
 #include <cuda_fp16.h>
 #include <algorithm>
 #include <chrono>
@@ -59,10 +59,9 @@ struct MHopArgs {
   int nsys, ntile;
   double *part;             // NRM: part[j * nsb + site block] = sum of |dst_j|^2 (NRM 1) or of the new
   int nsb;                  //   |r_j|^2 (NRM 2) over the block
-  // NRM = 2, the last step of the iteration's second Hphi: the CG update of launch slot j
-  // (x_j += alpha p_j, r_j -= alpha q_j with q_j = the step's output, never stored)
-  float2 *x[kMR], *r[kMR];  // FP32 even-site words
-  MSpin p;
+  // NRM = 2, the last step of the iteration's second Hphi: the residual update of launch
+  // slot j (r_j -= alpha q_j with q_j = the step's output, never stored)
+  float2 *r[kMR];           // FP32 even-site words
   const double *scal;
   int sys[kMR];             // global system index of launch slot j (its scalars)
 };
@@ -268,20 +267,16 @@ __global__ void __launch_bounds__(kHopThreads, MinBlocks<R>::value) k_mhop(MHopA
           if (NRM != 2) sq = fmaf(out[k].x, out[k].x, fmaf(out[k].y, out[k].y, sq));
         }
         if constexpr (NRM == 2) {
-          // x += alpha p ; r -= alpha q on the (even) site, |r|^2 of the site
+          // r -= alpha q on the (even) site, |r|^2 of the site (x += alpha p rides with
+          // p = r + beta p in k_m_xpay, which reads p anyway)
           const float al = (float)a.scal[a.sys[s0 + r] * kW + M_ALPHA];
-          float2 pp[12];
-          sload<16>(pp, a.p.d[s0 + r], a.p.n[s0 + r], 0, h, g.Vh);
-          float2 *xs = a.x[s0 + r], *rs = a.r[s0 + r];
+          float2 *rs = a.r[s0 + r];
 #pragma unroll
           for (int k = 0; k < 12; k++) {
             const long i = (long)k * g.Vh + h;
-            float2 xi = xs[i], ri = rs[i];
-            xi.x = fmaf(al, pp[k].x, xi.x);
-            xi.y = fmaf(al, pp[k].y, xi.y);
+            float2 ri = rs[i];
             ri.x = fmaf(-al, out[k].x, ri.x);
             ri.y = fmaf(-al, out[k].y, ri.y);
-            xs[i] = xi;
             rs[i] = ri;
             sq = fmaf(ri.x, ri.x, fmaf(ri.y, ri.y, sq));
           }
@@ -354,17 +349,24 @@ __global__ void k_m_beta(double *scal, const double *part, int n, MVec v, int pa
   }
 }
 
-// p_i = r_i + beta_i p_i
+// x_i += alpha_i p_i ; p_i = r_i + beta_i p_i
 __global__ void __launch_bounds__(kVecThreads) k_m_xpay(const double *scal, MVec v, int Vh) {
   const int j = blockIdx.y;
   const float b = (float)scal[v.sys[j] * kW + M_BETA];
+  const float al = (float)scal[v.sys[j] * kW + M_ALPHA];
   const float2 *r = v.r[j];
+  float2 *x = v.x[j];
   for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += gridDim.x * blockDim.x) {
     float2 pp[12];
     sload<16>(pp, v.p.d[j], v.p.n[j], 0, h, Vh);
 #pragma unroll
     for (int k = 0; k < 12; k++) {
-      const float2 ri = r[(long)k * Vh + h];
+      const long i = (long)k * Vh + h;
+      const float2 ri = r[i];
+      float2 xi = x[i];
+      xi.x = fmaf(al, pp[k].x, xi.x);                 // x += alpha p with this iteration's p
+      xi.y = fmaf(al, pp[k].y, xi.y);
+      x[i] = xi;
       pp[k] = make_float2(fmaf(b, pp[k].x, ri.x), fmaf(b, pp[k].y, ri.y));
     }
     sstore<16>(v.p.d[j], v.p.n[j], pp, 0, h, Vh);
@@ -581,7 +583,7 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
   };
   int var = 2;                                // index into kVariants
   // t = Hphi p (first; mode 1 adds the <p, A p> partials) or Hphi t (second; mode 2 fuses the
-  // CG update, x += alpha p, r -= alpha Hphi t, with the |r|^2 partials), o the odd sites
+  // residual update, r -= alpha Hphi t, with the |r|^2 partials), o the odd sites
   auto hphi = [&](int mode, bool second) {
     MHopArgs a{};
     a.g = L.g;
@@ -603,8 +605,7 @@ int cg_mixed_mrhs(Lattice &L, const yg_inv_par &par, int nrhs, double *const *xs
       b.dst.n[j] = second ? nullptr : s.t.n;
       a.C[j] = clov[act[j]];
       b.C[j] = clov[act[j]];
-      b.x[j] = s.fx; b.r[j] = s.fr;
-      b.p.d[j] = s.p.d; b.p.n[j] = s.p.n;
+      b.r[j] = s.fr;
       b.sys[j] = act[j];
     }
     a.coeff = 0.5f; a.lo = Vh; a.n = Vh;

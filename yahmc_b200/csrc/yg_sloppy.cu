@@ -194,14 +194,13 @@ __global__ void __launch_bounds__(TPB, MINB) k_shop_shaped(SHopArgs a) {
   griddep_launch();
 }
 
-// The last Schur step of the iteration's second Hphi with the CG update as its epilogue:
-// q = Hphi t stays in registers, alpha = |r|^2 / <p, A p> (every block sums the partials of
-// the NRM hop in the same order), x += alpha p, r -= alpha q on the site, and the per-block
-// partials of the new |r|^2 go to part_r.  q is never stored.  Resident grid, grid-stride.
+// The last Schur step of the iteration's second Hphi with the residual update as its
+// epilogue: q = Hphi t stays in registers, alpha = |r|^2 / <p, A p> (every block sums the
+// partials of the NRM hop in the same order), r -= alpha q on the site, and the per-block
+// partials of the new |r|^2 go to part_r.  q is never stored; x += alpha p is left to the
+// p = r + beta p pass, which reads p anyway.  Resident grid, grid-stride.
 struct SCgArgs {
-  float2 *x, *r;                  // FP32 even-site words
-  const void *p;                  // search direction in the spinor format
-  const float *pn;
+  float2 *r;                      // FP32 even-site words
   double *scal;
   const double *part_pq;
   int n_pq;
@@ -224,19 +223,15 @@ __device__ __forceinline__ void shop_cg_body(const SHopArgs &a, const SCgArgs &c
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < a.n; t += gridDim.x * blockDim.x) {
     SiteNbr n;
     site_nbr(n, a.g, a.lo + t);
-    float2 q[12], pp[12];
+    float2 q[12];
     shop_out<P, LP, CP, K, 2>(q, a, a.lo + t, n);
-    sload<P>(pp, c.p, c.pn, 0, t, Vh);
     float s = 0.f;
 #pragma unroll
     for (int k = 0; k < 12; k++) {
       const long i = (long)k * Vh + t;
-      float2 xi = c.x[i], ri = c.r[i];
-      xi.x = fmaf(al, pp[k].x, xi.x);
-      xi.y = fmaf(al, pp[k].y, xi.y);
+      float2 ri = c.r[i];
       ri.x = fmaf(-al, q[k].x, ri.x);
       ri.y = fmaf(-al, q[k].y, ri.y);
-      c.x[i] = xi;
       c.r[i] = ri;
       s = fmaf(ri.x, ri.x, fmaf(ri.y, ri.y, s));
     }
@@ -439,7 +434,8 @@ __global__ void __launch_bounds__(256) k_s_from_d(void *dst, float *dn, const do
   }
 }
 
-// |r|^2 from the update's partials, beta = |r|^2 / |r_old|^2, p = r + beta p; block 0
+// |r|^2 from the update's partials, beta = |r|^2 / |r_old|^2, x += alpha p, p = r + beta p
+// (x and p in one pass: the p it reads is the direction of this iteration); block 0
 // stores |r|^2 for the next iteration and into *hist, then counts the iteration (S_ITER)
 // and stores the count into *seq (hist and seq are mapped host memory, which the host polls
 // one iteration later).  Nothing in the arguments changes between iterations of the same
@@ -447,7 +443,7 @@ __global__ void __launch_bounds__(256) k_s_from_d(void *dst, float *dn, const do
 template <int P>
 __global__ void __launch_bounds__(256) k_s_xpay(void *p, float *pn, double *scal, const double *part_r, int n_r,
                                                 int par, double *hist, unsigned long long *seq, const float2 *r,
-                                                int Vh) {
+                                                float2 *x, int Vh) {
   griddep_wait();
   const double rr = sum_partials(part_r, n_r);
   const float b = (float)(rr / scal[S_RR0 + par]);
@@ -459,12 +455,18 @@ __global__ void __launch_bounds__(256) k_s_xpay(void *p, float *pn, double *scal
     __threadfence_system();
     *reinterpret_cast<volatile unsigned long long *>(seq) = (unsigned long long)done;
   }
+  const float al = (float)scal[S_ALPHA];
   for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += gridDim.x * blockDim.x) {
     float2 pp[12];
     sload<P>(pp, p, pn, 0, h, Vh);
 #pragma unroll
     for (int k = 0; k < 12; k++) {
-      float2 ri = r[(long)k * Vh + h];
+      const long i = (long)k * Vh + h;
+      const float2 ri = r[i];
+      float2 xi = x[i];
+      xi.x = fmaf(al, pp[k].x, xi.x);                 // x += alpha p with the p of this iteration
+      xi.y = fmaf(al, pp[k].y, xi.y);
+      x[i] = xi;
       pp[k] = make_float2(fmaf(b, pp[k].x, ri.x), fmaf(b, pp[k].y, ri.y));
     }
     sstore<P>(p, pn, pp, 0, h, Vh);
@@ -715,9 +717,9 @@ static void sloppy_hphi(Lattice &L, SField dst, SField src, SField tmp, bool nrm
   L.mvm += 2;
 }
 
-// q = Hphi(t) with the CG update fused into its last step: x += alpha p, r -= alpha q and the
+// q = Hphi(t) with the residual update fused into its last step: r -= alpha q and the
 // partials of the new |r|^2 (par = iteration parity, selecting the |r|^2 slot)
-static void sloppy_hphi_cg(Lattice &L, SField t, SField tmp, float *x, float *r, SField p, int par) {
+static void sloppy_hphi_cg(Lattice &L, SField t, SField tmp, float *r, int par) {
   SHopArgs a{};
   a.g = L.g;
   a.U = L.sl_links.p;
@@ -734,9 +736,7 @@ static void sloppy_hphi_cg(Lattice &L, SField t, SField tmp, float *x, float *r,
   b.coeff = -0.5f;
   b.lo = 0;
   SCgArgs c{};
-  c.x = reinterpret_cast<float2 *>(x);
   c.r = reinterpret_cast<float2 *>(r);
-  c.p = p.data; c.pn = p.norm;
   c.scal = dscal(L);
   c.part_pq = part_pq(L);
   c.n_pq = L.sl_gnrm[shape_nrm(L)];
@@ -759,11 +759,11 @@ static void sloppy_hphi_cg(Lattice &L, SField t, SField tmp, float *x, float *r,
   L.mvm += 2;
 }
 
-static void sloppy_xpay(Lattice &L, SField p, const float *r, int par, double *hist) {
+static void sloppy_xpay(Lattice &L, SField p, const float *r, float *x, int par, double *hist) {
   YG_SPINOR_DISPATCH(L.sl_prec, {
     launch_pdl(k_s_xpay<SP>, L.sl_grid_vec, 256, L.stream, p.data, p.norm, dscal(L), part_r(L), L.sl_gcg[shape_cg(L)],
                par,
-               hist, hist_seq(L), (const float2 *)r, (int)L.Vh);
+               hist, hist_seq(L), (const float2 *)r, (float2 *)x, (int)L.Vh);
     YG_LAUNCHED();
   });
 }
@@ -853,10 +853,10 @@ struct IterGraphs {
 
 // Mixed-precision CG on Hphi_sq with the compressed inner operator.  x and r of the inner
 // iterations are FP32, p and Hphi p are in the inner storage format, A p = Hphi Hphi p stays
-// in registers: the x and r updates are the epilogue of the operator's last step.  alpha
-// and beta live on the device, so an inner iteration is five launches (four operator steps
-// and p = r + beta p), replayed as one CUDA graph per iteration, and no host
-// synchronisation; the host
+// in registers: the r update is the epilogue of the operator's last step, the x update rides
+// with p = r + beta p.  alpha and beta live on the device, so an inner iteration is five
+// launches (four operator steps and x += alpha p, p = r + beta p), replayed as one CUDA graph
+// per iteration, and no host synchronisation; the host
 // reads each iteration's |r|^2 one iteration late (while the next one runs) and then
 // decides on a reliable update: b - A x is recomputed with the FP64 operator whenever the
 // iterated |r| fell below delta times its value at the last update, r is replaced by it
@@ -933,8 +933,8 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int 
       for (int gp = 0; gp < 2; gp++)
         graphs.capture(L, gp, [&] {
           sloppy_hphi(L, t, p, o, true);
-          sloppy_hphi_cg(L, t, o, fx, fr, p, gp);
-          sloppy_xpay(L, p, fr, gp, const_cast<double *>(hist) + gp);
+          sloppy_hphi_cg(L, t, o, fr, gp);
+          sloppy_xpay(L, p, fr, fx, gp, const_cast<double *>(hist) + gp);
         });
     }
     while (true) {
@@ -947,8 +947,8 @@ int cg_mixed_sloppy(Lattice &L, const yg_inv_par &par, int prec, int reals, int 
         graphs.launch(L, slot);
       } else {
         sloppy_hphi(L, t, p, o, true);
-        sloppy_hphi_cg(L, t, o, fx, fr, p, slot);
-        sloppy_xpay(L, p, fr, slot, const_cast<double *>(hist) + slot);
+        sloppy_hphi_cg(L, t, o, fr, slot);
+        sloppy_xpay(L, p, fr, fx, slot, const_cast<double *>(hist) + slot);
       }
       it++;
       if (!pending) { pending = true; continue; }
@@ -1090,7 +1090,6 @@ static void tune_shape(Lattice &L, double mass, int reals) {
   const int mvm0 = L.mvm;
   SField p = sfield(L, 41), t = sfield(L, 44), o = sfield(L, 45);
   float *fr = reinterpret_cast<float *>(L.scratch_field(40));
-  float *fx = reinterpret_cast<float *>(L.scratch_field(42));
   sloppy_from_d(L, p, L.scratch_field(3));
   set_scalar(L, S_RR0, 1.0);
   cudaEvent_t e0, e1;
@@ -1119,7 +1118,7 @@ static void tune_shape(Lattice &L, double mass, int reals) {
   sloppy_hphi(L, t, p, o, true);            // the <p, A p> partials the update kernel reads
   for (int v = 0; v < kStep2Shapes; v++) {
     L.sl_shape_c = v;
-    const float ms = timed([&] { sloppy_hphi_cg(L, t, o, fx, fr, p, 0); });
+    const float ms = timed([&] { sloppy_hphi_cg(L, t, o, fr, 0); });
     if (v == 0 || ms < best_c) { best_c = ms; vc = v; }
     if (std::getenv("YG_TUNE_LOG"))
       fprintf(stderr, "yg tune inner Hphi with the CG update: step 2 cut for %d blocks/SM: %.4f ms\n", kStep2Min[v],
