@@ -346,15 +346,6 @@ __global__ void __launch_bounds__(128) k_hop(HopArgs<R> a) {
   if (t < a.n) hop_body<D, R, EPI>(a, t);
 }
 
-// The d = 3 FP64 Schur steps with registers cut for 4 resident blocks per SM (128 instead of
-// 140-142: 16 instead of 12 warps per SM); the steps are bound by memory latency, which the
-// extra warps hide better than the few spilled words cost.
-template <int D, typename R, int EPI>
-__global__ void __launch_bounds__(128, 4) k_hop_occ(HopArgs<R> a) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < a.n) hop_body<D, R, EPI>(a, t);
-}
-
 // clover_kernel (dirac.cpp:25-107) standalone: dst (=|+=) A psi over [lo, lo+n)
 template <int D>
 __global__ void __launch_bounds__(128) k_clover(double2 *dst, const double2 *src, const double2 *cl, Geom g,
@@ -519,10 +510,6 @@ __global__ void k_logdet(double *out, const double2 *ldl, int Vh) {
 template <int D, typename R>
 static void launch_hop_epi(const HopArgs<R> &a, int epi, cudaStream_t s) {
   const int t = 128;
-  if constexpr (D == 3 && sizeof(R) == sizeof(double)) {
-    if (epi == EPI_CLOVADD) { k_hop_occ<D, R, EPI_CLOVADD><<<nblk(a.n, t), t, 0, s>>>(a); return; }
-    if (epi == EPI_CLOVPK) { k_hop_occ<D, R, EPI_CLOVPK><<<nblk(a.n, t), t, 0, s>>>(a); return; }
-  }
   switch (epi) {
     case EPI_PLAIN: k_hop<D, R, EPI_PLAIN><<<nblk(a.n, t), t, 0, s>>>(a); break;
     case EPI_CLOVINV: k_hop<D, R, EPI_CLOVINV><<<nblk(a.n, t), t, 0, s>>>(a); break;
